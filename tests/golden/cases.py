@@ -1,0 +1,148 @@
+"""Small box workloads pinned by golden vectors from the reference.
+
+Each case is a reference config dict (keys as in the reference's config files)
+plus the seeds of its synthetic catalogs.  Catalogs are regenerated from the
+seeds (numpy PCG64 is deterministic) and checked against the stored position
+checksum, so the fixtures only hold results.
+"""
+from __future__ import annotations
+
+import copy
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+_BASE = dict(
+    geometry="box-like",
+    rsd=[0, 0, 1],
+    apply_rsd=False,
+    cosmology={"h": 0.6766, "Omega0": 0.31},
+    redshift_box=0.0,
+    compensation=True,
+)
+
+# (name, config overrides, catalogs: {letter: (seed, n_particles, weighted)})
+CASES = [
+    ("pk_auto_cic_il", dict(statistic="pk", correlation_mode="auto", nmesh=[32] * 3,
+                            boxsize=[1000.0] * 3, sampler="cic", interlaced=True,
+                            k_min=0.005, k_max=0.095, k_bins=9, poles=[0, 2, 4]),
+     {"a": (11, 20000, False)}),
+    ("pk_cross_tsc_noil", dict(statistic="pk", correlation_mode="cross", nmesh=[32] * 3,
+                               boxsize=[800.0] * 3, sampler="tsc", interlaced=False,
+                               k_min=0.01, k_max=0.11, k_bins=5, poles=[0, 1, 2], rsd=[0, 1, 0]),
+     {"a": (12, 15000, True), "b": (13, 12000, False)}),
+    ("pk_auto_ngp_k0", dict(statistic="pk", correlation_mode="auto", nmesh=[32] * 3,
+                            boxsize=[1000.0] * 3, sampler="ngp", interlaced=True,
+                            k_min=0.0, k_max=0.09, k_bins=6, poles=[0, 2]),
+     {"a": (14, 20000, False)}),
+    ("pk_auto_pcs_noil", dict(statistic="pk", correlation_mode="auto", nmesh=[32] * 3,
+                              boxsize=[1000.0] * 3, sampler="pcs", interlaced=False,
+                              k_min=0.005, k_max=0.095, k_bins=9, poles=[0, 2, 4],
+                              rsd=[0.6, 0.0, 0.8]),
+     {"a": (15, 20000, False)}),
+    ("bk_diag_000_tsc", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="tsc", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[0, 0, 0],
+                             data_vector_mode="diagonal", shotnoise_mode="ana"),
+     {"a": (21, 20000, False)}),
+    ("bk_diag_202_tsc", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="tsc", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[2, 0, 2],
+                             data_vector_mode="diagonal", shotnoise_mode="both"),
+     {"a": (21, 20000, False)}),
+    ("bk_diag_110_cic", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="cic", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[1, 1, 0],
+                             data_vector_mode="diagonal", shotnoise_mode="fft"),
+     {"a": (22, 20000, True)}),
+    ("bk_full_000_pcs", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="pcs", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[0, 0, 0],
+                             data_vector_mode="full", shotnoise_mode="both", block_size=2),
+     {"a": (23, 20000, False)}),
+    ("bk_full_202_pcs", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="pcs", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[2, 0, 2],
+                             data_vector_mode="full", shotnoise_mode="both", block_size="full"),
+     {"a": (23, 20000, False)}),
+    ("bk_full_112_cic", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="cic", interlaced=False,
+                             k_min=0.005, k_max=0.045, k_bins=3, angu_config=[1, 1, 2],
+                             data_vector_mode="full", shotnoise_mode="both", block_size=1),
+     {"a": (24, 20000, False)}),
+    ("bk_full_220_ngp", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="ngp", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=3, angu_config=[2, 2, 0],
+                             data_vector_mode="full", shotnoise_mode="fft"),
+     {"a": (25, 20000, False)}),
+    ("bk_cross_aab_full", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="aab",
+                               nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="tsc", interlaced=True,
+                               k_min=0.005, k_max=0.045, k_bins=3, angu_config=[0, 0, 0],
+                               data_vector_mode="full", shotnoise_mode="both"),
+     {"a": (26, 15000, False), "b": (27, 12000, True)}),
+    ("bk_cross_abb_diag", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="abb",
+                               nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="cic", interlaced=True,
+                               k_min=0.005, k_max=0.045, k_bins=4, angu_config=[2, 0, 2],
+                               data_vector_mode="diagonal", shotnoise_mode="both"),
+     {"a": (26, 15000, False), "b": (27, 12000, True)}),
+    ("bk_cross_abc_full", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="abc",
+                               nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="tsc", interlaced=False,
+                               k_min=0.005, k_max=0.045, k_bins=3, angu_config=[2, 0, 2],
+                               data_vector_mode="full", shotnoise_mode="ana"),
+     {"a": (26, 15000, False), "b": (27, 12000, True), "c": (28, 10000, False)}),
+]
+
+
+def catalog_positions(seed, n_particles, boxsize):
+    from cosmonpc_b200.mocks import lognormal_box
+
+    return lognormal_box(n_particles, boxsize, seed, grid=32)
+
+
+def catalog_weights(seed, n):
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    return 0.5 + rng.random(n)
+
+
+def build_case(name, workdir):
+    """Write the case's catalogs under ``workdir`` and return (config, checksums)."""
+    for cname, over, cats in CASES:
+        if cname != name:
+            continue
+        cfg = copy.deepcopy(_BASE)
+        cfg.update(copy.deepcopy(over))
+        L = cfg["boxsize"][0]
+        weighted = any(v[2] for v in cats.values())
+        cfg["column_names"] = ["x", "y", "z", "w"] if weighted else ["x", "y", "z"]
+        catalogs = {"data_a": None, "randoms_a": None, "data_b": None, "randoms_b": None}
+        sums = {}
+        os.makedirs(workdir, exist_ok=True)
+        for letter, (seed, npart, wflag) in cats.items():
+            pos = catalog_positions(seed, npart, L)
+            arr = pos
+            if weighted:
+                w = catalog_weights(seed, len(pos)) if wflag else np.ones(len(pos))
+                arr = np.column_stack([pos, w])
+            path = os.path.join(workdir, "%s_%s.npy" % (name, letter))
+            np.save(path, arr)
+            catalogs["data_" + letter] = path
+            sums[letter] = float(np.sum(arr))
+        cfg["catalogs"] = catalogs
+        cfg["output_dir"] = os.path.join(workdir, "out_" + name)
+        return cfg, sums
+    raise KeyError(name)
+
+
+def flatten_result(res):
+    """Numeric keys of a result dict as a flat {name: ndarray} mapping."""
+    out = {}
+    for k, v in res.items():
+        if k == "SN_terms":
+            for kk, vv in v.items():
+                out["SN_terms." + kk] = np.asarray(vv)
+        elif k in ("B_sugi", "Bk_raw", "Shot_noise", "I_norm", "k_eff", "nmodes", "k_num",
+                   "P_shot") or (k.startswith("P") and k[1:].isdigit()):
+            out[k] = np.asarray(v)
+    return out

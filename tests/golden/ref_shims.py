@@ -1,0 +1,188 @@
+"""Import the unmodified reference package on one CPU process.
+
+Used only by ``make_golden.py`` in a container that has the reference sources.
+The reference imports ``mpi4py``, ``numexpr``, ``pmesh``, ``astropy``, ``fitsio``
+and ``h5py``; none is installed here, so this module places stand-ins in
+``sys.modules`` before the import:
+
+* ``mpi4py.MPI``: a one-rank communicator whose reductions are identities.
+* ``numexpr.evaluate``: evaluates the expression string with numpy in the
+  caller's frame (the form ``sympy.lambdify(..., "numexpr")`` emits).
+* ``pmesh.pm.ParticleMesh``: ``oracle.pmesh_lite`` (restated pmesh behaviour).
+* ``astropy.cosmology.FlatLambdaCDM``: comoving distance by ``scipy.integrate.quad``.
+* ``fitsio`` / ``h5py``: placeholders (box ``.npy`` workloads never reach them).
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+import types
+
+import numpy as np
+
+REFERENCE_SRC = os.environ.get("COSMONPC_REFERENCE_SRC", "/root/reference/src")
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REPO = os.path.dirname(os.path.dirname(_HERE))
+
+
+class _Comm:
+    rank = 0
+    size = 1
+
+    def Get_rank(self):
+        return 0
+
+    def Get_size(self):
+        return 1
+
+    def reduce(self, x, op=None, root=0):
+        return x
+
+    def allreduce(self, x, op=None):
+        return x
+
+    def bcast(self, x, root=0):
+        return x
+
+    def gather(self, x, root=0):
+        return [x]
+
+    def allgather(self, x):
+        return [x]
+
+    def Barrier(self):
+        return None
+
+    def barrier(self):
+        return None
+
+    def Allreduce(self, sendbuf, recvbuf, op=None):
+        src = sendbuf[0] if isinstance(sendbuf, (list, tuple)) else sendbuf
+        dst = recvbuf[0] if isinstance(recvbuf, (list, tuple)) else recvbuf
+        np.copyto(np.asarray(dst), np.asarray(src))
+
+
+def _install_mpi():
+    mpi4py = types.ModuleType("mpi4py")
+    MPI = types.ModuleType("mpi4py.MPI")
+    MPI.COMM_WORLD = _Comm()
+    MPI.SUM, MPI.MIN, MPI.MAX = "sum", "min", "max"
+    MPI.DOUBLE = "double"
+
+    class Request:
+        @staticmethod
+        def Waitall(reqs):
+            return None
+
+    MPI.Request = Request
+    mpi4py.MPI = MPI
+    sys.modules["mpi4py"] = mpi4py
+    sys.modules["mpi4py.MPI"] = MPI
+
+
+def _install_numexpr():
+    ne = types.ModuleType("numexpr")
+    ne.__version__ = "2.14.1"
+    funcs = {n: getattr(np, n) for n in (
+        "sqrt", "sin", "cos", "tan", "exp", "log", "abs", "real", "imag", "conj",
+        "where", "arctan2", "arcsin", "arccos", "arctan", "sinh", "cosh", "tanh")}
+    funcs["complex"] = lambda a, b: np.asarray(a) + 1j * np.asarray(b)
+
+    def evaluate(ex, local_dict=None, global_dict=None, **kw):
+        frame = sys._getframe(1)
+        ns = dict(funcs)
+        ns.update(frame.f_globals if global_dict is None else global_dict)
+        ns.update(frame.f_locals if local_dict is None else local_dict)
+        return eval(ex, {"__builtins__": {}}, ns)
+
+    ne.evaluate = evaluate
+    sys.modules["numexpr"] = ne
+
+
+def _install_pmesh():
+    sys.path.insert(0, _REPO)
+    from oracle import pmesh_lite
+
+    pmesh = types.ModuleType("pmesh")
+    pm = types.ModuleType("pmesh.pm")
+    pm.ParticleMesh = pmesh_lite.ParticleMesh
+    pm.RealField = pmesh_lite.RealField
+    pm.ComplexField = pmesh_lite.ComplexField
+    pm.TransposedComplexField = pmesh_lite.ComplexField
+    pmesh.ParticleMesh = pmesh_lite.ParticleMesh
+    pmesh.pm = pm
+    sys.modules["pmesh"] = pmesh
+    sys.modules["pmesh.pm"] = pm
+
+
+def _install_astropy():
+    from scipy.integrate import quad
+
+    astropy = types.ModuleType("astropy")
+    cosmo = types.ModuleType("astropy.cosmology")
+    units = types.ModuleType("astropy.units")
+
+    class _Q(float):
+        @property
+        def value(self):
+            return float(self)
+
+        def to(self, unit):
+            return self
+
+    class FlatLambdaCDM:
+        def __init__(self, H0=70.0, Om0=0.3, Tcmb0=0.0, **kw):
+            self.H0 = _Q(float(getattr(H0, "value", H0)))
+            self.Om0 = float(Om0)
+            self.h = self.H0 / 100.0
+
+        def efunc(self, z):
+            z = np.asarray(z, dtype=np.float64)
+            return np.sqrt(self.Om0 * (1 + z) ** 3 + (1 - self.Om0))
+
+        def comoving_distance(self, z):
+            c = 299792.458
+            zz = np.atleast_1d(np.asarray(z, dtype=np.float64))
+            out = np.array([quad(lambda t: 1.0 / float(self.efunc(t)), 0.0, zi)[0] for zi in zz])
+            out *= c / self.H0
+            return _Arr(out.reshape(np.shape(z)))
+
+    class _Arr(np.ndarray):
+        def __new__(cls, a):
+            return np.asarray(a).view(cls)
+
+        @property
+        def value(self):
+            return np.asarray(self)
+
+    cosmo.FlatLambdaCDM = FlatLambdaCDM
+    cosmo.Planck18 = FlatLambdaCDM(67.66, 0.30966)
+    units.Mpc = 1.0
+    units.km = 1.0
+    units.s = 1.0
+    astropy.cosmology = cosmo
+    astropy.units = units
+    sys.modules["astropy"] = astropy
+    sys.modules["astropy.cosmology"] = cosmo
+    sys.modules["astropy.units"] = units
+
+
+def _install_placeholders():
+    for name in ("fitsio", "h5py"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+
+
+def import_reference():
+    """Install the stand-ins and return the reference's ``cosmonpc`` package."""
+    _install_mpi()
+    _install_numexpr()
+    _install_pmesh()
+    _install_astropy()
+    _install_placeholders()
+    if REFERENCE_SRC not in sys.path:
+        sys.path.insert(0, REFERENCE_SRC)
+    import cosmonpc  # noqa: F401  (the reference package)
+    import cosmonpc.task_executor as te
+
+    return te
