@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: Sugiyama bispectrum, box, 256^3 full data vector.
+
+Workload (one "step" = one data vector): a seeded lognormal box catalog of
+4e6 particles in a 2000 Mpc/h box, PCS interlaced paint on 256^3, 20 k-bins
+over 0.01-0.20 h/Mpc, angular configurations (0,0,0) and (2,0,2) full 20x20
+((0,2,2) is their transpose), shot noise "both" (analytical and FFT S3).
+
+value  = seconds per data vector of the fast form (FP32 fields, FP64
+         accumulation, shared transforms) with the catalog resident in HBM.
+e2e    = the same through the public in-memory API with the catalog in pinned
+         host memory: H2D of positions and D2H of the results every step.
+plain  = the FP64 per-configuration drop-in on the same catalog (reported,
+         with the max relative error of the fast form against it).
+
+Multi-GPU (torchrun): each rank measures its own mock (replicas, weak scaling,
+no data-path collective); timing is max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOAD = dict(n_particles=4_000_000, boxsize=2000.0, nmesh=256, sampler="pcs", interlaced=True,
+                k_min=0.01, k_max=0.20, k_bins=20, angu_configs=[(0, 0, 0), (2, 0, 2)],
+                data_vector_mode="full", shotnoise_mode="both")
+SMALL = dict(WORKLOAD, n_particles=500_000, nmesh=128, boxsize=1000.0, k_max=0.19, k_bins=12)
+METRIC = "bk_sugi 256^3 full-mode s/data-vector"
+UNIT = "s/data-vector"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_baseline_estimate(workload, seed):
+    """Time the oracle port (numpy/scipy, all host threads) on a bounded sample
+    of the workload and extrapolate to one data vector by operation counts.
+
+    The reference computes each angular configuration in its own run_stats
+    call (paint + forward transforms each), with F-field and pair counts per
+    config as in clustering_estimator.py:867-995 and :1182-1384."""
+    import numpy as np
+
+    from cosmonpc_b200.mocks import BASE_SEED, lognormal_box
+    from oracle import angular as oang
+    from oracle import box as obox
+    from oracle.pmesh_lite import _ifftn
+
+    n, L = workload["nmesh"], workload["boxsize"]
+    pos = lognormal_box(workload["n_particles"], L, seed)
+    w = np.ones(len(pos))
+    t0 = time.perf_counter()
+    field = obox.paint_field(pos, w, n, L, workload["sampler"], workload["interlaced"])
+    t_paint = time.perf_counter() - t0
+    geo = obox.KGeom(n, L)
+    t0 = time.perf_counter()
+    c = obox._fwd(field)
+    t_fft = time.perf_counter() - t0
+    edges = np.linspace(workload["k_min"], workload["k_max"], workload["k_bins"] + 1)
+    mask = np.logical_and(geo.knorm >= edges[3], geo.knorm < edges[4])
+    y = oang.ylm_function(2, 0, True)(*geo.khat)
+    t0 = time.perf_counter()
+    F1 = _ifftn(c * y * mask) * float(n) ** 3
+    F2 = _ifftn(c * mask) * float(n) ** 3
+    t_field = (time.perf_counter() - t0) / 2
+    G = np.real(_ifftn(c))
+    t0 = time.perf_counter()
+    for _ in range(3):
+        np.sum(G * F1 * F2)
+    t_pair = (time.perf_counter() - t0) / 3
+    B = workload["k_bins"]
+    ncfg = len(workload["angu_configs"])
+    fields, pairs = 0, 0
+    for (l1, l2, L_) in workload["angu_configs"]:
+        f = B if (l1 == l2) else 2 * B
+        p = B * (B + 1) // 2 if (l1 == l2) else B * B
+        fields += f * (2 if workload["shotnoise_mode"] in ("fft", "both") else 1)
+        pairs += p * (2 if workload["shotnoise_mode"] in ("fft", "both") else 1)
+    ffts = ncfg * (1 + 2 + 1)  # r2c(delta), c2r(G), c2r(S3 source) + the paint's combine counted in t_paint
+    total = ncfg * t_paint + ffts * t_fft + fields * t_field + pairs * t_pair
+    sample = (f"oracle port, 1 interlaced paint of {len(pos)} particles + 1 forward FFT + 2 shell fields + "
+              f"3 triple sums at {n}^3, extrapolated to {ncfg} configs x (paint + {ffts // ncfg} FFTs) + "
+              f"{fields} shell fields + {pairs} triple sums")
+    return total, sample, os.cpu_count()
+
+
+# ----------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="128^3 profiling case (for ncu captures)")
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    workload = SMALL if args.small else WORKLOAD
+    from cosmonpc_b200.mocks import BASE_SEED
+
+    seed = BASE_SEED + 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        vals = []
+        info = None
+        for i in range(args.warmup + args.steps):
+            v, sample, cores = cpu_baseline_estimate(workload, seed)
+            if i >= args.warmup:
+                vals.append(v)
+            info = (sample, cores)
+        value = sum(vals) / len(vals)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "bk_sugi box full 256^3, 4e6 lognormal particles, PCS interlaced, "
+                                       "20 bins 0.01-0.20, (000)+(202), shotnoise both"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[1], "kind": "port", "sample": info[0]},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from cosmonpc_b200 import _lib, api, build
+    from cosmonpc_b200.mocks import lognormal_box
+
+    build.build()
+    W = workload
+    pos_host = lognormal_box(W["n_particles"], W["boxsize"], seed + 1000 * rank)
+    pos_pinned = torch.from_numpy(pos_host).pin_memory()
+    pos_dev = pos_pinned.cuda()
+    common = dict(nmesh=W["nmesh"], boxsize=W["boxsize"], sampler=W["sampler"], interlaced=W["interlaced"],
+                  k_min=W["k_min"], k_max=W["k_max"], k_bins=W["k_bins"], angu_configs=W["angu_configs"],
+                  data_vector_mode=W["data_vector_mode"], shotnoise_mode=W["shotnoise_mode"])
+
+    def step_resident():
+        return api.bk_sugi_box_vector(pos_dev, None, precision="f32", **common)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_resident()
+    barrier()
+    # ---- timed region (device resident inputs)
+    _lib.timer = _lib.KernelTimer()
+    launches0 = _lib.launch_count
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.steps):
+            res_fast = step_resident()
+        ev1.record()
+        barrier()
+    t_fast = ev0.elapsed_time(ev1) / 1000.0
+    launches = (_lib.launch_count - launches0) // args.steps
+    ksum = _lib.timer.summary()
+    _lib.timer = None
+    t_fast = max_over_ranks(t_fast)
+    value = t_fast / (args.steps * world)
+
+    # ---- end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            r = api.bk_sugi_box_vector(pos_pinned.numpy(), None, precision="f32", **common)
+        e1.record()
+        barrier()
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+        d2h = sum(sum(np.asarray(v).nbytes for k, v in d.items() if k != "SN_terms")
+                  + sum(np.asarray(v).nbytes for v in d["SN_terms"].values()) for d in r)
+        e2e = {"value": t_e2e / (args.steps * world), "unit": UNIT,
+               "h2d_bytes_per_step": int(pos_host.nbytes), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- plain FP64 per-configuration path, and the error of the fast form against it
+    plain = None
+    max_rel = None
+    if args.plain_steps > 0:
+        barrier()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record()
+        for _ in range(args.plain_steps):
+            res_plain = api.bk_sugi_box_plain(pos_dev, None, **common)
+        p1.record()
+        barrier()
+        plain = max_over_ranks(p0.elapsed_time(p1) / 1000.0) / args.plain_steps
+        max_rel = 0.0
+        for a, b in zip(res_fast, res_plain):
+            for key in ("B_sugi", "Bk_raw", "Shot_noise"):
+                den = np.max(np.abs(b[key]))
+                if den > 0:
+                    max_rel = max(max_rel, float(np.max(np.abs(a[key] - b[key])) / den))
+            for key, v in b["SN_terms"].items():
+                den = np.max(np.abs(v))
+                if den > 0:
+                    max_rel = max(max_rel, float(np.max(np.abs(a["SN_terms"][key] - v)) / den))
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    peak, peak_kind = _peaks()
+    ours = {k: v for k, v in ksum.items() if not k.startswith("cufft")}
+    dom_name = max(ours, key=lambda k: ours[k][1])
+    cnt, tms, nbytes = ksum[dom_name]
+    achieved = (nbytes / cnt) / (tms / cnt / 1000.0) / 1e9
+    kernels = {k: {"launches_per_step": v[0] // args.steps, "ms_per_step": v[1] / args.steps,
+                   "GB_per_s": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] > 0 and v[2] else None}
+               for k, v in sorted(ksum.items(), key=lambda kv: -kv[1][1])}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cv, sample, cores = cpu_baseline_estimate(W, seed)
+        cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_fast / args.steps * 1000.0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulation", "data": "synthetic",
+        "config": {"workload": "bk_sugi box full %d^3, %.0e lognormal particles, %s interlaced, %d bins %.2f-%.2f, "
+                               "(000)+(202) [(022) = transpose], shotnoise %s"
+                               % (W["nmesh"], W["n_particles"], W["sampler"].upper(), W["k_bins"], W["k_min"],
+                                  W["k_max"], W["shotnoise_mode"]),
+                   "l2": "working set > L2 (shell fields %.1f GB)" % (
+                       (3 * W["k_bins"]) * W["nmesh"] ** 3 * 4 / 1e9),
+                   "parallelism": "replicas x%d" % world},
+        "e2e": e2e,
+        "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),
+                      "max_rel_err_fast_vs_plain": max_rel},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None},
+        "kernels": kernels,
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,83 @@
+"""In-memory entry points (no catalog files): one call turns a catalog held in
+host or device memory into the reference's result dictionaries.
+
+``bk_sugi_box_vector`` is the fast form: several angular configurations of one
+catalog share the paint, the forward transforms, G, the shell fields and the
+FFT shot-noise shells; fields are FP32 with FP64 accumulation.
+``bk_sugi_box_plain`` is the plain drop-in form: FP64 throughout, one
+configuration per call (as ``run_stats`` is called once per configuration).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import clustering_estimator as ce
+from . import engine
+
+
+def _to_device(pos, weight):
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if isinstance(pos, np.ndarray):
+        tp = torch.from_numpy(np.ascontiguousarray(pos, dtype=np.float64))
+        if not tp.is_pinned():
+            tp = tp.pin_memory()
+        pos = tp.to(dev, non_blocking=True)
+    if isinstance(weight, np.ndarray):
+        tw = torch.from_numpy(np.ascontiguousarray(weight, dtype=np.float64)).pin_memory()
+        weight = tw.to(dev, non_blocking=True)
+    return pos, weight
+
+
+def _weight_sum(pos, weight):
+    if weight is None:
+        return float(pos.shape[0])
+    if isinstance(weight, np.ndarray):
+        return float(np.sum(weight))
+    return float(weight.sum().item())
+
+
+def box_attrs(n_gal, weight_sum, boxsize, **settings):
+    """stat_attrs of an auto box run (mesh_generator.py:56-60, :106-117)."""
+    attrs = dict(settings)
+    attrs.update({"NZ_a": weight_sum / float(np.prod(np.array([boxsize] * 3))), "N_gal_a": int(n_gal)})
+    return attrs
+
+
+def bk_sugi_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins,
+                       angu_configs, data_vector_mode="full", shotnoise_mode="both",
+                       precision="f32", block_size="full"):
+    """Auto bispectrum multipoles of one box catalog for every configuration in
+    ``angu_configs`` (list of (l1, l2, L)); returns a list of result dicts."""
+    wsum = _weight_sum(pos, weight)
+    dpos, dw = _to_device(pos, weight)
+    pm = engine.paint(dpos, dw, nmesh, boxsize, sampler, interlaced, precision, sum_w=wsum)
+    attrs = box_attrs(dpos.shape[0], wsum, boxsize, boxsize=[boxsize] * 3, nmesh=[nmesh] * 3,
+                      k_min=k_min, k_max=k_max, k_bins=k_bins, sampler=sampler, interlaced=interlaced,
+                      data_vector_mode=data_vector_mode, shotnoise_mode=shotnoise_mode)
+    return ce.bk_sugi_box_multi({"a": pm}, "auto", "aaa", [tuple(c) for c in angu_configs], attrs,
+                                precision=precision, block_size=block_size)
+
+
+def bk_sugi_box_plain(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins,
+                      angu_configs, data_vector_mode="full", shotnoise_mode="both", block_size="full"):
+    """The plain FP64 drop-in: one full per-configuration call each, like
+    repeated ``run_stats`` calls without the file I/O."""
+    out = []
+    for cfg in angu_configs:
+        out += bk_sugi_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins,
+                                  [cfg], data_vector_mode, shotnoise_mode, precision="f64",
+                                  block_size=block_size)
+    return out
+
+
+def pk_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles,
+                  rsd=(0, 0, 1), precision="f32"):
+    """Auto power-spectrum multipoles of one box catalog."""
+    wsum = _weight_sum(pos, weight)
+    dpos, dw = _to_device(pos, weight)
+    pm = engine.paint(dpos, dw, nmesh, boxsize, sampler, interlaced, precision, sum_w=wsum)
+    attrs = box_attrs(dpos.shape[0], wsum, boxsize, boxsize=[boxsize] * 3, nmesh=[nmesh] * 3,
+                      k_min=k_min, k_max=k_max, k_bins=k_bins, sampler=sampler, interlaced=interlaced,
+                      poles=list(poles), rsd=list(rsd))
+    return ce.calculate_power_spectrum_box(pm, None, "auto", attrs)

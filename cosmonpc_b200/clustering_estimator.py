@@ -1,0 +1,407 @@
+"""Box-geometry estimators on the device (drop-in for the reference's
+``calculate_power_spectrum_box`` and ``calculate_bk_sugi_box``).
+
+Inputs are :class:`engine.PaintedMesh` objects (the painted "rfields"); outputs
+are the same result dictionaries, keys and dtypes as the reference
+(src/cosmonpc/clustering_estimator.py:566-746 and :749-1555).  Host code here
+only does O(k_bins^2) scalar algebra in FP64; every per-mode and per-cell sum
+runs on the GPU.
+"""
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+import torch
+
+from . import _lib, angular, engine
+
+
+def _precision(stat_attrs, kwargs):
+    p = kwargs.get("precision", stat_attrs.get("precision", "f64"))
+    if p not in engine.PRECISION:
+        raise ValueError("precision must be 'f64' or 'f32'")
+    return p
+
+
+# ===================================================================== pk
+def calculate_power_spectrum_box(rfield_a, rfield_b, correlation_mode, stat_attrs, comm=None, **kwargs):
+    """Power-spectrum multipoles in a periodic box (clustering_estimator.py:566-746)."""
+    poles = stat_attrs["poles"]
+    boxsize, nmesh = np.array(stat_attrs["boxsize"]), np.array(stat_attrs["nmesh"])
+    k_min, k_max, k_bins = stat_attrs["k_min"], stat_attrs["k_max"], stat_attrs["k_bins"]
+    sampler, interlaced = stat_attrs["sampler"], stat_attrs["interlaced"]
+    rsd = np.array(stat_attrs["rsd"], dtype=np.float64)
+    P_shot = 1.0 / stat_attrs["NZ_a"] if correlation_mode == "auto" else 0.0
+    NZ_a = stat_attrs["NZ_a"]
+    NZ_b = stat_attrs["NZ_b"] if correlation_mode == "cross" else None
+    n = int(nmesh[0])
+    L = float(boxsize[0])
+
+    k_edge = np.linspace(k_min, k_max, k_bins + 1)
+    comp = _lib.COMP_SINC if interlaced else _lib.COMP_SHOTNOISE
+    # r2c + compensation, zero mode cleared (ce:599-636)
+    ca = engine.finish_delta(rfield_a, 1.0, comp, 0.0)
+    cb = engine.finish_delta(rfield_b, 1.0, comp, 0.0) if correlation_mode == "cross" else ca
+    prec = rfield_a.precision
+    code = engine.PRECISION[prec][0]
+
+    counts, ksum = engine.kbin_counts(n, L, k_edge)
+    even = [p for p in poles if not p & 1]
+    sums = None
+    if even:
+        ctx = _lib.Context.get()
+        dsum = torch.empty((len(even), k_bins), dtype=torch.float64, device=ca.device)
+        ctx.pk_bins(code, n, L, ca, cb, k_edge, even, rsd, dsum)
+        sums = dsum.cpu().numpy()
+    k_num = counts.cpu().numpy()
+    k_eff = ksum.cpu().numpy() / k_num
+    results = {"k_eff": k_eff, "k_num": k_num}
+    for pole in poles:
+        if pole & 1:
+            res = np.zeros(k_bins).astype("float128")
+        else:
+            res = sums[even.index(pole)] / k_num
+            if correlation_mode == "auto":
+                res *= boxsize.prod() ** (-1) * (nmesh.prod() ** 2) / NZ_a ** 2
+            else:
+                res *= boxsize.prod() ** (-1) * nmesh.prod() ** 2 / (NZ_a * NZ_b)
+            if pole == 0:
+                res -= P_shot
+            else:
+                res *= 2 * pole + 1
+        results.update({"P%d" % pole: res, "P_shot": P_shot})
+    return results
+
+
+# ================================================================ bk_sugi
+def _legs_for_signal(l1, l2, m1, m2, correlation_mode, tracer_type):
+    """Which fields feed the two shell legs (clustering_estimator.py:898-970)."""
+    leg1 = (l1, m1, 0, False)
+    same_tracer = correlation_mode == "auto" or tracer_type == "aab"
+    if same_tracer and l1 == l2 and m1 == m2:
+        return engine.PairSpec(leg1, "eq")
+    if same_tracer and l1 == l2 and m1 == -m2:
+        return engine.PairSpec(leg1, "conj", sign=(-1.0) ** (m1 + l1))
+    src2 = 0 if tracer_type in ("aaa", "aab") else 1
+    return engine.PairSpec(leg1, "leg", (l2, m2, src2, False))
+
+
+def _legs_for_s3fft(l1, l2, m1, m2):
+    """Shell legs of the FFT S3 term: conj(Y) on a unit spectrum (ce:1215-1219)."""
+    leg1 = (l1, m1, 2, True)
+    if l1 == l2 and m1 == m2:
+        return engine.PairSpec(leg1, "eq")
+    if l1 == l2 and m1 == -m2:
+        return engine.PairSpec(leg1, "conj", sign=(-1.0) ** (m1 + l1))
+    return engine.PairSpec(leg1, "leg", (l2, m2, 2, True))
+
+
+def _plan_blocks(specs, k_bins, n, precision, requested, diagonal):
+    """Bin block size and shell-field capacity for one pair_sums call.
+
+    ``requested`` is the reference's block_size (ce:867-879): "full"/None means all
+    bins at once.  The block shrinks further if the fields do not fit in HBM.
+    """
+    if diagonal or requested == "full" or requested is None:
+        bs = k_bins
+    elif isinstance(requested, (int, np.integer)) and 1 <= requested <= k_bins:
+        bs = int(requested)
+    else:
+        raise ValueError("For full mode, block_size must be 1, 'full', or an integer in [1, k_bins].")
+    row_legs = {ps.leg1 for ps in specs}
+    col_legs = {ps.leg1 if ps.mode != "leg" else ps.leg2 for ps in specs}
+    comps = lambda legs: sum(len(engine.leg_components(l[0], l[1])) for l in legs)
+    union_pb = comps(row_legs | col_legs)
+    split_pb = comps(row_legs) + (comps(col_legs) if not diagonal else comps(col_legs - row_legs))
+
+    def need(b):
+        return union_pb * b if b == k_bins else split_pb * b
+
+    cap = engine.fields_capacity(n, precision, need(bs))
+    while bs > 1 and need(bs) > cap:
+        bs = (bs + 1) // 2
+    if need(bs) > cap:
+        raise MemoryError("not enough device memory for one block of shell fields")
+    return bs, need(bs)
+
+
+def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_attrs,
+                      precision="f64", block_size=None, shotnoise_ana_all_eff=True):
+    """Sugiyama bispectrum multipoles for several angular configurations of one
+    set of painted meshes, sharing the forward transforms, G, the shell fields and
+    the FFT shot-noise shells among configurations.
+
+    Returns one reference-format result dict per configuration.  Called with a
+    single configuration this is ``calculate_bk_sugi_box``.
+    """
+    data_vector_mode = stat_attrs.get("data_vector_mode", "diagonal")
+    shotnoise_mode = stat_attrs.get("shotnoise_mode", "ana")
+    diagonal = data_vector_mode == "diagonal"
+    if data_vector_mode not in ("diagonal", "full"):
+        raise ValueError("data_vector_mode must be either 'diagonal' or 'full'.")
+    boxsize = np.array(stat_attrs["boxsize"])
+    nmesh = np.array(stat_attrs["nmesh"])
+    k_min, k_max, k_bins = stat_attrs["k_min"], stat_attrs["k_max"], stat_attrs["k_bins"]
+    sampler = stat_attrs["sampler"]
+    n = int(nmesh[0])
+    L = float(boxsize[0])
+    V = boxsize.prod()
+    N3 = nmesh.prod()
+    vol_per_cell = V / N3
+    window = _lib.WINDOW[sampler]
+
+    letters = ["a"] + (["b"] if correlation_mode == "cross" else []) + (["c"] if tracer_type == "abc" else [])
+    NZ = {t: stat_attrs["NZ_" + t] for t in letters}
+    N_gal = {t: stat_attrs["N_gal_" + t] for t in letters}
+
+    k_edge = np.linspace(k_min, k_max, k_bins + 1)
+    # overdensity spectra: r2c(rho/dV - NZ), compensated (ce:808-837)
+    spec = {}
+    for t in letters:
+        m = meshes[t]
+        k0 = (m.sum_w / float(N3)) / vol_per_cell - NZ[t]
+        spec[t] = engine.finish_delta(m, 1.0 / vol_per_cell, _lib.COMP_SINC, k0)
+
+    counts, ksum = engine.kbin_counts(n, L, k_edge)
+    k_num = counts.cpu().numpy()
+    k_eff = ksum.cpu().numpy() / k_num
+
+    g_letter = "a" if correlation_mode == "auto" else ("c" if tracer_type == "abc" else "b")
+    # G_00 = Re c2r(delta); only |k| < 2 k_max reaches the triple sums
+    G = engine.band_limited_field(n, L, spec[g_letter], 2.0 * k_max, precision)
+
+    # ---- signal: shell fields and pair sums for every magnetic sub-configuration
+    per_cfg = []
+    specs = []
+    for (l1, l2, L_) in angu_configs:
+        cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
+        entries = []
+        for ss, (m1, m2, _) in enumerate(cfgs):
+            ps = _legs_for_signal(l1, l2, m1, m2, correlation_mode, tracer_type)
+            entries.append((len(specs), (m1, m2), tj[ss]))
+            specs.append(ps)
+        per_cfg.append(entries)
+
+    spec_b = spec.get("b")
+    bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal)
+    sf = engine.ShellFields(n, L, k_edge, precision, spec["a"], spec_b, capacity=capacity)
+    sums = engine.pair_sums(G, sf, specs, k_bins, diagonal, bs)
+    del sf, G
+
+    # ---- k3 bins (ce:1063-1074)
+    k_center = 0.5 * (k_edge[1:] + k_edge[:-1])
+    k3_edge = np.linspace(2 * k_min, 2 * k_max, k_bins * 2 + 1)[:-1]
+    k3_center = 0.5 * (k3_edge[1:] + k3_edge[:-1])
+    k3_bins = len(k3_center)
+    c3, s3 = engine.kbin_counts(n, L, k3_edge)
+    k_num_k3 = c3.cpu().numpy()
+    k3_eff = s3.cpu().numpy() / k_num_k3
+
+    other = spec["a"] if correlation_mode == "auto" else spec["b"]
+    code = engine.PRECISION[precision][0]
+    ctx = _lib.Context.get()
+    need_fft = shotnoise_mode in ("fft", "both") and tracer_type not in ("abc", "abb")
+    src_field = None
+    results = []
+    sn_cache = {}
+    for ci, (l1, l2, L_) in enumerate(angu_configs):
+        N_ells = (2 * l1 + 1) * (2 * l2 + 1) * (2 * L_ + 1)
+        H_ells = angular.wigner3j(l1, l2, L_, 0, 0, 0)
+        cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
+        if diagonal:
+            total_res = np.zeros(k_bins).astype("complex128")
+        else:
+            total_res = np.zeros((k_bins, k_bins)).astype("complex128")
+        for (idx, (m1, m2), three_j) in per_cfg[ci]:
+            sub = three_j * sums[idx]
+            total_res += sub if (m1, m2) == (0, 0) else 2 * np.real(sub)
+
+        SN3_fft = None
+        if tracer_type == "abc":
+            SN0, SN1, SN2, SN3 = 0.0, 0.0, 0.0, 0.0
+        else:
+            SN0 = N_gal["a"] if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
+            key = (L_, SN0)
+            if key not in sn_cache:
+                d = torch.empty(2 * k3_bins, dtype=torch.float64, device=spec["a"].device)
+                yl0 = angular.harmonic(L_, 0, True) if L_ != 0 else None
+                ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                            float(SN0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d)
+                dd = d.cpu().numpy()
+                sn_cache[key] = dd[0::2] + 1j * dd[1::2]
+            total_sum = sn_cache[key]
+            SN1, SN2 = 0.0, 0.0
+            if l1 == L_ and l2 == 0:
+                if correlation_mode == "auto":
+                    SN1 = (total_sum / k_num_k3)[: len(k_center)]
+                    SN1 *= 2 * L_ + 1
+                    if l1 == 0:
+                        SN2 = SN1.copy()
+                elif correlation_mode == "cross" and tracer_type == "abb":
+                    SN1 = (total_sum / k_num_k3)[: len(k_center)]
+                    SN1 *= 2 * L_ + 1
+            if not diagonal:
+                SN1_full = np.zeros((k_bins, k_bins)).astype("c16")
+                SN2_full = np.zeros((k_bins, k_bins)).astype("c16")
+                if np.isscalar(SN1) or np.ndim(SN1) == 0:
+                    SN1_full[:] = SN1
+                else:
+                    for i in range(k_bins):
+                        SN1_full[i, :] = SN1[i]
+                if np.isscalar(SN2) or np.ndim(SN2) == 0:
+                    SN2_full[:] = SN2
+                else:
+                    for i in range(k_bins):
+                        SN2_full[:, i] = SN2[i]
+                SN1, SN2 = SN1_full, SN2_full
+
+            def s3_ana():
+                if tracer_type == "abb":
+                    return 0.0
+                weighted_k_num = k_num_k3 / k3_center
+                if diagonal:
+                    s3 = np.zeros(k_bins, dtype="complex128")
+                    for i in range(k_bins):
+                        if shotnoise_ana_all_eff:
+                            q = angular.q_ells_eff(i, i, k_eff, l1, l2, L_, k3_eff)
+                        else:
+                            q = _q_ells_center(i, i, k_center, k_min, k_max, k_bins, l1, l2, L_)
+                        numer = np.sum(q * total_sum / k3_center)
+                        denom = np.sum(weighted_k_num[: 2 * i + 1])
+                        if denom > 0:
+                            s3[i] = numer / denom
+                else:
+                    s3 = np.zeros((k_bins, k_bins), dtype="complex128")
+                    for i in range(k_bins):
+                        for j in range(k_bins):
+                            if shotnoise_ana_all_eff:
+                                q = angular.q_ells_eff(i, j, k_eff, l1, l2, L_, k3_eff)
+                            else:
+                                q = _q_ells_center(i, j, k_center, k_min, k_max, k_bins, l1, l2, L_)
+                            vb = angular.valid_k3_bins(k_center[i], k_center[j], k_min, k_max, k_bins)
+                            numer = np.sum(q * total_sum / k3_center)
+                            denom = np.sum(weighted_k_num * vb)
+                            if denom > 0:
+                                s3[i, j] = numer / denom
+                return s3 * (H_ells * N_ells)
+
+            def s3_fft():
+                nonlocal src_field
+                if tracer_type == "abb":
+                    return np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
+                sn0_src = float(N_gal["a"]) if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
+                skey = ("src", sn0_src)
+                if skey not in sn_cache:
+                    cdt = engine.PRECISION[precision][2]
+                    src_spec = torch.empty_like(spec["a"], dtype=cdt)
+                    d = torch.empty(2 * k3_bins, dtype=torch.float64, device=spec["a"].device)
+                    ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                                sn0_src if correlation_mode == "auto" else 0.0, window, None, k3_edge, d,
+                                source=src_spec, band=2.0 * k_max)
+                    rdt = engine.PRECISION[precision][1]
+                    fld = torch.empty(n * n * n, dtype=rdt, device=spec["a"].device)
+                    ctx.c2r(code, n, 1, src_spec, fld)
+                    del src_spec
+                    sn_cache[skey] = fld
+                src = sn_cache[skey]
+                sp = []
+                for (m1, m2, _) in cfgs:
+                    sp.append(_legs_for_s3fft(l1, l2, m1, m2))
+                bsf, capf = _plan_blocks(sp, k_bins, n, precision, block_size, diagonal)
+                sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
+                ss_list = engine.pair_sums(src, sfu, sp, k_bins, diagonal, bsf)
+                del sfu
+                s3 = np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
+                for ss, (m1, m2, _) in enumerate(cfgs):
+                    S = ss_list[ss]
+                    if diagonal:
+                        sub = np.zeros(k_bins, dtype="complex128")
+                        for i in range(k_bins):
+                            if k_num[i] > 0:
+                                sub[i] = tj[ss] * S[i] / (k_num[i] ** 2)
+                    else:
+                        sub = np.zeros((k_bins, k_bins), dtype="complex128")
+                        for i in range(k_bins):
+                            for j in range(k_bins):
+                                if k_num[i] > 0 and k_num[j] > 0:
+                                    sub[i, j] = tj[ss] * S[i, j] / (k_num[i] * k_num[j])
+                    s3 += sub if (m1, m2) == (0, 0) else 2.0 * np.real(sub)
+                s3 *= H_ells * N_ells
+                s3 *= 1 / nmesh.prod()
+                return s3
+
+            if shotnoise_mode == "ana":
+                SN3 = s3_ana()
+            elif shotnoise_mode == "fft":
+                SN3 = s3_fft()
+            elif shotnoise_mode == "both":
+                SN3 = s3_ana()
+                SN3_fft = s3_fft()
+            else:
+                raise ValueError("shotnoise_mode must be either 'ana', 'fft', or 'both'.")
+
+        # normalisation (ce:1495-1548)
+        if correlation_mode == "auto":
+            I_norm = (N_gal["a"] ** 3) / (V ** 2)
+        elif tracer_type == "aab":
+            I_norm = (N_gal["a"] ** 2 * N_gal["b"]) / (V ** 2)
+        elif tracer_type == "abb":
+            I_norm = (N_gal["a"] * N_gal["b"] ** 2) / (V ** 2)
+        else:
+            I_norm = (N_gal["a"] * N_gal["b"] * N_gal["c"]) / (V ** 2)
+        total_shot_noise = SN0 + SN1 + SN2 + SN3
+        total_res = total_res * (N_ells * H_ells / I_norm)
+        if not diagonal:
+            total_res *= V ** 2 / np.outer(k_num[:k_bins], k_num[:k_bins])
+        else:
+            total_res *= V ** 2 / (k_num[: len(total_res)]) ** 2
+        total_res *= vol_per_cell
+        total_shot_noise *= 1 / I_norm
+        final_bk = total_res - total_shot_noise
+        sn_terms = {"SN0": SN0 / I_norm, "SN1": SN1 / I_norm, "SN2": SN2 / I_norm, "SN3": SN3 / I_norm}
+        if shotnoise_mode == "both":
+            sn_terms["SN3_FFT"] = SN3_fft / I_norm
+        results.append({
+            "B_sugi": final_bk, "SN_terms": sn_terms, "I_norm": I_norm, "Shot_noise": total_shot_noise,
+            "Bk_raw": total_res, "k_eff": k_eff, "nmodes": k_num,
+        })
+    return results
+
+
+def _q_ells_center(i, j, k_center, k_min, k_max, k_bins, l1, l2, L):
+    """q_l with bin-centre wavenumbers (math_evaluator.py:560-589)."""
+    k3_edge = np.linspace(2 * k_min, 2 * k_max, k_bins * 2 + 1)[:-1]
+    k3_center = 0.5 * (k3_edge[1:] + k3_edge[:-1])
+    q = np.zeros(len(k3_center))
+    lmin = min(l1, l2)
+    k1, k2 = k_center[i], k_center[j]
+    for nn in range(-lmin, lmin + 1):
+        tj = angular.wigner3j(l1, l2, L, nn, -nn, 0)
+        a13 = np.zeros(len(k3_center))
+        a23 = np.zeros(len(k3_center))
+        for t, k3 in enumerate(k3_center):
+            if abs(k1 - k2) <= k3 <= (k1 + k2):
+                a13[t] = angular.assoc_legendre(l1, nn, (k3 ** 2 + k1 ** 2 - k2 ** 2) / (2 * k1 * k3))
+                a23[t] = angular.assoc_legendre(l2, -nn, (k3 ** 2 + k2 ** 2 - k1 ** 2) / (2 * k2 * k3))
+        a13 *= (-1) ** (l1 + nn)
+        a23 *= (-1) ** (l2 - nn)
+        q += (-1) ** nn * tj * a13 * a23
+    return q
+
+
+def calculate_bk_sugi_box(rfield_a, rfield_b, rfield_c, correlation_mode, stat_attrs, comm=None, **kwargs):
+    """Sugiyama bispectrum multipole in a periodic box (clustering_estimator.py:749-1555)."""
+    precision = _precision(stat_attrs, kwargs)
+    tracer_type = stat_attrs["tracer_type"]
+    meshes = {"a": rfield_a}
+    if correlation_mode == "cross":
+        meshes["b"] = rfield_b
+        if tracer_type == "abc":
+            meshes["c"] = rfield_c
+    block_size = stat_attrs.get("block_size", 1 if stat_attrs.get("data_vector_mode", "diagonal") == "diagonal" else "full")
+    res = bk_sugi_box_multi(meshes, correlation_mode, tracer_type, [tuple(stat_attrs["angu_config"])], stat_attrs,
+                            precision=precision, block_size=block_size,
+                            shotnoise_ana_all_eff=kwargs.get("shotnoise_ana_all_eff", True))
+    logging.getLogger(__name__).info("bk_sugi box finished")
+    return res[0]

@@ -1,0 +1,153 @@
+// Context, error reporting and cuFFT plan cache.
+#include <cstdio>
+#include <stdexcept>
+
+#include "internal.h"
+
+namespace cnpc {
+
+int fail(cnpc_ctx *ctx, int status, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    return status;
+}
+
+int check_cuda(cnpc_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return CNPC_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(ctx, CNPC_ENOMEM, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    return fail(ctx, CNPC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int check_launch(cnpc_ctx *ctx, const char *what) {
+    return check_cuda(ctx, cudaGetLastError(), what);
+}
+
+int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream) {
+    if (ctx->scratch_bytes >= bytes) return CNPC_OK;
+    if (ctx->scratch) {
+        // the previous scratch may still be read by work queued on `stream`
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return check_cuda(ctx, e, "scratch sync");
+        cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    size_t want = bytes < (size_t)(1 << 20) ? (size_t)(1 << 20) : bytes;
+    cudaError_t e = cudaMalloc(&ctx->scratch, want);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "scratch alloc");
+    ctx->scratch_bytes = want;
+    return CNPC_OK;
+}
+
+static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, cufftHandle *out) {
+    auto key = std::make_tuple((int)type, n, batch);
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end()) {
+        *out = it->second;
+        return CNPC_OK;
+    }
+    cufftHandle h;
+    int dims[3] = {n, n, n};
+    cufftResult r = cufftPlanMany(&h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch);
+    if (r != CUFFT_SUCCESS) {
+        if (r == CUFFT_ALLOC_FAILED)
+            return fail(ctx, CNPC_ENOMEM, "cufftPlanMany: allocation failed");
+        return fail(ctx, CNPC_ECUFFT, "cufftPlanMany failed with code " + std::to_string((int)r));
+    }
+    ctx->plans[key] = h;
+    *out = h;
+    return CNPC_OK;
+}
+
+}  // namespace cnpc
+
+using namespace cnpc;
+
+extern "C" {
+
+int cnpc_version(void) { return 100; }
+
+const char *cnpc_status_string(int status) {
+    switch (status) {
+        case CNPC_OK: return "ok";
+        case CNPC_EINVAL: return "invalid argument";
+        case CNPC_ENOMEM: return "out of device memory";
+        case CNPC_ECUDA: return "CUDA error";
+        case CNPC_ECUFFT: return "cuFFT error";
+        case CNPC_ETIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+int cnpc_ctx_create(cnpc_ctx **ctx, int device) {
+    if (!ctx) return CNPC_EINVAL;
+    *ctx = nullptr;
+    cnpc_ctx *c = new (std::nothrow) cnpc_ctx();
+    if (!c) return CNPC_ENOMEM;
+    c->device = device;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        delete c;
+        return CNPC_ECUDA;
+    }
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return CNPC_ECUDA;
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+        c->num_sms = sms;
+    *ctx = c;
+    return CNPC_OK;
+}
+
+int cnpc_ctx_destroy(cnpc_ctx *ctx) {
+    if (!ctx) return CNPC_OK;
+    for (auto &kv : ctx->plans) cufftDestroy(kv.second);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    delete ctx;
+    return CNPC_OK;
+}
+
+const char *cnpc_ctx_last_error(cnpc_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real, void *d_spec,
+                 cnpc_stream_t stream) {
+    CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
+    CNPC_REQUIRE(ctx, batch >= 1, "batch must be >= 1");
+    CNPC_REQUIRE(ctx, d_real && d_spec, "null buffer");
+    CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
+    cufftHandle h;
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_R2C : CUFFT_D2Z, n, batch, &h);
+    if (st) return st;
+    cufftSetStream(h, (cudaStream_t)stream);
+    cufftResult r = dtype == CNPC_F32
+                        ? cufftExecR2C(h, (cufftReal *)d_real, (cufftComplex *)d_spec)
+                        : cufftExecD2Z(h, (cufftDoubleReal *)d_real, (cufftDoubleComplex *)d_spec);
+    if (r != CUFFT_SUCCESS) return fail(ctx, CNPC_ECUFFT, "cufftExec r2c failed " + std::to_string((int)r));
+    return CNPC_OK;
+}
+
+int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec, void *d_real,
+                 cnpc_stream_t stream) {
+    CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
+    CNPC_REQUIRE(ctx, batch >= 1, "batch must be >= 1");
+    CNPC_REQUIRE(ctx, d_real && d_spec, "null buffer");
+    CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
+    cufftHandle h;
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_C2R : CUFFT_Z2D, n, batch, &h);
+    if (st) return st;
+    cufftSetStream(h, (cudaStream_t)stream);
+    cufftResult r = dtype == CNPC_F32
+                        ? cufftExecC2R(h, (cufftComplex *)d_spec, (cufftReal *)d_real)
+                        : cufftExecZ2D(h, (cufftDoubleComplex *)d_spec, (cufftDoubleReal *)d_real);
+    if (r != CUFFT_SUCCESS) return fail(ctx, CNPC_ECUFFT, "cufftExec c2r failed " + std::to_string((int)r));
+    return CNPC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Internal (host-side) declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "cosmonpc_b200.h"
+
+struct cnpc_ctx {
+    int device = 0;
+    std::string last_error;
+    // cuFFT plans keyed by (type, n, batch)
+    std::map<std::tuple<int, int, int>, cufftHandle> plans;
+    // scratch for per-block partial sums of the x-space reductions
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int num_sms = 148;
+};
+
+namespace cnpc {
+
+int fail(cnpc_ctx *ctx, int status, const std::string &msg);
+int check_cuda(cnpc_ctx *ctx, cudaError_t e, const char *what);
+int check_launch(cnpc_ctx *ctx, const char *what);
+int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream);
+
+}  // namespace cnpc
+
+#define CNPC_REQUIRE(ctx, cond, msg)                                  \
+    do {                                                              \
+        if (!(cond)) return ::cnpc::fail((ctx), CNPC_EINVAL, (msg));  \
+    } while (0)
+
+#define CNPC_GUARD_BEGIN try {
+#define CNPC_GUARD_END(ctx)                                                       \
+    }                                                                             \
+    catch (const std::exception &ex) {                                            \
+        return ::cnpc::fail((ctx), CNPC_EINVAL, std::string("exception: ") + ex.what()); \
+    }                                                                             \
+    catch (...) {                                                                 \
+        return ::cnpc::fail((ctx), CNPC_EINVAL, "unknown exception");             \
+    }

@@ -1,0 +1,442 @@
+// k-space stages: forward finish (interlace + compensation), mode counts,
+// shell sums for pk and the bk shot-noise terms, and shell-spectrum synthesis.
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace cnpc {
+
+struct EdgeSet {
+    int n;
+    double e[CNPC_MAX_EDGES];
+};
+struct HarmTable {
+    int n;
+    cnpc_harmonic h[CNPC_MAX_HARMONICS];
+};
+struct ItemTable {
+    int n;
+    cnpc_shell_item it[CNPC_MAX_ITEMS];
+};
+
+static int grid_for(cnpc_ctx *ctx, int64_t work, int threads, int per_sm = 8) {
+    int64_t want = (work + threads - 1) / threads;
+    int64_t cap = (int64_t)ctx->num_sms * per_sm;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+// Sum v into bins s[bin] over the lanes of a warp (all 32 lanes must call;
+// bin < 0 means "no contribution").
+__device__ inline void warp_bin_add(double *s, int bin, double v) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned active = __ballot_sync(full, bin >= 0);
+    while (active) {
+        const int leader = __ffs(active) - 1;
+        const int b = __shfl_sync(full, bin, leader);
+        const unsigned same = __ballot_sync(full, bin == b);
+        double x = (bin == b) ? v : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(full, x, o);
+        if (lane == leader) atomicAdd(&s[b], x);
+        active &= ~same;
+    }
+}
+
+// ---------------------------------------------------------------- forward
+template <typename T>
+__global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int n, double L,
+                                      double inv_n3, double scale, int comp, int p, double k0,
+                                      double band, int64_t nh) {
+    const double H = L / n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
+        Mode m = mode_of(t, n);
+        double kx, ky, kz;
+        const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+        double re = (double)spec[t].x * inv_n3, im = (double)spec[t].y * inv_n3;
+        if (spec2) {
+            const double ph = 0.5 * ((kx * H + ky * H) + kz * H);
+            double sp, cp;
+            sincos(ph, &sp, &cp);
+            const double r2 = (double)spec2[t].x * inv_n3, i2 = (double)spec2[t].y * inv_n3;
+            re = 0.5 * re + 0.5 * (r2 * cp - i2 * sp);
+            im = 0.5 * im + 0.5 * (r2 * sp + i2 * cp);
+        }
+        const double f = scale * comp_factor(comp, p, kx * H, ky * H, kz * H);
+        re *= f;
+        im *= f;
+        if (t == 0) {
+            re = k0;
+            im = 0.0;
+        }
+        if (band > 0.0 && kn >= band) re = im = 0.0;
+        spec[t] = mk<T>((T)re, (T)im);
+    }
+}
+
+// ------------------------------------------------------------ mode counts
+__global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *counts, double *ksum,
+                                   int64_t nh) {
+    extern __shared__ double sm[];
+    const int nb = edges.n - 1;
+    for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) sm[i] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+         base += wstride) {
+        const int64_t t = base + lane;
+        int bin = -1;
+        double kn = 0.0, mult = 0.0;
+        if (t < nh) {
+            Mode m = mode_of(t, n);
+            double kx, ky, kz;
+            kn = knorm_exact(m, L, &kx, &ky, &kz);
+            bin = find_bin(kn, edges.e, edges.n);
+            mult = m.mult;
+        }
+        warp_bin_add(sm, bin, mult);
+        warp_bin_add(sm + nb, bin, mult * kn);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        if (sm[i] != 0.0) atomicAdd(&counts[i], sm[i]);
+        if (sm[nb + i] != 0.0) atomicAdd(&ksum[i], sm[nb + i]);
+    }
+}
+
+// --------------------------------------------------------------- pk sums
+struct PoleSet {
+    int n;
+    int l[CNPC_MAX_POLES];
+    double los[3];
+};
+
+template <typename T>
+__global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, EdgeSet edges,
+                               PoleSet poles, double *sums, int64_t nh) {
+    extern __shared__ double sm[];
+    const int nb = edges.n - 1;
+    for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x) sm[i] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+         base += wstride) {
+        const int64_t t = base + lane;
+        int bin = -1;
+        double pv = 0.0, mu = 0.0;
+        if (t < nh) {
+            Mode m = mode_of(t, n);
+            double kx, ky, kz;
+            const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+            bin = find_bin(kn, edges.e, edges.n);
+            if (bin >= 0) {
+                const cpx_t<T> va = a[t], vb = b[t];
+                pv = m.mult * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+                if (kn > 0.0)
+                    mu = (kx / kn) * poles.los[0] + (ky / kn) * poles.los[1] + (kz / kn) * poles.los[2];
+            }
+        }
+        for (int q = 0; q < poles.n; ++q) {
+            // Legendre P_l(mu) by the three-term recurrence
+            const int l = poles.l[q];
+            double p0 = 1.0, p1 = mu;
+            double pl = (l == 0) ? 1.0 : mu;
+            for (int j = 1; j < l; ++j) {
+                pl = ((2 * j + 1) * mu * p1 - j * p0) / (j + 1);
+                p0 = p1;
+                p1 = pl;
+            }
+            warp_bin_add(sm + q * nb, bin, pv * pl);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x)
+        if (sm[i] != 0.0) atomicAdd(&sums[i], sm[i]);
+}
+
+// ------------------------------------------------------- shot-noise sums
+template <typename T>
+__global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, double vsq,
+                               double sn0, int p, int use_y, cnpc_harmonic yl0, EdgeSet edges,
+                               double *sums, cpx_t<T> *source, double band, int64_t nh) {
+    extern __shared__ double sm[];
+    const int nb = edges.n - 1;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) sm[i] = 0.0;
+    __syncthreads();
+    const double H = L / n;
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+         base += wstride) {
+        const int64_t t = base + lane;
+        int bin = -1;
+        double val = 0.0;
+        if (t < nh) {
+            Mode m = mode_of(t, n);
+            double kx, ky, kz;
+            const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+            const cpx_t<T> va = a[t], vb = b[t];
+            double pr = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+            const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
+            if (sn0 != 0.0) pr -= sn0 * comp_factor(CNPC_COMP_BKNOISE, p, kx * H, ky * H, kz * H);
+            if (source) {
+                const bool keep = !(band > 0.0) || kn < band;
+                source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+            }
+            bin = find_bin(kn, edges.e, edges.n);
+            if (bin >= 0) {
+                double y = 1.0;
+                if (use_y) {
+                    const bool origin = kn == 0.0;
+                    const double ik = origin ? 0.0 : 1.0 / kn;
+                    y = harmonic_eval<double>(yl0, kx * ik, ky * ik, kz * ik, origin).x;
+                }
+                val = m.mult * pr * y;
+            }
+        }
+        warp_bin_add(sm, bin, val);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        if (sm[i] != 0.0) atomicAdd(&sums[2 * i], sm[i]);
+}
+
+// --------------------------------------------------------- shell spectra
+template <typename T>
+__global__ void shell_spectra_kernel(const cpx_t<T> *A, const cpx_t<T> *B, int n, double L,
+                                     EdgeSet edges, HarmTable harm, ItemTable items,
+                                     cpx_t<T> *out, int64_t nh) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const cpx_t<T> zero = mk<T>((T)0, (T)0);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
+        Mode m = mode_of(t, n);
+        double kx, ky, kz;
+        const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+        const int bin = find_bin(kn, edges.e, edges.n);
+        if (bin < 0) {
+            for (int j = 0; j < items.n; ++j) out[(int64_t)j * nh + t] = zero;
+            continue;
+        }
+        const bool origin = kn == 0.0;
+        const double ik = origin ? 0.0 : 1.0 / kn;
+        const T x = (T)(kx * ik), y = (T)(ky * ik), z = (T)(kz * ik);
+        for (int j = 0; j < items.n; ++j) {
+            const cnpc_shell_item it = items.it[j];
+            cpx_t<T> v = zero;
+            if (it.bin == bin) {
+                const cnpc_harmonic &h = harm.h[it.harmonic];
+                cpx_t<T> Y = harmonic_eval<T>(h, x, y, z, origin);
+                if (it.conj) Y.y = -Y.y;
+                // phi = Re Y / Im Y (even l) or i Im Y / -i Re Y (odd l)
+                cpx_t<T> phi;
+                if ((h.l & 1) == 0)
+                    phi = it.component == 0 ? mk<T>(Y.x, (T)0) : mk<T>(Y.y, (T)0);
+                else
+                    phi = it.component == 0 ? mk<T>((T)0, Y.y) : mk<T>((T)0, -Y.x);
+                cpx_t<T> s;
+                if (it.source == 0)
+                    s = A[t];
+                else if (it.source == 1)
+                    s = B[t];
+                else
+                    s = mk<T>((T)1, (T)0);
+                v = mk<T>(s.x * phi.x - s.y * phi.y, s.x * phi.y + s.y * phi.x);
+            }
+            out[(int64_t)j * nh + t] = v;
+        }
+    }
+}
+
+static int load_edges(cnpc_ctx *ctx, const double *h_edges, int nedges, EdgeSet *es) {
+    CNPC_REQUIRE(ctx, h_edges != nullptr, "null edges");
+    CNPC_REQUIRE(ctx, nedges >= 2 && nedges <= CNPC_MAX_EDGES, "nedges out of range (2..257)");
+    for (int i = 0; i + 1 < nedges; ++i)
+        CNPC_REQUIRE(ctx, h_edges[i] < h_edges[i + 1], "edges must be increasing");
+    es->n = nedges;
+    std::memcpy(es->e, h_edges, sizeof(double) * nedges);
+    return CNPC_OK;
+}
+
+static int check_common(cnpc_ctx *ctx, int dtype, int n, double boxsize) {
+    CNPC_REQUIRE(ctx, ctx != nullptr, "null context");
+    CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
+    CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
+    CNPC_REQUIRE(ctx, boxsize > 0.0, "boxsize must be positive");
+    return CNPC_OK;
+}
+
+static inline int64_t half_modes(int n) { return (int64_t)n * n * (n / 2 + 1); }
+
+}  // namespace cnpc
+
+using namespace cnpc;
+
+extern "C" {
+
+int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
+                        const void *d_spec2, double scale, int comp, int window, double k0_value,
+                        double band_kmax, cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_spec != nullptr, "null spectrum");
+    CNPC_REQUIRE(ctx, comp >= 0 && comp <= 3, "bad compensation kind");
+    CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
+    const int64_t nh = half_modes(n);
+    const double inv_n3 = 1.0 / ((double)n * n * n);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int threads = 256;
+    const int blocks = grid_for(ctx, nh, threads);
+    if (dtype == CNPC_F32)
+        forward_finish_kernel<float><<<blocks, threads, 0, s>>>(
+            (float2 *)d_spec, (const float2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
+            k0_value, band_kmax, nh);
+    else
+        forward_finish_kernel<double><<<blocks, threads, 0, s>>>(
+            (double2 *)d_spec, (const double2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
+            k0_value, band_kmax, nh);
+    return check_launch(ctx, "forward_finish_kernel");
+}
+
+int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges, int nedges,
+                     double *d_counts, double *d_ksum, cnpc_stream_t stream) {
+    int st = check_common(ctx, CNPC_F64, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_counts && d_ksum, "null output");
+    EdgeSet es;
+    st = load_edges(ctx, h_edges, nedges, &es);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = nedges - 1;
+    st = check_cuda(ctx, cudaMemsetAsync(d_counts, 0, sizeof(double) * nb, s), "memset");
+    if (st) return st;
+    st = check_cuda(ctx, cudaMemsetAsync(d_ksum, 0, sizeof(double) * nb, s), "memset");
+    if (st) return st;
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, 2 * nb * sizeof(double), s>>>(
+        n, boxsize, es, d_counts, d_ksum, nh);
+    return check_launch(ctx, "kbin_counts_kernel");
+}
+
+int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                 const void *d_spec_b, const double *h_edges, int nedges, const int *h_poles,
+                 int npoles, const double *h_los, double *d_sums, cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_spec_a && d_spec_b && d_sums && h_poles && h_los, "null argument");
+    CNPC_REQUIRE(ctx, npoles >= 1 && npoles <= CNPC_MAX_POLES, "npoles out of range (1..8)");
+    EdgeSet es;
+    st = load_edges(ctx, h_edges, nedges, &es);
+    if (st) return st;
+    PoleSet ps;
+    ps.n = npoles;
+    for (int i = 0; i < npoles; ++i) {
+        CNPC_REQUIRE(ctx, h_poles[i] >= 0 && h_poles[i] <= 16, "pole out of range (0..16)");
+        ps.l[i] = h_poles[i];
+    }
+    for (int d = 0; d < 3; ++d) ps.los[d] = h_los[d];
+    const int nb = nedges - 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * nb * npoles, s), "memset");
+    if (st) return st;
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    const size_t smem = sizeof(double) * nb * npoles;
+    if (dtype == CNPC_F32)
+        pk_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ps, d_sums, nh);
+    else
+        pk_bins_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ps, d_sums, nh);
+    return check_launch(ctx, "pk_bins_kernel");
+}
+
+int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                 const void *d_spec_b, double volume_sq, double sn0, int window,
+                 const cnpc_harmonic *h_yl0, const double *h_edges, int nedges, double *d_sums,
+                 void *d_source, double band_kmax, cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_spec_a && d_spec_b && d_sums, "null argument");
+    CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
+    EdgeSet es;
+    st = load_edges(ctx, h_edges, nedges, &es);
+    if (st) return st;
+    cnpc_harmonic y;
+    std::memset(&y, 0, sizeof(y));
+    if (h_yl0) {
+        y = *h_yl0;
+        CNPC_REQUIRE(ctx, y.l >= 0 && y.l <= 8 && y.m == 0, "Y_L0 harmonic expected");
+    }
+    const int nb = nedges - 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nb, s), "memset");
+    if (st) return st;
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    const size_t smem = sizeof(double) * nb;
+    if (dtype == CNPC_F32)
+        sn_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, volume_sq, sn0, window,
+            h_yl0 ? 1 : 0, y, es, d_sums, (float2 *)d_source, band_kmax, nh);
+    else
+        sn_bins_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, volume_sq, sn0,
+            window, h_yl0 ? 1 : 0, y, es, d_sums, (double2 *)d_source, band_kmax, nh);
+    return check_launch(ctx, "sn_bins_kernel");
+}
+
+int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                       const void *d_spec_b, const double *h_edges, int nedges,
+                       const cnpc_harmonic *h_harmonics, int nharmonics,
+                       const cnpc_shell_item *h_items, int nitems, void *d_out,
+                       cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_out != nullptr, "null output");
+    CNPC_REQUIRE(ctx, nitems >= 1 && nitems <= CNPC_MAX_ITEMS, "nitems out of range (1..256)");
+    CNPC_REQUIRE(ctx, nharmonics >= 1 && nharmonics <= CNPC_MAX_HARMONICS, "nharmonics out of range");
+    CNPC_REQUIRE(ctx, h_harmonics && h_items, "null table");
+    EdgeSet es;
+    st = load_edges(ctx, h_edges, nedges, &es);
+    if (st) return st;
+    HarmTable ht;
+    ht.n = nharmonics;
+    for (int i = 0; i < nharmonics; ++i) {
+        const cnpc_harmonic &h = h_harmonics[i];
+        CNPC_REQUIRE(ctx, h.l >= 0 && h.l <= 8 && h.m >= -h.l && h.m <= h.l, "bad harmonic (l<=8, |m|<=l)");
+        ht.h[i] = h;
+    }
+    ItemTable itab;
+    itab.n = nitems;
+    for (int j = 0; j < nitems; ++j) {
+        const cnpc_shell_item &it = h_items[j];
+        CNPC_REQUIRE(ctx, it.bin >= 0 && it.bin < nedges - 1, "item bin out of range");
+        CNPC_REQUIRE(ctx, it.harmonic >= 0 && it.harmonic < nharmonics, "item harmonic out of range");
+        CNPC_REQUIRE(ctx, it.component == 0 || it.component == 1, "item component must be 0/1");
+        CNPC_REQUIRE(ctx, it.source >= 0 && it.source <= 2, "item source must be 0..2");
+        CNPC_REQUIRE(ctx, it.source != 0 || d_spec_a, "item needs spectrum A");
+        CNPC_REQUIRE(ctx, it.source != 1 || d_spec_b, "item needs spectrum B");
+        itab.it[j] = it;
+    }
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == CNPC_F32)
+        shell_spectra_kernel<float><<<grid_for(ctx, nh, threads), threads, 0, s>>>(
+            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ht, itab,
+            (float2 *)d_out, nh);
+    else
+        shell_spectra_kernel<double><<<grid_for(ctx, nh, threads), threads, 0, s>>>(
+            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ht, itab,
+            (double2 *)d_out, nh);
+    return check_launch(ctx, "shell_spectra_kernel");
+}
+
+}  // extern "C"

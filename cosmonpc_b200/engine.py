@@ -1,0 +1,299 @@
+"""Device pipeline: meshes, spectra, shell fields and x-space contractions.
+
+Every numeric step runs in libcosmonpc_b200.so kernels or cuFFT; torch only
+allocates device memory and provides the stream.  Two precisions:
+
+* ``"f64"`` -- the plain drop-in: float64 meshes, Z2D/D2Z transforms, FP64
+  shell fields and FP64 contractions.
+* ``"f32"`` -- the fast form: float32 meshes and shell fields (C2R/R2C),
+  FP64 mode sums and FP64 accumulation of the x-space contractions.
+
+Layout (see include/cosmonpc_b200.h): real meshes n^3 (z fastest), spectra
+n x n x (n/2+1) complex (cuFFT R2C layout).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib, angular
+
+PRECISION = {
+    "f32": (_lib.F32, torch.float32, torch.complex64),
+    "f64": (_lib.F64, torch.float64, torch.complex128),
+}
+
+
+def _device():
+    if not torch.cuda.is_available():
+        raise RuntimeError("cosmonpc_b200 needs a CUDA device; none is available")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+class PaintedMesh:
+    """Unnormalised R2C spectra of one painted catalog (and its +1/2-cell twin).
+
+    Stands in for the reference's painted ``RealField`` (mesh_generator.py:172-224):
+    the interlaced combination is applied when an estimator finishes the forward
+    transform, fused with its scaling and compensation.
+    """
+
+    def __init__(self, raw, n, boxsize, sampler, interlaced, n_gal, sum_w, precision):
+        self.raw = raw
+        self.n = n
+        self.boxsize = float(boxsize)
+        self.sampler = sampler
+        self.window = _lib.WINDOW[sampler]
+        self.interlaced = bool(interlaced)
+        self.N_gal = n_gal
+        self.sum_w = sum_w
+        self.precision = precision
+        self.used = False
+
+
+def paint(pos, weight, n, boxsize, sampler, interlaced, precision="f64", sum_w=None):
+    """Paint a catalog held on the device and return its forward spectra."""
+    ctx = _lib.Context.get()
+    code, rdt, cdt = PRECISION[precision]
+    dev = _device()
+    pos = pos.to(device=dev, dtype=torch.float64).contiguous()
+    if weight is not None:
+        weight = weight.to(device=dev, dtype=torch.float64).contiguous()
+    nb = 2 if interlaced else 1
+    mesh = torch.empty((nb, n, n, n), dtype=rdt, device=dev)
+    ctx.paint(code, pos, weight, n, float(boxsize), _lib.WINDOW[sampler], mesh[0],
+              mesh[1] if interlaced else None)
+    spec = torch.empty((nb, n, n, n // 2 + 1), dtype=cdt, device=dev)
+    ctx.r2c(code, n, nb, mesh, spec)
+    del mesh
+    if sum_w is None:
+        sum_w = float(pos.shape[0]) if weight is None else float(weight.sum().item())
+    return PaintedMesh(spec, n, boxsize, sampler, interlaced, int(pos.shape[0]), sum_w, precision)
+
+
+def finish_delta(pm, scale, comp, k0, band=0.0):
+    """Interlace-combine, scale and compensate in place; returns the spectrum view.
+
+    A PaintedMesh is consumed by one estimator (as the reference's rfield is
+    overwritten in place, clustering_estimator.py:808)."""
+    if pm.used:
+        raise ValueError("painted mesh already consumed by an estimator")
+    pm.used = True
+    ctx = _lib.Context.get()
+    code = PRECISION[pm.precision][0]
+    spec2 = pm.raw[1] if pm.interlaced else None
+    ctx.forward_finish(code, pm.n, pm.boxsize, pm.raw[0], spec2, float(scale), comp, pm.window,
+                       float(k0), band)
+    return pm.raw[0]
+
+
+def kbin_counts(n, boxsize, edges):
+    ctx = _lib.Context.get()
+    dev = _device()
+    nb = len(edges) - 1
+    counts = torch.empty(nb, dtype=torch.float64, device=dev)
+    ksum = torch.empty(nb, dtype=torch.float64, device=dev)
+    ctx.kbin_counts(n, float(boxsize), edges, counts, ksum)
+    return counts, ksum
+
+
+# ------------------------------------------------------------ shell fields
+def leg_components(l, m):
+    """Real component fields of the complex shell field of Y_lm (see header)."""
+    if m == 0:
+        return (0,) if l % 2 == 0 else (1,)
+    return (0, 1)
+
+
+class ShellFields:
+    """Real shell fields c2r(src * Y_lm * mask_bin) synthesised in FFT batches.
+
+    A leg is (l, m, source, conj) with source 0 (spectrum A), 1 (spectrum B) or
+    2 (unit spectrum).  Fields are stored as rows of one [capacity, n^3] tensor.
+    """
+
+    def __init__(self, n, boxsize, edges, precision, spec_a, spec_b, capacity, fft_batch=8,
+                 racah=True):
+        self.n = n
+        self.boxsize = float(boxsize)
+        self.edges = np.asarray(edges, dtype=np.float64)
+        self.precision = precision
+        self.code, self.rdt, self.cdt = PRECISION[precision]
+        self.spec_a = spec_a
+        self.spec_b = spec_b
+        self.racah = racah
+        dev = _device()
+        self.capacity = int(capacity)
+        self.fields = torch.empty((self.capacity, n * n * n), dtype=self.rdt, device=dev)
+        self.fft_batch = max(1, min(int(fft_batch), self.capacity))
+        self.scratch = torch.empty((self.fft_batch, n, n, n // 2 + 1), dtype=self.cdt, device=dev)
+        self.slot = {}
+        self.free = list(range(self.capacity))[::-1]
+
+    def key(self, leg, b, comp):
+        return (tuple(leg), int(b), int(comp))
+
+    def release_all(self):
+        self.slot.clear()
+        self.free = list(range(self.capacity))[::-1]
+
+    def release(self, keys):
+        for k in keys:
+            s = self.slot.pop(k, None)
+            if s is not None:
+                self.free.append(s)
+
+    def ensure(self, keys):
+        """Synthesise every (leg, bin, comp) in ``keys`` not yet resident."""
+        ctx = _lib.Context.get()
+        todo = [k for k in dict.fromkeys(keys) if k not in self.slot]
+        if len(todo) > len(self.free):
+            raise MemoryError("shell-field cache too small for this block")
+        harm_index = {}
+        harmonics = []
+        for i in range(0, len(todo), self.fft_batch):
+            batch = todo[i:i + self.fft_batch]
+            items = []
+            for (leg, b, comp) in batch:
+                l, m, src, conj = leg
+                hk = (l, m)
+                if hk not in harm_index:
+                    harm_index[hk] = len(harmonics)
+                    harmonics.append(angular.harmonic(l, m, self.racah))
+                items.append(_lib.ShellItem(b, harm_index[hk], comp, src, 1 if conj else 0))
+            ctx.shell_spectra(self.code, self.n, self.boxsize, self.spec_a, self.spec_b, self.edges,
+                              harmonics, items, self.scratch)
+            slots = [self.free.pop() for _ in batch]
+            # contiguous slots let one batched c2r write every field of the batch
+            if slots == list(range(slots[0], slots[0] + len(slots))):
+                ctx.c2r(self.code, self.n, len(batch), self.scratch, self.fields[slots[0]:slots[0] + len(slots)])
+            else:
+                for j, s in enumerate(slots):
+                    ctx.c2r(self.code, self.n, 1, self.scratch[j], self.fields[s])
+            for k, s in zip(batch, slots):
+                self.slot[k] = s
+
+
+def band_limited_field(n, boxsize, spec, kmax_band, precision, racah=True):
+    """Real field c2r(spec * 1[|k| < kmax_band]) (a copy; spec is left intact)."""
+    sf = ShellFields(n, boxsize, [0.0, float(kmax_band)], precision, spec, None, capacity=1, fft_batch=1)
+    sf.ensure([sf.key((0, 0, 0, False), 0, 0)])
+    out = sf.fields[0]
+    del sf.scratch
+    return out
+
+
+def contract(G, sf, rows, cols):
+    """T[i, j] = sum_x G F_rows[i] F_cols[j] (FP64 host array)."""
+    ctx = _lib.Context.get()
+    ncell = sf.n ** 3
+    T = np.zeros((len(rows), len(cols)))
+    if not rows or not cols:
+        return T
+    ridx = [sf.slot[k] for k in rows]
+    cidx = [sf.slot[k] for k in cols]
+    dev = _device()
+    for r0 in range(0, len(ridx), 128):
+        for c0 in range(0, len(cidx), 128):
+            rr = ridx[r0:r0 + 128]
+            cc = cidx[c0:c0 + 128]
+            out = torch.empty(len(rr) * len(cc), dtype=torch.float64, device=dev)
+            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
+            T[r0:r0 + len(rr), c0:c0 + len(cc)] = out.cpu().numpy().reshape(len(rr), len(cc))
+    return T
+
+
+# ---------------------------------------------------- pair-sum assembly
+class PairSpec:
+    """One magnetic sub-configuration's sum_x G F1_i F2_j.
+
+    mode "leg": F2 from its own leg; "eq": F2 = F1; "conj": F2 = sign * conj(F1).
+    """
+
+    def __init__(self, leg1, mode, leg2=None, sign=1.0):
+        self.leg1 = tuple(leg1)
+        self.mode = mode
+        self.leg2 = tuple(leg2) if leg2 is not None else None
+        self.sign = sign
+
+    def row_keys(self, sf, bins):
+        l, m = self.leg1[0], self.leg1[1]
+        return [sf.key(self.leg1, b, c) for b in bins for c in leg_components(l, m)]
+
+    def col_keys(self, sf, bins):
+        leg = self.leg1 if self.mode != "leg" else self.leg2
+        return [sf.key(leg, b, c) for b in bins for c in leg_components(leg[0], leg[1])]
+
+
+def assemble(ps, T, rows, cols, rbins, cbins):
+    """Complex S[i, j] over the (rbins x cbins) block from the real Gram T."""
+    ri = {k: i for i, k in enumerate(rows)}
+    ci = {k: j for j, k in enumerate(cols)}
+    leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
+
+    def t(k1, k2):
+        i = ri.get(k1)
+        j = ci.get(k2)
+        if i is None or j is None:
+            return 0.0
+        return T[i, j]
+
+    S = np.zeros((len(rbins), len(cbins)), dtype=np.complex128)
+    for a, bi in enumerate(rbins):
+        R1, I1 = (ps.leg1, bi, 0), (ps.leg1, bi, 1)
+        for c, bj in enumerate(cbins):
+            R2, I2 = (leg2, bj, 0), (leg2, bj, 1)
+            if ps.mode == "conj":
+                re = t(R1, R2) + t(I1, I2)
+                im = t(I1, R2) - t(R1, I2)
+                S[a, c] = ps.sign * complex(re, im)
+            else:
+                re = t(R1, R2) - t(I1, I2)
+                im = t(R1, I2) + t(I1, R2)
+                S[a, c] = complex(re, im)
+    return S
+
+
+def pair_sums(G, sf, pair_specs, k_bins, diagonal, block_size):
+    """Evaluate every PairSpec over all bins; returns a list of complex arrays
+    (k_bins x k_bins, or k_bins for diagonal mode).
+
+    Bins are processed in blocks of ``block_size`` rows x columns so that at most
+    the fields of one row block and one column block are resident
+    (clustering_estimator.py:911-981 bounds memory the same way).
+    """
+    results = [np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype=np.complex128)
+               for _ in pair_specs]
+    bs = k_bins if block_size is None else int(block_size)
+    blocks = [list(range(b0, min(k_bins, b0 + bs))) for b0 in range(0, k_bins, bs)]
+    for bi in blocks:
+        row_keys = []
+        for ps in pair_specs:
+            row_keys += ps.row_keys(sf, bi)
+        row_keys = list(dict.fromkeys(row_keys))
+        col_blocks = [bi] if diagonal else blocks
+        for bj in col_blocks:
+            col_keys = []
+            for ps in pair_specs:
+                col_keys += ps.col_keys(sf, bj)
+            col_keys = list(dict.fromkeys(col_keys))
+            keep = set(row_keys)
+            sf.release([k for k in list(sf.slot) if k not in keep and k not in set(col_keys)])
+            sf.ensure(row_keys + col_keys)
+            T = contract(G, sf, row_keys, col_keys)
+            for r, ps in enumerate(pair_specs):
+                S = assemble(ps, T, row_keys, col_keys, bi, bj)
+                if diagonal:
+                    results[r][bi] = np.diag(S)
+                else:
+                    results[r][bi[0]:bi[-1] + 1, bj[0]:bj[-1] + 1] = S
+        sf.release_all()
+    return results
+
+
+def fields_capacity(n, precision, want, reserve_bytes=0):
+    """How many real n^3 fields fit in the free HBM (leaving headroom)."""
+    esz = 4 if precision == "f32" else 8
+    free, _ = torch.cuda.mem_get_info()
+    avail = int(free * 0.8) - reserve_bytes
+    return max(1, min(int(want), avail // (esz * n ** 3)))

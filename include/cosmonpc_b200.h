@@ -1,0 +1,187 @@
+/*
+ * cosmonpc_b200.h -- C ABI of the B200 mesh-estimator library (libcosmonpc_b200.so).
+ *
+ * The reference (zhaoruiyang98/CosmoNPC) is pure Python; its mesh path calls
+ * pmesh (paint / r2c / c2r), numexpr (Y_lm, Legendre) and numpy (bincount,
+ * triple products).  Each entry point below replaces one of those steps and
+ * cites the reference lines it stands in for (paths inside the reference
+ * project).  Conventions shared by all entry points:
+ *
+ *  - Every function returns an int status (CNPC_OK = 0) and never throws.
+ *  - All pointers named d_* are device pointers owned by the caller; h_*
+ *    pointers are host memory read before the function returns.
+ *  - Work is enqueued on the given stream; nothing synchronises the host.
+ *  - dtype selects the arithmetic: CNPC_F32 (float / float2 fields, FP64
+ *    accumulators) or CNPC_F64 (double / double2 fields throughout).
+ *  - Real meshes are n*n*n, x slowest, z fastest.  Spectra are the half
+ *    spectrum of a real field in cuFFT R2C layout: n*n*(n/2+1) complex,
+ *    index (ix, iy, iz), n_x = ix - n*(ix >= n/2) (same for y), n_z = iz.
+ *  - A context owns cached cuFFT plans and is not thread-safe; use one
+ *    context per host thread.
+ */
+#ifndef COSMONPC_B200_H
+#define COSMONPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *cnpc_stream_t; /* == cudaStream_t */
+typedef struct cnpc_ctx cnpc_ctx;
+
+enum cnpc_status {
+    CNPC_OK = 0,
+    CNPC_EINVAL = 1,   /* bad argument (maps to ValueError)              */
+    CNPC_ENOMEM = 2,   /* device allocation refused (MemoryError)        */
+    CNPC_ECUDA = 3,    /* CUDA runtime error                             */
+    CNPC_ECUFFT = 4,   /* cuFFT error                                    */
+    CNPC_ETIMEOUT = 5  /* a bounded device-side wait gave up             */
+};
+
+enum cnpc_dtype { CNPC_F32 = 0, CNPC_F64 = 1 };
+
+/* mass-assignment window order p: NGP 1, CIC 2, TSC 3, PCS 4 */
+enum cnpc_window { CNPC_NGP = 1, CNPC_CIC = 2, CNPC_TSC = 3, CNPC_PCS = 4 };
+
+/* k-space window compensation (math_evaluator.py:206-309) */
+enum cnpc_comp {
+    CNPC_COMP_NONE = 0,
+    CNPC_COMP_SINC = 1,      /* v / prod sinc(w/2)^p            me:206-248 */
+    CNPC_COMP_SHOTNOISE = 2, /* v / prod sqrt(C_p(sin^2(w/2)))  me:251-275 */
+    CNPC_COMP_BKNOISE = 3    /* v * prod C_p / sinc^(2p)        me:278-309 */
+};
+
+/* Spherical harmonic descriptor.  Value on a unit vector (x, y, z):
+ *   Y = norm * poly(z) * (x + i y)^|m|, conjugated and multiplied by
+ *   (-1)^|m| when m < 0; poly has degree l-|m| (coef[0] constant term).
+ * origin_re/origin_im: the value used at the k = 0 mode, where the reference
+ * evaluates its polynomial at (0, 0, 0) (math_evaluator.py:12-22, :35-131). */
+typedef struct cnpc_harmonic {
+    int l;
+    int m;
+    double norm;
+    double coef[9];
+    double origin_re;
+    double origin_im;
+} cnpc_harmonic;
+
+/* One real shell field to synthesise (see cnpc_shell_spectra). */
+typedef struct cnpc_shell_item {
+    int bin;       /* index into the edges: mask = e[bin] <= |k| < e[bin+1]   */
+    int harmonic;  /* index into the harmonic table                           */
+    int component; /* 0: real part of the complex shell field, 1: imaginary   */
+    int source;    /* 0: spectrum A, 1: spectrum B, 2: unit spectrum (=1)     */
+    int conj;      /* 1: use conj(Y) instead of Y                             */
+} cnpc_shell_item;
+
+#define CNPC_MAX_EDGES 257
+#define CNPC_MAX_HARMONICS 16
+#define CNPC_MAX_ITEMS 256
+#define CNPC_MAX_POLES 8
+
+/* ---------------------------------------------------------------- context */
+int cnpc_ctx_create(cnpc_ctx **ctx, int device);
+int cnpc_ctx_destroy(cnpc_ctx *ctx);
+/* Text of the last error recorded in this context ("" if none). */
+const char *cnpc_ctx_last_error(cnpc_ctx *ctx);
+const char *cnpc_status_string(int status);
+/* Library version as major*10000 + minor*100 + patch. */
+int cnpc_version(void);
+
+/* ------------------------------------------------------------------ paint
+ * Replaces pmesh ParticleMesh.paint as called by pm_painter
+ * (src/cosmonpc/mesh_generator.py:172-224, :199, :204-205).
+ * h/d_pos: (np, 3) float64 positions; d_weight: np float64 or NULL (weight 1).
+ * Zeroes and fills d_mesh (node i at x = i*L/n, window order `window`); when
+ * d_mesh_shifted is non-NULL also paints the +1/2-cell interlaced mesh in the
+ * same pass (pm.affine.shift(0.5), mesh_generator.py:201-205). */
+int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_weight,
+               int64_t np, int n, double boxsize, int window,
+               void *d_mesh, void *d_mesh_shifted, cnpc_stream_t stream);
+
+/* --------------------------------------------------------------------- FFT
+ * Replace RealField.r2c / ComplexField.c2r of pmesh.  Unnormalised cuFFT
+ * transforms of `batch` contiguous fields; the 1/n^3 of pmesh's r2c is folded
+ * into cnpc_forward_finish.  c2r may overwrite its input. */
+int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real,
+                 void *d_spec, cnpc_stream_t stream);
+int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec,
+                 void *d_real, cnpc_stream_t stream);
+
+/* Finishes the forward transform in place on d_spec:
+ *   c = s1 / n^3                       (d_spec2 == NULL)
+ *   c = 0.5 s1/n^3 + 0.5 s2/n^3 e^{i(kx+ky+kz)H/2}  (interlaced combine,
+ *                                        mesh_generator.py:211-218)
+ *   c *= scale, then the compensation `comp` of window order `window`
+ *   (clustering_estimator.py:599-603, :815-816), and the k = 0 mode is set to
+ *   k0_value (the reference clears it for pk, ce:634-636, and it equals
+ *   (sum w / n^3)/dV - NZ for the bk overdensity, ce:808-816).
+ *   band_kmax > 0 zeroes modes with |k| >= band_kmax. */
+int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
+                        const void *d_spec2, double scale, int comp, int window,
+                        double k0_value, double band_kmax, cnpc_stream_t stream);
+
+/* -------------------------------------------------------- k-bin statistics
+ * get_kbin_count (math_evaluator.py:452-481): full-space mode counts and sum
+ * of |k| per bin [e_b, e_{b+1}), |k| computed in FP64 as
+ * sqrt((kx^2 + ky^2) + kz^2) with k = (2 n) pi / L.  d_counts / d_ksum get
+ * nedges-1 doubles each. */
+int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges,
+                     int nedges, double *d_counts, double *d_ksum, cnpc_stream_t stream);
+
+/* Power-spectrum shell sums for calculate_power_spectrum_box
+ * (clustering_estimator.py:638-693): for each pole l in h_poles,
+ *   sum_{k in bin} (Re a Re b + Im a Im b) * P_l(khat . los)
+ * over full k-space (half spectrum times multiplicity), FP64 accumulators.
+ * d_spec_b may equal d_spec_a.  d_sums: npoles * (nedges-1) doubles. */
+int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                 const void *d_spec_b, const double *h_edges, int nedges,
+                 const int *h_poles, int npoles, const double *h_los, double *d_sums,
+                 cnpc_stream_t stream);
+
+/* Shot-noise shell sums for calculate_bk_sugi_box (ce:1405-1434) and the
+ * S3-FFT source spectrum (ce:1187-1210):
+ *   P(k) = V^2 a(k) conj(b(k)) - sn0 * W_bknoise(k)
+ *   d_sums[2*bin + {0,1}] = sum_{bin} P(k) * Y_L0(khat)   (complex, FP64)
+ * with harmonic h_yl0 (NULL: 1).  If d_source is non-NULL, P(k) (without Y)
+ * is also written there, zeroed at |k| >= band_kmax when band_kmax > 0. */
+int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                 const void *d_spec_b, double volume_sq, double sn0, int window,
+                 const cnpc_harmonic *h_yl0, const double *h_edges, int nedges,
+                 double *d_sums, void *d_source, double band_kmax, cnpc_stream_t stream);
+
+/* Shell spectra: replaces (ylm_weighted_cfield * mask_i) before .c2r() in
+ * clustering_estimator.py:898-969, :1012-1050, :1215-1219.  For each item j,
+ * writes half spectrum j of d_out (n*n*(n/2+1) complex each):
+ *   src(k) * mask_bin(|k|) * phi(k)
+ * where the complex shell field F = c2r(src * Y * mask) is split into real
+ * fields Re F = c2r(src * phi_re), Im F = c2r(src * phi_im) with
+ *   even l: phi_re = Re Y,   phi_im = Im Y
+ *   odd l:  phi_re = i Im Y, phi_im = -i Re Y
+ * (valid because src is Hermitian on |k| < k_Nyquist). */
+int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize,
+                       const void *d_spec_a, const void *d_spec_b,
+                       const double *h_edges, int nedges,
+                       const cnpc_harmonic *h_harmonics, int nharmonics,
+                       const cnpc_shell_item *h_items, int nitems, void *d_out,
+                       cnpc_stream_t stream);
+
+/* ------------------------------------------------------ x-space reductions
+ * Replaces np.sum(G * F1 * F2) of clustering_estimator.py:972, :1051, :1257,
+ * :1341 for real component fields.
+ * Gram form: d_out[i*nb + j] = sum_x G(x) F_{a_i}(x) F_{b_j}(x), FP64 result,
+ * where field f starts at d_fields + f * field_stride (elements).
+ * Per-block partials live in the context's scratch buffer, so calls on one
+ * context must not overlap on different streams. */
+int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
+                       const void *d_fields, int64_t field_stride,
+                       const int *h_a, int na, const int *h_b, int nb, double *d_out,
+                       cnpc_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COSMONPC_B200_H */
