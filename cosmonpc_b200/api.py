@@ -37,10 +37,10 @@ def _weight_sum(pos, weight):
     return float(weight.sum().item())
 
 
-def box_attrs(n_gal, weight_sum, boxsize, **settings):
+def box_attrs(n_gal, weight_sum, box_length, **settings):
     """stat_attrs of an auto box run (mesh_generator.py:56-60, :106-117)."""
     attrs = dict(settings)
-    attrs.update({"NZ_a": weight_sum / float(np.prod(np.array([boxsize] * 3))), "N_gal_a": int(n_gal)})
+    attrs.update({"NZ_a": weight_sum / float(np.prod(np.array([box_length] * 3))), "N_gal_a": int(n_gal)})
     return attrs
 
 

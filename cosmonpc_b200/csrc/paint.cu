@@ -21,11 +21,11 @@ template <int P> __device__ inline double bspline(double s) {
 }
 
 template <int P> __device__ inline void axis_weights(double g, int n, int *idx, double *w) {
-    int base = (P % 2 == 0) ? (int)floor(g) - (P / 2 - 1) : (int)floor(g + 0.5) - (P - 1) / 2;
+    int base = (P % 2 == 0) ? (int)floor(g) - (P / 2 - 1) : (int)floor(__dadd_rn(g, 0.5)) - (P - 1) / 2;
 #pragma unroll
     for (int o = 0; o < P; ++o) {
         int node = base + o;
-        w[o] = bspline<P>((double)node - g);
+        w[o] = bspline<P>(__dsub_rn((double)node, g));
         int r = node % n;
         idx[o] = r < 0 ? r + n : r;
     }
@@ -55,12 +55,15 @@ __global__ void paint_kernel(const double *__restrict__ pos, const double *__res
                              int64_t np, int n, double scale, T *mesh, T *mesh_shifted) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
-        const double gx = pos[3 * i + 0] * scale;
-        const double gy = pos[3 * i + 1] * scale;
-        const double gz = pos[3 * i + 2] * scale;
+        // separately rounded products and sums (no FMA contraction), so grid
+        // coordinates match the restated pmesh affine transform bit for bit
+        const double gx = __dmul_rn(pos[3 * i + 0], scale);
+        const double gy = __dmul_rn(pos[3 * i + 1], scale);
+        const double gz = __dmul_rn(pos[3 * i + 2], scale);
         const double mass = weight ? weight[i] : 1.0;
         deposit<T, P>(mesh, n, gx, gy, gz, mass);
-        if (mesh_shifted) deposit<T, P>(mesh_shifted, n, gx + 0.5, gy + 0.5, gz + 0.5, mass);
+        if (mesh_shifted)
+            deposit<T, P>(mesh_shifted, n, __dadd_rn(gx, 0.5), __dadd_rn(gy, 0.5), __dadd_rn(gz, 0.5), mass);
     }
 }
 

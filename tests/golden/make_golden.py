@@ -33,7 +33,9 @@ from ref_shims import import_reference  # noqa: E402
 def main(names=None):
     te = import_reference()
     logging.disable(logging.INFO)
-    work = tempfile.mkdtemp(prefix="cnpc_golden_")
+    # catalogs live in a folder named "golden": the bispectrum output file name
+    # carries the catalog's parent folder name (task_executor.py:305-309)
+    work = os.path.join(tempfile.mkdtemp(prefix="cnpc_golden_"), "golden")
     for name, _, _ in CASES:
         if names and name not in names:
             continue

@@ -33,7 +33,7 @@ def _run(cfg, precision, tmp_path):
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 @pytest.mark.parametrize("name", [c[0] for c in CASES])
 def test_golden_case(name, precision, tmp_path):
-    cfg, _ = build_case(name, str(tmp_path))
+    cfg, _ = build_case(name, str(tmp_path / "golden"))
     gold = np.load("%s/%s.npz" % (GOLDEN, name))
     res, fname = _run(cfg, precision, tmp_path)
     assert fname == str(gold["output_name"])

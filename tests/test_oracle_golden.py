@@ -12,7 +12,7 @@ NAMES = [c[0] for c in CASES]
 def test_oracle_matches_reference_golden(name, tmp_path):
     from oracle.driver import run_box
 
-    cfg, sums = build_case(name, str(tmp_path))
+    cfg, sums = build_case(name, str(tmp_path / "golden"))
     gold = np.load("%s/%s.npz" % (GOLDEN, name))
     for letter, s in sums.items():
         assert s == pytest.approx(float(gold["checksum." + letter]), rel=0, abs=1e-6), \
