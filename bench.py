@@ -62,7 +62,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -97,7 +97,14 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+            err = ""
+            if self.proc is not None and self.proc.stderr is not None:
+                try:
+                    err = self.proc.stderr.read()[:200]
+                except Exception:
+                    pass
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"],
+                    "note": (self.lines[:2], err)}
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 

@@ -215,3 +215,69 @@ def valid_k3_bins(k1, k2, k_min, k_max, k_bins):
     e = np.linspace(2 * k_min, 2 * k_max, 2 * k_bins + 1)[:-1]
     c = 0.5 * (e[1:] + e[:-1])
     return np.logical_and(c >= abs(k1 - k2), c <= (k1 + k2))
+
+
+def assoc_legendre_array(l, m, mu):
+    """Vectorised ``assoc_legendre`` (same conventions) over an array of mu."""
+    ma = abs(m)
+    mu = np.asarray(mu, dtype=np.float64)
+    if ma > l:
+        return np.zeros_like(mu)
+    q = reduced_assoc_coeffs(l, ma)
+    poly = np.zeros_like(mu)
+    for c in reversed(q):
+        poly = poly * mu + float(c)
+    with np.errstate(invalid="ignore"):
+        val = poly * (1.0 - mu * mu) ** (0.5 * ma) if ma else poly
+    if m < 0:
+        val = val * ((-1) ** ma * math.factorial(l - ma) / math.factorial(l + ma))
+    return val
+
+
+def q_ells_matrix(k1s, l1, l2, L, k3s):
+    """q_{l1 l2 L}(k1_i, k1_j, k3_t) for every (i, j, t) at once
+    (math_evaluator.py:560-616 evaluated on arrays): shape (B, B, K3)."""
+    k1 = np.asarray(k1s, dtype=np.float64)[:, None, None]
+    k2 = np.asarray(k1s, dtype=np.float64)[None, :, None]
+    k3 = np.asarray(k3s, dtype=np.float64)[None, None, :]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        valid = np.logical_and(np.abs(k1 - k2) <= k3, k3 <= (k1 + k2))
+        mu13 = np.where(valid, (k3 ** 2 + k1 ** 2 - k2 ** 2) / (2 * k1 * k3), 0.0)
+        mu23 = np.where(valid, (k3 ** 2 + k2 ** 2 - k1 ** 2) / (2 * k2 * k3), 0.0)
+    q = np.zeros(valid.shape)
+    lmin = min(l1, l2)
+    for n in range(-lmin, lmin + 1):
+        tj = wigner3j(l1, l2, L, n, -n, 0)
+        if tj == 0.0:
+            continue
+        a13 = np.where(valid, assoc_legendre_array(l1, n, mu13), 0.0) * (-1) ** (l1 + n)
+        a23 = np.where(valid, assoc_legendre_array(l2, -n, mu23), 0.0) * (-1) ** (l2 - n)
+        q += (-1) ** n * tj * a13 * a23
+    return q
+
+
+def s3_analytic(total_sum, k_num_k3, k_edge, k3_center, q, diagonal):
+    """Analytical S3 contraction (clustering_estimator.py:1081-1180) given the
+    q kernel array from ``q_ells_matrix``; returns the (unnormalised) S3."""
+    k_bins = len(k_edge) - 1
+    weighted = k_num_k3 / k3_center
+    terms = total_sum / k3_center
+    if diagonal:
+        s3 = np.zeros(k_bins, dtype="complex128")
+        for i in range(k_bins):
+            numer = np.sum(q[i, i] * terms)
+            denom = np.sum(weighted[: 2 * i + 1])
+            if denom > 0:
+                s3[i] = numer / denom
+        return s3
+    k_center = 0.5 * (k_edge[1:] + k_edge[:-1])
+    kc1 = k_center[:, None, None]
+    kc2 = k_center[None, :, None]
+    k3c = k3_center[None, None, :]
+    vb = np.logical_and(k3c >= np.abs(kc1 - kc2), k3c <= (kc1 + kc2))
+    numer = np.sum(q * terms[None, None, :], axis=2)
+    denom = np.sum(weighted[None, None, :] * vb, axis=2)
+    s3 = np.zeros((k_bins, k_bins), dtype="complex128")
+    ok = denom > 0
+    s3[ok] = numer[ok] / denom[ok]
+    return s3

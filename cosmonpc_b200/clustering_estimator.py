@@ -132,14 +132,19 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
     set of painted meshes, sharing the forward transforms, G, the shell fields and
     the FFT shot-noise shells among configurations.
 
-    Returns one reference-format result dict per configuration.  Called with a
-    single configuration this is ``calculate_bk_sugi_box``.
+    All device work is enqueued first; the host reads the mode counts and the
+    shot-noise shell sums as soon as they are ready (the analytical S3 algebra
+    overlaps the remaining GPU work) and the pair sums last.  Returns one
+    reference-format result dict per configuration; with a single configuration
+    this is ``calculate_bk_sugi_box``.
     """
     data_vector_mode = stat_attrs.get("data_vector_mode", "diagonal")
     shotnoise_mode = stat_attrs.get("shotnoise_mode", "ana")
-    diagonal = data_vector_mode == "diagonal"
     if data_vector_mode not in ("diagonal", "full"):
         raise ValueError("data_vector_mode must be either 'diagonal' or 'full'.")
+    if shotnoise_mode not in ("ana", "fft", "both"):
+        raise ValueError("shotnoise_mode must be either 'ana', 'fft', or 'both'.")
+    diagonal = data_vector_mode == "diagonal"
     boxsize = np.array(stat_attrs["boxsize"])
     nmesh = np.array(stat_attrs["nmesh"])
     k_min, k_max, k_bins = stat_attrs["k_min"], stat_attrs["k_max"], stat_attrs["k_bins"]
@@ -150,87 +155,109 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
     N3 = nmesh.prod()
     vol_per_cell = V / N3
     window = _lib.WINDOW[sampler]
+    code, rdt, cdt = engine.PRECISION[precision]
+    ctx = _lib.Context.get()
 
     letters = ["a"] + (["b"] if correlation_mode == "cross" else []) + (["c"] if tracer_type == "abc" else [])
     NZ = {t: stat_attrs["NZ_" + t] for t in letters}
     N_gal = {t: stat_attrs["N_gal_" + t] for t in letters}
 
+    # ---- overdensity spectra: r2c(rho/dV - NZ), compensated (ce:808-837)
     k_edge = np.linspace(k_min, k_max, k_bins + 1)
-    # overdensity spectra: r2c(rho/dV - NZ), compensated (ce:808-837)
     spec = {}
     for t in letters:
         m = meshes[t]
         k0 = (m.sum_w / float(N3)) / vol_per_cell - NZ[t]
         spec[t] = engine.finish_delta(m, 1.0 / vol_per_cell, _lib.COMP_SINC, k0)
+    dev = spec["a"].device
 
-    counts, ksum = engine.kbin_counts(n, L, k_edge)
-    k_num = counts.cpu().numpy()
-    k_eff = ksum.cpu().numpy() / k_num
-
-    g_letter = "a" if correlation_mode == "auto" else ("c" if tracer_type == "abc" else "b")
-    # G_00 = Re c2r(delta); only |k| < 2 k_max reaches the triple sums
-    G = engine.band_limited_field(n, L, spec[g_letter], 2.0 * k_max, precision)
-
-    # ---- signal: shell fields and pair sums for every magnetic sub-configuration
-    per_cfg = []
-    specs = []
-    for (l1, l2, L_) in angu_configs:
-        cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
-        entries = []
-        for ss, (m1, m2, _) in enumerate(cfgs):
-            ps = _legs_for_signal(l1, l2, m1, m2, correlation_mode, tracer_type)
-            entries.append((len(specs), (m1, m2), tj[ss]))
-            specs.append(ps)
-        per_cfg.append(entries)
-
-    spec_b = spec.get("b")
-    bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal)
-    sf = engine.ShellFields(n, L, k_edge, precision, spec["a"], spec_b, capacity=capacity)
-    sums = engine.pair_sums(G, sf, specs, k_bins, diagonal, bs)
-    del sf, G
-
-    # ---- k3 bins (ce:1063-1074)
+    # ---- mode counts on k and k3 bins (ce:858-865, :1063-1074)
     k_center = 0.5 * (k_edge[1:] + k_edge[:-1])
     k3_edge = np.linspace(2 * k_min, 2 * k_max, k_bins * 2 + 1)[:-1]
     k3_center = 0.5 * (k3_edge[1:] + k3_edge[:-1])
     k3_bins = len(k3_center)
-    c3, s3 = engine.kbin_counts(n, L, k3_edge)
-    k_num_k3 = c3.cpu().numpy()
-    k3_eff = s3.cpu().numpy() / k_num_k3
+    counts_k = engine.HostCopy(torch.stack(engine.kbin_counts(n, L, k_edge)))
+    counts_k3 = engine.HostCopy(torch.stack(engine.kbin_counts(n, L, k3_edge)))
 
-    other = spec["a"] if correlation_mode == "auto" else spec["b"]
-    code = engine.PRECISION[precision][0]
-    ctx = _lib.Context.get()
-    need_fft = shotnoise_mode in ("fft", "both") and tracer_type not in ("abc", "abb")
-    src_field = None
+    # ---- shot-noise shell sums P(k) Y_L0 on k3 bins (ce:1394-1434) and the
+    #      band-limited S3-FFT source field (ce:1187-1210)
+    other = spec["a"] if correlation_mode == "auto" else spec.get("b")
+    sn_sums = {}
+    src_fields = {}
+    cfg_info = []
+    for (l1, l2, L_) in angu_configs:
+        sn0 = N_gal["a"] if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
+        cfg_info.append(sn0)
+        if tracer_type == "abc":
+            continue
+        key = (L_, sn0)
+        if key not in sn_sums:
+            d = torch.empty(2 * k3_bins, dtype=torch.float64, device=dev)
+            yl0 = angular.harmonic(L_, 0, True) if L_ != 0 else None
+            ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                        float(sn0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d)
+            sn_sums[key] = engine.HostCopy(d)
+        if shotnoise_mode in ("fft", "both") and tracer_type != "abb" and sn0 not in src_fields:
+            src_spec = torch.empty(spec["a"].shape, dtype=cdt, device=dev)
+            d = torch.empty(2 * k3_bins, dtype=torch.float64, device=dev)
+            ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                        float(sn0) if correlation_mode == "auto" else 0.0, window, None, k3_edge, d,
+                        source=src_spec, band=2.0 * k_max)
+            fld = torch.empty(n * n * n, dtype=rdt, device=dev)
+            ctx.c2r(code, n, 1, src_spec, fld)
+            del src_spec
+            src_fields[sn0] = fld
+
+    # ---- signal: G_00 = Re c2r(delta) band-limited to |k| < 2 k_max (the only
+    #      modes the triple sums see), shell fields, pair sums (ce:867-1061)
+    g_letter = "a" if correlation_mode == "auto" else ("c" if tracer_type == "abc" else "b")
+    G = engine.band_limited_field(n, L, spec[g_letter], 2.0 * k_max, precision)
+    specs, per_cfg = [], []
+    for (l1, l2, L_) in angu_configs:
+        cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
+        entries = []
+        for ss, (m1, m2, _) in enumerate(cfgs):
+            entries.append((len(specs), (m1, m2), tj[ss]))
+            specs.append(_legs_for_signal(l1, l2, m1, m2, correlation_mode, tracer_type))
+        per_cfg.append(entries)
+    bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal)
+    sf = engine.ShellFields(n, L, k_edge, precision, spec["a"], spec.get("b"), capacity=capacity)
+    signal = engine.pair_sums(G, sf, specs, k_bins, diagonal, bs)
+    del sf, G
+
+    # ---- S3 by FFT: data-independent shells conj(Y) mask on a unit spectrum
+    #      contracted with the source field (ce:1182-1384)
+    s3fft = {}
+    for ci, (l1, l2, L_) in enumerate(angu_configs):
+        sn0 = cfg_info[ci]
+        if sn0 not in src_fields:
+            continue
+        cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
+        sp = [_legs_for_s3fft(l1, l2, m1, m2) for (m1, m2, _) in cfgs]
+        bsf, capf = _plan_blocks(sp, k_bins, n, precision, block_size, diagonal)
+        sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
+        s3fft[ci] = engine.pair_sums(src_fields[sn0], sfu, sp, k_bins, diagonal, bsf)
+        del sfu
+
+    # ---- host algebra while the GPU drains the queue
+    ck = counts_k.get()
+    k_num, k_eff = ck[0].copy(), ck[1] / ck[0]
+    c3 = counts_k3.get()
+    k_num_k3, k3_eff = c3[0].copy(), c3[1] / c3[0]
+
     results = []
-    sn_cache = {}
+    sig = None
     for ci, (l1, l2, L_) in enumerate(angu_configs):
         N_ells = (2 * l1 + 1) * (2 * l2 + 1) * (2 * L_ + 1)
         H_ells = angular.wigner3j(l1, l2, L_, 0, 0, 0)
         cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
-        if diagonal:
-            total_res = np.zeros(k_bins).astype("complex128")
-        else:
-            total_res = np.zeros((k_bins, k_bins)).astype("complex128")
-        for (idx, (m1, m2), three_j) in per_cfg[ci]:
-            sub = three_j * sums[idx]
-            total_res += sub if (m1, m2) == (0, 0) else 2 * np.real(sub)
-
         SN3_fft = None
         if tracer_type == "abc":
             SN0, SN1, SN2, SN3 = 0.0, 0.0, 0.0, 0.0
         else:
-            SN0 = N_gal["a"] if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
-            key = (L_, SN0)
-            if key not in sn_cache:
-                d = torch.empty(2 * k3_bins, dtype=torch.float64, device=spec["a"].device)
-                yl0 = angular.harmonic(L_, 0, True) if L_ != 0 else None
-                ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                            float(SN0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d)
-                dd = d.cpu().numpy()
-                sn_cache[key] = dd[0::2] + 1j * dd[1::2]
-            total_sum = sn_cache[key]
+            SN0 = cfg_info[ci]
+            dd = sn_sums[(L_, SN0)].get()
+            total_sum = dd[0::2] + 1j * dd[1::2]
             SN1, SN2 = 0.0, 0.0
             if l1 == L_ and l2 == 0:
                 if correlation_mode == "auto":
@@ -259,73 +286,28 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
             def s3_ana():
                 if tracer_type == "abb":
                     return 0.0
-                weighted_k_num = k_num_k3 / k3_center
-                if diagonal:
-                    s3 = np.zeros(k_bins, dtype="complex128")
-                    for i in range(k_bins):
-                        if shotnoise_ana_all_eff:
-                            q = angular.q_ells_eff(i, i, k_eff, l1, l2, L_, k3_eff)
-                        else:
-                            q = _q_ells_center(i, i, k_center, k_min, k_max, k_bins, l1, l2, L_)
-                        numer = np.sum(q * total_sum / k3_center)
-                        denom = np.sum(weighted_k_num[: 2 * i + 1])
-                        if denom > 0:
-                            s3[i] = numer / denom
+                if shotnoise_ana_all_eff:
+                    q = angular.q_ells_matrix(k_eff, l1, l2, L_, k3_eff)
                 else:
-                    s3 = np.zeros((k_bins, k_bins), dtype="complex128")
-                    for i in range(k_bins):
-                        for j in range(k_bins):
-                            if shotnoise_ana_all_eff:
-                                q = angular.q_ells_eff(i, j, k_eff, l1, l2, L_, k3_eff)
-                            else:
-                                q = _q_ells_center(i, j, k_center, k_min, k_max, k_bins, l1, l2, L_)
-                            vb = angular.valid_k3_bins(k_center[i], k_center[j], k_min, k_max, k_bins)
-                            numer = np.sum(q * total_sum / k3_center)
-                            denom = np.sum(weighted_k_num * vb)
-                            if denom > 0:
-                                s3[i, j] = numer / denom
-                return s3 * (H_ells * N_ells)
+                    q = angular.q_ells_matrix(k_center, l1, l2, L_, k3_center)
+                return angular.s3_analytic(total_sum, k_num_k3, k_edge, k3_center, q, diagonal) * (H_ells * N_ells)
 
             def s3_fft():
-                nonlocal src_field
                 if tracer_type == "abb":
                     return np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
-                sn0_src = float(N_gal["a"]) if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
-                skey = ("src", sn0_src)
-                if skey not in sn_cache:
-                    cdt = engine.PRECISION[precision][2]
-                    src_spec = torch.empty_like(spec["a"], dtype=cdt)
-                    d = torch.empty(2 * k3_bins, dtype=torch.float64, device=spec["a"].device)
-                    ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                                sn0_src if correlation_mode == "auto" else 0.0, window, None, k3_edge, d,
-                                source=src_spec, band=2.0 * k_max)
-                    rdt = engine.PRECISION[precision][1]
-                    fld = torch.empty(n * n * n, dtype=rdt, device=spec["a"].device)
-                    ctx.c2r(code, n, 1, src_spec, fld)
-                    del src_spec
-                    sn_cache[skey] = fld
-                src = sn_cache[skey]
-                sp = []
-                for (m1, m2, _) in cfgs:
-                    sp.append(_legs_for_s3fft(l1, l2, m1, m2))
-                bsf, capf = _plan_blocks(sp, k_bins, n, precision, block_size, diagonal)
-                sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
-                ss_list = engine.pair_sums(src, sfu, sp, k_bins, diagonal, bsf)
-                del sfu
+                ss_list = s3fft[ci].result()
                 s3 = np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
                 for ss, (m1, m2, _) in enumerate(cfgs):
                     S = ss_list[ss]
                     if diagonal:
                         sub = np.zeros(k_bins, dtype="complex128")
-                        for i in range(k_bins):
-                            if k_num[i] > 0:
-                                sub[i] = tj[ss] * S[i] / (k_num[i] ** 2)
+                        ok = k_num > 0
+                        sub[ok] = tj[ss] * S[ok] / (k_num[ok] ** 2)
                     else:
                         sub = np.zeros((k_bins, k_bins), dtype="complex128")
-                        for i in range(k_bins):
-                            for j in range(k_bins):
-                                if k_num[i] > 0 and k_num[j] > 0:
-                                    sub[i, j] = tj[ss] * S[i, j] / (k_num[i] * k_num[j])
+                        ok = np.outer(k_num > 0, k_num > 0)
+                        with np.errstate(divide="ignore", invalid="ignore"):
+                            sub[ok] = (tj[ss] * S / np.outer(k_num, k_num))[ok]
                     s3 += sub if (m1, m2) == (0, 0) else 2.0 * np.real(sub)
                 s3 *= H_ells * N_ells
                 s3 *= 1 / nmesh.prod()
@@ -335,11 +317,16 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
                 SN3 = s3_ana()
             elif shotnoise_mode == "fft":
                 SN3 = s3_fft()
-            elif shotnoise_mode == "both":
+            else:
                 SN3 = s3_ana()
                 SN3_fft = s3_fft()
-            else:
-                raise ValueError("shotnoise_mode must be either 'ana', 'fft', or 'both'.")
+
+        if sig is None:
+            sig = signal.result()
+        total_res = np.zeros(k_bins if diagonal else (k_bins, k_bins)).astype("complex128")
+        for (idx, (m1, m2), three_j) in per_cfg[ci]:
+            sub = three_j * sig[idx]
+            total_res += sub if (m1, m2) == (0, 0) else 2 * np.real(sub)
 
         # normalisation (ce:1495-1548)
         if correlation_mode == "auto":
@@ -351,7 +338,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         else:
             I_norm = (N_gal["a"] * N_gal["b"] * N_gal["c"]) / (V ** 2)
         total_shot_noise = SN0 + SN1 + SN2 + SN3
-        total_res = total_res * (N_ells * H_ells / I_norm)
+        total_res *= N_ells * H_ells / I_norm
         if not diagonal:
             total_res *= V ** 2 / np.outer(k_num[:k_bins], k_num[:k_bins])
         else:
@@ -361,6 +348,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         final_bk = total_res - total_shot_noise
         sn_terms = {"SN0": SN0 / I_norm, "SN1": SN1 / I_norm, "SN2": SN2 / I_norm, "SN3": SN3 / I_norm}
         if shotnoise_mode == "both":
+            # the reference divides None by I_norm here for tracer "abc" (TypeError)
             sn_terms["SN3_FFT"] = SN3_fft / I_norm
         results.append({
             "B_sugi": final_bk, "SN_terms": sn_terms, "I_norm": I_norm, "Shot_noise": total_shot_noise,

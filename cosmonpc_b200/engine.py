@@ -183,23 +183,41 @@ def band_limited_field(n, boxsize, spec, kmax_band, precision, racah=True):
     return out
 
 
+class HostCopy:
+    """A device tensor copied to pinned host memory without blocking the host;
+    ``get()`` waits only for that copy."""
+
+    def __init__(self, t):
+        self.host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        self.host.copy_(t, non_blocking=True)
+        self.event = torch.cuda.Event()
+        self.event.record()
+
+    def get(self):
+        self.event.synchronize()
+        return self.host.numpy()
+
+
 def contract(G, sf, rows, cols):
-    """T[i, j] = sum_x G F_rows[i] F_cols[j] (FP64 host array)."""
+    """Device tensor T[i, j] = sum_x G F_rows[i] F_cols[j] (FP64), enqueued only."""
     ctx = _lib.Context.get()
     ncell = sf.n ** 3
-    T = np.zeros((len(rows), len(cols)))
+    dev = _device()
+    T = torch.zeros((len(rows), len(cols)), dtype=torch.float64, device=dev)
     if not rows or not cols:
         return T
     ridx = [sf.slot[k] for k in rows]
     cidx = [sf.slot[k] for k in cols]
-    dev = _device()
     for r0 in range(0, len(ridx), 128):
         for c0 in range(0, len(cidx), 128):
             rr = ridx[r0:r0 + 128]
             cc = cidx[c0:c0 + 128]
-            out = torch.empty(len(rr) * len(cc), dtype=torch.float64, device=dev)
-            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
-            T[r0:r0 + len(rr), c0:c0 + len(cc)] = out.cpu().numpy().reshape(len(rr), len(cc))
+            if r0 == 0 and c0 == 0 and len(rr) == len(ridx) and len(cc) == len(cidx):
+                ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, T)
+            else:
+                out = torch.empty((len(rr), len(cc)), dtype=torch.float64, device=dev)
+                ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
+                T[r0:r0 + len(rr), c0:c0 + len(cc)] = out
     return T
 
 
@@ -254,16 +272,44 @@ def assemble(ps, T, rows, cols, rbins, cbins):
     return S
 
 
+class DeferredPairSums:
+    """Pair sums whose device Grams are still in flight; ``result()`` copies
+    them to the host once and assembles the complex sums."""
+
+    def __init__(self, pair_specs, k_bins, diagonal):
+        self.pair_specs = pair_specs
+        self.k_bins = k_bins
+        self.diagonal = diagonal
+        self.blocks = []
+
+    def add(self, T, rows, cols, bi, bj):
+        self.blocks.append((HostCopy(T), rows, cols, bi, bj))
+
+    def result(self):
+        k_bins = self.k_bins
+        results = [np.zeros((k_bins, k_bins) if not self.diagonal else k_bins, dtype=np.complex128)
+                   for _ in self.pair_specs]
+        for hc, rows, cols, bi, bj in self.blocks:
+            T = hc.get()
+            for r, ps in enumerate(self.pair_specs):
+                S = assemble(ps, T, rows, cols, bi, bj)
+                if self.diagonal:
+                    results[r][bi] = np.diag(S)
+                else:
+                    results[r][bi[0]:bi[-1] + 1, bj[0]:bj[-1] + 1] = S
+        return results
+
+
 def pair_sums(G, sf, pair_specs, k_bins, diagonal, block_size):
-    """Evaluate every PairSpec over all bins; returns a list of complex arrays
-    (k_bins x k_bins, or k_bins for diagonal mode).
+    """Enqueue every PairSpec over all bins; returns a DeferredPairSums whose
+    ``result()`` is a list of complex arrays (k_bins x k_bins, or k_bins in
+    diagonal mode).
 
     Bins are processed in blocks of ``block_size`` rows x columns so that at most
     the fields of one row block and one column block are resident
     (clustering_estimator.py:911-981 bounds memory the same way).
     """
-    results = [np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype=np.complex128)
-               for _ in pair_specs]
+    out = DeferredPairSums(pair_specs, k_bins, diagonal)
     bs = k_bins if block_size is None else int(block_size)
     blocks = [list(range(b0, min(k_bins, b0 + bs))) for b0 in range(0, k_bins, bs)]
     for bi in blocks:
@@ -277,18 +323,12 @@ def pair_sums(G, sf, pair_specs, k_bins, diagonal, block_size):
             for ps in pair_specs:
                 col_keys += ps.col_keys(sf, bj)
             col_keys = list(dict.fromkeys(col_keys))
-            keep = set(row_keys)
-            sf.release([k for k in list(sf.slot) if k not in keep and k not in set(col_keys)])
+            keep = set(row_keys) | set(col_keys)
+            sf.release([k for k in list(sf.slot) if k not in keep])
             sf.ensure(row_keys + col_keys)
-            T = contract(G, sf, row_keys, col_keys)
-            for r, ps in enumerate(pair_specs):
-                S = assemble(ps, T, row_keys, col_keys, bi, bj)
-                if diagonal:
-                    results[r][bi] = np.diag(S)
-                else:
-                    results[r][bi[0]:bi[-1] + 1, bj[0]:bj[-1] + 1] = S
+            out.add(contract(G, sf, row_keys, col_keys), row_keys, col_keys, bi, bj)
         sf.release_all()
-    return results
+    return out
 
 
 def fields_capacity(n, precision, want, reserve_bytes=0):

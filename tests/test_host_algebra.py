@@ -83,3 +83,14 @@ def test_pair_assembly_matches_complex_brute_force():
         F2m = {"leg": F2, "eq": F1, "conj": -np.conj(F1)}[mode]
         ref = np.array([[np.sum(G * F1[i] * F2m[j]) for j in range(nb)] for i in range(nb)])
         np.testing.assert_allclose(S, ref, atol=1e-12)
+
+
+def test_vectorised_q_matches_oracle():
+    k_eff = np.array([0.012, 0.021, 0.033, 0.041, np.nan])
+    k3 = np.linspace(0.02, 0.09, 9)
+    for cfg in [(0, 0, 0), (2, 0, 2), (1, 1, 2), (2, 2, 0), (1, 1, 0)]:
+        Q = A.q_ells_matrix(k_eff, *cfg, k3)
+        for i in range(4):
+            for j in range(4):
+                np.testing.assert_allclose(Q[i, j], O.q_ells_eff(i, j, k_eff, *cfg, k3), atol=1e-13)
+        assert np.all(Q[4] == 0) and np.all(Q[:, 4] == 0)
