@@ -222,21 +222,27 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         per_cfg.append(entries)
     bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal)
     sf = engine.ShellFields(n, L, k_edge, precision, spec["a"], spec.get("b"), capacity=capacity)
-    signal = engine.pair_sums(G, sf, specs, k_bins, diagonal, bs)
+    signal = engine.pair_sums([(G, specs)], sf, k_bins, diagonal, bs)[0]
     del sf, G
 
-    # ---- S3 by FFT: data-independent shells conj(Y) mask on a unit spectrum
-    #      contracted with the source field (ce:1182-1384)
-    s3fft = {}
+    # ---- S3 by FFT: data-independent shells conj(Y) mask on a unit spectrum,
+    #      shared by every configuration, contracted with each configuration's
+    #      source field (ce:1182-1384)
+    s3_groups, s3_index = [], {}
     for ci, (l1, l2, L_) in enumerate(angu_configs):
         sn0 = cfg_info[ci]
         if sn0 not in src_fields:
             continue
         cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)
-        sp = [_legs_for_s3fft(l1, l2, m1, m2) for (m1, m2, _) in cfgs]
-        bsf, capf = _plan_blocks(sp, k_bins, n, precision, block_size, diagonal)
+        s3_index[ci] = len(s3_groups)
+        s3_groups.append((src_fields[sn0], [_legs_for_s3fft(l1, l2, m1, m2) for (m1, m2, _) in cfgs]))
+    s3fft = {}
+    if s3_groups:
+        all_sp = [ps for (_, sp) in s3_groups for ps in sp]
+        bsf, capf = _plan_blocks(all_sp, k_bins, n, precision, block_size, diagonal)
         sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
-        s3fft[ci] = engine.pair_sums(src_fields[sn0], sfu, sp, k_bins, diagonal, bsf)
+        outs = engine.pair_sums(s3_groups, sfu, k_bins, diagonal, bsf)
+        s3fft = {ci: outs[gi] for ci, gi in s3_index.items()}
         del sfu
 
     # ---- host algebra while the GPU drains the queue

@@ -300,35 +300,41 @@ class DeferredPairSums:
         return results
 
 
-def pair_sums(G, sf, pair_specs, k_bins, diagonal, block_size):
-    """Enqueue every PairSpec over all bins; returns a DeferredPairSums whose
-    ``result()`` is a list of complex arrays (k_bins x k_bins, or k_bins in
-    diagonal mode).
+def pair_sums(groups, sf, k_bins, diagonal, block_size):
+    """Enqueue sum_x G F1 F2 for every group (G, [PairSpec, ...]) over all bins,
+    with one shared shell-field cache; returns one DeferredPairSums per group
+    (``result()`` gives complex arrays k_bins x k_bins, or k_bins in diagonal
+    mode).
 
     Bins are processed in blocks of ``block_size`` rows x columns so that at most
     the fields of one row block and one column block are resident
     (clustering_estimator.py:911-981 bounds memory the same way).
     """
-    out = DeferredPairSums(pair_specs, k_bins, diagonal)
+    outs = [DeferredPairSums(specs, k_bins, diagonal) for (_, specs) in groups]
     bs = k_bins if block_size is None else int(block_size)
     blocks = [list(range(b0, min(k_bins, b0 + bs))) for b0 in range(0, k_bins, bs)]
     for bi in blocks:
-        row_keys = []
-        for ps in pair_specs:
-            row_keys += ps.row_keys(sf, bi)
-        row_keys = list(dict.fromkeys(row_keys))
+        rows_g = []
+        for (_, specs) in groups:
+            rk = []
+            for ps in specs:
+                rk += ps.row_keys(sf, bi)
+            rows_g.append(list(dict.fromkeys(rk)))
         col_blocks = [bi] if diagonal else blocks
         for bj in col_blocks:
-            col_keys = []
-            for ps in pair_specs:
-                col_keys += ps.col_keys(sf, bj)
-            col_keys = list(dict.fromkeys(col_keys))
-            keep = set(row_keys) | set(col_keys)
+            cols_g = []
+            for (_, specs) in groups:
+                ck = []
+                for ps in specs:
+                    ck += ps.col_keys(sf, bj)
+                cols_g.append(list(dict.fromkeys(ck)))
+            keep = set().union(*rows_g, *cols_g)
             sf.release([k for k in list(sf.slot) if k not in keep])
-            sf.ensure(row_keys + col_keys)
-            out.add(contract(G, sf, row_keys, col_keys), row_keys, col_keys, bi, bj)
+            sf.ensure([k for r in rows_g for k in r] + [k for c in cols_g for k in c])
+            for gi, (G, _) in enumerate(groups):
+                outs[gi].add(contract(G, sf, rows_g[gi], cols_g[gi]), rows_g[gi], cols_g[gi], bi, bj)
         sf.release_all()
-    return out
+    return outs
 
 
 def fields_capacity(n, precision, want, reserve_bytes=0):
