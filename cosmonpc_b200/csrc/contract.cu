@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
     __shared__ int abort_flag;
     const int nf = P.nunion + 1;  // staged rows: G then the union fields
     const int64_t stage_elems = (int64_t)nf * P.chunk;
-    T *stage[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + stage_elems};
+    T *const stage0 = reinterpret_cast<T *>(smem_raw);
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
         mbar_expect_tx(&bars[s], bytes * (uint32_t)nf);
         for (int u = 0; u < nf; ++u) {
             const T *src = u == 0 ? g + c0 : fields + (int64_t)P.union_field[u - 1] * P.field_stride + c0;
-            bulk_g2s(stage[s] + (int64_t)u * P.chunk, src, bytes, &bars[s]);
+            bulk_g2s(stage0 + s * stage_elems + (int64_t)u * P.chunk, src, bytes, &bars[s]);
         }
     };
 
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
     for (int64_t c0 = first; c0 < P.ncell; c0 += step, ++it) {
         const int s = it & 1;
         const int64_t valid = min((int64_t)P.chunk, P.ncell - c0);
-        T *sb = stage[s];
+        T *sb = stage0 + s * stage_elems;
         if (use_async) {
             // prefetch the next chunk into the other stage (freed by the
             // __syncthreads at the end of the previous iteration)
