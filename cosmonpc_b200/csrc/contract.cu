@@ -39,7 +39,7 @@ template <> struct TileShape<float> { static constexpr int TM = 8, TN = 8; };
 template <> struct TileShape<double> { static constexpr int TM = 8, TN = 4; };
 
 struct GramParams {
-    int na, nb, nunion, ct, ntiles, ngroups, chunk, flush_chunks, async_ok;
+    int na, nb, nunion, ct, ntiles, ngroups, chunk, flush_chunks;
     int64_t ncell, field_stride;
     int a_slot[kMaxRows];
     int b_slot[kMaxRows];
@@ -101,6 +101,28 @@ __device__ inline void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint
 }
 __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+__device__ inline void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+constexpr int kStages = 4;
+
+// Tiles handled by block group g and the warp -> (tile, phase) map: the tiles
+// of a group are spread over the 16 warps; a tile with several warps splits
+// its cells between them (phase p of n takes every n-th 32-cell slice).
+struct WarpWork {
+    int tile, phase, nphase;
+};
+__device__ inline WarpWork warp_work(int group, int warp, int ntiles) {
+    const int t0 = group * kWarps;
+    const int nt = min(kWarps, ntiles - t0);
+    WarpWork w;
+    w.tile = t0 + warp % nt;
+    w.phase = warp / nt;
+    w.nphase = (kWarps - 1 - warp % nt) / nt + 1;
+    return w;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
                                                         const T *__restrict__ fields,
@@ -109,8 +131,9 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
     constexpr int TM = TileShape<T>::TM, TN = TileShape<T>::TN, NV = TM * TN;
     constexpr int PER_LANE = NV / 32;  // tile elements owned by a lane after the fold
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bars[2];
-    __shared__ int abort_flag;
+    __shared__ __align__(8) uint64_t full_bar[kStages];
+    __shared__ __align__(8) uint64_t empty_bar[kStages];
+    __shared__ volatile int abort_flag;
     const int nf = P.nunion + 1;  // staged rows: G then the union fields
     const int64_t stage_elems = (int64_t)nf * P.chunk;
     T *const stage0 = reinterpret_cast<T *>(smem_raw);
@@ -120,10 +143,9 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
     const int group = blockIdx.x % P.ngroups;
     const int xr = blockIdx.x / P.ngroups;
     const int nxr = gridDim.x / P.ngroups;
-    const int tile = group * kWarps + warp;
-    const bool active = tile < P.ntiles;
-    const int rt = active ? tile / P.ct : 0;
-    const int cti = active ? tile % P.ct : 0;
+    const WarpWork ww = warp_work(group, warp, P.ntiles);
+    const int rt = ww.tile / P.ct;
+    const int cti = ww.tile % P.ct;
 
     int rs[TM], cs[TN];
 #pragma unroll
@@ -140,121 +162,113 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
 
     const int64_t first = (int64_t)xr * P.chunk;
     const int64_t step = (int64_t)nxr * P.chunk;
-    const bool use_async = P.async_ok != 0;
+    const int nchunk = first < P.ncell ? (int)((P.ncell - first + step - 1) / step) : 0;
+    const bool producer = threadIdx.x == 0;
 
-    // issue the bulk copies of the chunk starting at c0 into stage s (one thread)
-    auto issue = [&](int64_t c0, int s) {
+    auto issue = [&](int k) {  // bulk copies of this block's k-th chunk
+        const int s = k % kStages;
+        const int64_t c0 = first + (int64_t)k * step;
         const int64_t valid = min((int64_t)P.chunk, P.ncell - c0);
         const uint32_t bytes = (uint32_t)(valid * sizeof(T));
+        T *dst = stage0 + s * stage_elems;
         fence_proxy_async();
-        mbar_expect_tx(&bars[s], bytes * (uint32_t)nf);
+        mbar_expect_tx(&full_bar[s], bytes * (uint32_t)nf);
         for (int u = 0; u < nf; ++u) {
             const T *src = u == 0 ? g + c0 : fields + (int64_t)P.union_field[u - 1] * P.field_stride + c0;
-            bulk_g2s(stage0 + s * stage_elems + (int64_t)u * P.chunk, src, bytes, &bars[s]);
+            bulk_g2s(dst + (int64_t)u * P.chunk, src, bytes, &full_bar[s]);
         }
     };
 
-    if (threadIdx.x == 0) {
+    if (producer) {
         abort_flag = 0;
-        if (use_async) {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], kWarps);
         }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (use_async && threadIdx.x == 0 && first < P.ncell) issue(first, 0);
+    int issued = 0;
+    if (producer)
+        for (; issued < min(nchunk, kStages - 1); ++issued) issue(issued);
 
     int since_flush = 0;
-    int it = 0;
-    int64_t issued_last = first;  // start of the newest chunk whose copies were issued
-    for (int64_t c0 = first; c0 < P.ncell; c0 += step, ++it) {
-        const int s = it & 1;
-        const int64_t valid = min((int64_t)P.chunk, P.ncell - c0);
-        T *sb = stage0 + s * stage_elems;
-        if (use_async) {
-            // prefetch the next chunk into the other stage (freed by the
-            // __syncthreads at the end of the previous iteration)
-            if (threadIdx.x == 0 && c0 + step < P.ncell && !abort_flag) {
-                issue(c0 + step, s ^ 1);
-                issued_last = c0 + step;
-            }
-            if (threadIdx.x == 0) {
-                if (!mbar_wait_bounded(&bars[s], (uint32_t)((it >> 1) & 1))) {
-                    abort_flag = 1;
-                    atomicExch(status, (int)CNPC_ETIMEOUT);
-                }
-            }
-            __syncthreads();
-            if (abort_flag) break;
-            // the other threads observe the completed phase through the barrier
-            // wait of thread 0 plus __syncthreads; re-check the phase locally to
-            // get acquire semantics on the copied bytes
-            mbar_try_wait(&bars[s], (uint32_t)((it >> 1) & 1));
-        } else {
-            __syncthreads();
-            for (int idx = threadIdx.x; idx < nf * P.chunk; idx += kThreads) {
-                const int u = idx / P.chunk, c = idx % P.chunk;
-                const int64_t cell = c0 + c;
-                T v = (T)0;
-                if (cell < P.ncell)
-                    v = u == 0 ? g[cell] : fields[(int64_t)P.union_field[u - 1] * P.field_stride + cell];
-                sb[(int64_t)u * P.chunk + c] = v;
-            }
-            __syncthreads();
-        }
-        if (active) {
-            for (int c = lane; c < valid; c += 32) {
-                const T gv = sb[c];
-                T av[TM], bv[TN];
-#pragma unroll
-                for (int r = 0; r < TM; ++r) av[r] = gv * sb[rs[r] + c];
-#pragma unroll
-                for (int q = 0; q < TN; ++q) bv[q] = sb[cs[q] + c];
-#pragma unroll
-                for (int r = 0; r < TM; ++r)
-#pragma unroll
-                    for (int q = 0; q < TN; ++q) acc[r * TN + q] += av[r] * bv[q];
-            }
-            if (sizeof(T) == 4 && ++since_flush == P.flush_chunks) {
-                since_flush = 0;
-                TransposeReduce<T, NV, 16>::run(acc, lane);
-#pragma unroll
-                for (int e = 0; e < PER_LANE; ++e) acc64[e] += (double)acc[e];
-#pragma unroll
-                for (int e = 0; e < NV; ++e) acc[e] = (T)0;
+    int k = 0;
+    for (; k < nchunk; ++k) {
+        const int s = k % kStages;
+        // producer: refill the stage freed by chunk k-1 with chunk k+kStages-1
+        if (producer && issued < nchunk && !abort_flag) {
+            const int sp = issued % kStages;
+            if (issued >= kStages && !mbar_wait_bounded(&empty_bar[sp], (uint32_t)(((issued / kStages) - 1) & 1))) {
+                abort_flag = 1;
+                atomicExch(status, (int)CNPC_ETIMEOUT);
+            } else {
+                issue(issued);
+                ++issued;
             }
         }
-        __syncthreads();  // every warp is done with stage s before it is refilled
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / kStages) & 1))) {
+            abort_flag = 1;
+            if (lane == 0) atomicExch(status, (int)CNPC_ETIMEOUT);
+        }
+        if (abort_flag) break;
+        const T *sb = stage0 + s * stage_elems;
+        const int64_t valid = min((int64_t)P.chunk, P.ncell - (first + (int64_t)k * step));
+        const int cstep = 32 * ww.nphase;
+        for (int c = lane + 32 * ww.phase; c < (int)valid; c += cstep) {
+            const T gv = sb[c];
+            T av[TM], bv[TN];
+#pragma unroll
+            for (int r = 0; r < TM; ++r) av[r] = gv * sb[rs[r] + c];
+#pragma unroll
+            for (int q = 0; q < TN; ++q) bv[q] = sb[cs[q] + c];
+#pragma unroll
+            for (int r = 0; r < TM; ++r)
+#pragma unroll
+                for (int q = 0; q < TN; ++q) acc[r * TN + q] += av[r] * bv[q];
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty_bar[s]);
+        if (sizeof(T) == 4 && ++since_flush == P.flush_chunks) {
+            since_flush = 0;
+            TransposeReduce<T, NV, 16>::run(acc, lane);
+#pragma unroll
+            for (int e = 0; e < PER_LANE; ++e) acc64[e] += (double)acc[e];
+#pragma unroll
+            for (int e = 0; e < NV; ++e) acc[e] = (T)0;
+        }
     }
-    if (use_async && abort_flag && threadIdx.x == 0) {
-        // drain the copies this block still has in flight (bounded) before
-        // exit: the chunk whose wait gave up and the newest prefetched chunk
-        mbar_wait_bounded(&bars[it & 1], (uint32_t)((it >> 1) & 1));
-        const int itl = (int)((issued_last - first) / step);
-        if (itl != it) mbar_wait_bounded(&bars[itl & 1], (uint32_t)((itl >> 1) & 1));
+    if (abort_flag && producer) {
+        // drain the copies still in flight (bounded) before the block exits
+        for (int j = k; j < issued; ++j) mbar_wait_bounded(&full_bar[j % kStages], (uint32_t)((j / kStages) & 1));
     }
-    __syncthreads();
-    if (!active) return;
     TransposeReduce<T, NV, 16>::run(acc, lane);
 #pragma unroll
     for (int e = 0; e < PER_LANE; ++e) acc64[e] += (double)acc[e];
-    double *dst = partial + ((int64_t)xr * P.ntiles + tile) * NV;
+    // per-warp partials: [block][warp][NV]
+    double *dst = partial + ((int64_t)blockIdx.x * kWarps + warp) * NV;
     const double nanv = __longlong_as_double(0x7ff8000000000000ll);
+    const bool bad = abort_flag != 0;
 #pragma unroll
-    for (int e = 0; e < PER_LANE; ++e) dst[lane * PER_LANE + e] = abort_flag ? nanv : acc64[e];
+    for (int e = 0; e < PER_LANE; ++e) dst[lane * PER_LANE + e] = bad ? nanv : acc64[e];
 }
 
+// out[i, j] = sum over every block of the group owning tile(i, j) and every
+// warp of that block assigned to the tile, in a fixed order.
 template <int TM, int TN>
-__global__ void gram_reduce_kernel(const double *partial, int nxr, int ntiles, int ct, int na, int nb,
-                                   double *out) {
+__global__ void gram_reduce_kernel(const double *partial, int nblocks, int ngroups, int ntiles, int ct,
+                                   int na, int nb, double *out) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= na * nb) return;
     const int i = o / nb, j = o % nb;
     const int tile = (i / TM) * ct + (j / TN);
     const int e = (i % TM) * TN + (j % TN);
+    const int group = tile / kWarps;
+    const int nt = min(kWarps, ntiles - group * kWarps);
+    const int local = tile - group * kWarps;
     double s = 0.0;
-    for (int x = 0; x < nxr; ++x) s += partial[((int64_t)x * ntiles + tile) * (TM * TN) + e];
+    for (int b = group; b < nblocks; b += ngroups)
+        for (int w = local; w < kWarps; w += nt) s += partial[((int64_t)b * kWarps + w) * (TM * TN) + e];
     out[o] = s;
 }
 
@@ -287,35 +301,33 @@ static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, i
     P.ncell = ncell;
     P.field_stride = stride;
     // bulk copies need 16-byte aligned sources and byte counts
-    P.async_ok = ((stride * sizeof(T)) % 16 == 0) && ((ncell * sizeof(T)) % 16 == 0) &&
-                 ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0);
-    // two stages of (G + union rows) x chunk in ~100 KB of shared memory
-    const size_t budget = 100 * 1024;
-    int chunk = (int)(budget / (2 * (size_t)(P.nunion + 1) * sizeof(T)));
+    CNPC_REQUIRE(ctx, ((stride * sizeof(T)) % 16 == 0) && ((ncell * sizeof(T)) % 16 == 0) &&
+                          ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0),
+                 "contraction needs 16-byte aligned fields, field_stride and ncell");
+    // kStages x (G + union rows) x chunk in ~200 KB of shared memory (1 block/SM)
+    const size_t budget = 200 * 1024;
+    int chunk = (int)(budget / (kStages * (size_t)(P.nunion + 1) * sizeof(T)));
     chunk = std::min(1024, chunk) / 32 * 32;
-    if (chunk < 32) chunk = 32;
+    CNPC_REQUIRE(ctx, chunk >= 32, "too many distinct fields for the shared-memory stages");
     P.chunk = chunk;
     P.flush_chunks = std::max(1, 2048 / chunk);  // ~64 cells per lane per FP32 partial
-    const size_t smem = 2 * (size_t)(P.nunion + 1) * chunk * sizeof(T);
+    const size_t smem = (size_t)kStages * (P.nunion + 1) * chunk * sizeof(T);
     int st = check_cuda(ctx, cudaFuncSetAttribute(gram_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem), "gram smem attribute");
     if (st) return st;
     const int64_t nchunks = (ncell + chunk - 1) / chunk;
-    int per_sm = (int)std::max<size_t>(1, (220 * 1024) / std::max<size_t>(smem + 1024, 1));
-    per_sm = std::min(per_sm, 2);
-    int64_t nxr = std::max<int64_t>(1, (int64_t)ctx->num_sms * per_sm / P.ngroups);
-    nxr = std::min<int64_t>(nxr, nchunks);
-    const size_t partial_bytes = (size_t)nxr * P.ntiles * TM * TN * sizeof(double) + 256;
+    int64_t nxr = std::min<int64_t>(std::max<int64_t>(1, ctx->num_sms / P.ngroups), nchunks);
+    const int nblocks = (int)(nxr * P.ngroups);
+    const size_t partial_bytes = (size_t)nblocks * kWarps * TM * TN * sizeof(double) + 256;
     st = ensure_scratch(ctx, partial_bytes, s);
     if (st) return st;
     int *status = reinterpret_cast<int *>(static_cast<char *>(ctx->scratch) + ctx->scratch_bytes - 256);
-    gram_kernel<T><<<(unsigned)(nxr * P.ngroups), kThreads, smem, s>>>(g, fields, P, (double *)ctx->scratch,
-                                                                        status);
+    gram_kernel<T><<<(unsigned)nblocks, kThreads, smem, s>>>(g, fields, P, (double *)ctx->scratch, status);
     st = check_launch(ctx, "gram_kernel");
     if (st) return st;
     const int nout = na * nb;
-    gram_reduce_kernel<TM, TN><<<(nout + 127) / 128, 128, 0, s>>>((const double *)ctx->scratch, (int)nxr,
-                                                                  P.ntiles, P.ct, na, nb, out);
+    gram_reduce_kernel<TM, TN><<<(nout + 127) / 128, 128, 0, s>>>((const double *)ctx->scratch, nblocks,
+                                                                  P.ngroups, P.ntiles, P.ct, na, nb, out);
     return check_launch(ctx, "gram_reduce_kernel");
 }
 
