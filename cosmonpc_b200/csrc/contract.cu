@@ -28,18 +28,13 @@
 
 namespace cnpc {
 
-constexpr int kWarps = 16;
-constexpr int kThreads = kWarps * 32;
 constexpr int kMaxRows = 128;
-constexpr int kMaxUnion = 256;
+constexpr int kMaxUnion = 264;
 constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up (~seconds)
 
-template <typename T> struct TileShape;
-template <> struct TileShape<float> { static constexpr int TM = 8, TN = 8; };
-template <> struct TileShape<double> { static constexpr int TM = 8, TN = 4; };
 
 struct GramParams {
-    int na, nb, nunion, ct, ntiles, ngroups, chunk, flush_chunks;
+    int na, nb, nunion, ncopy, g_row, ct, ntiles, ngroups, flush_chunks, nstages;
     int64_t ncell, field_stride;
     int a_slot[kMaxRows];
     int b_slot[kMaxRows];
@@ -105,37 +100,121 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-constexpr int kStages = 4;
+constexpr int kMaxStages = 4;
 
-// Tiles handled by block group g and the warp -> (tile, phase) map: the tiles
-// of a group are spread over the 16 warps; a tile with several warps splits
-// its cells between them (phase p of n takes every n-th 32-cell slice).
+// Chunk (cells per staged row) is a compile-time constant so that every
+// shared-memory operand offset in the inner loop is an immediate.
+template <typename T> struct ChunkOf;
+template <> struct ChunkOf<float> { static constexpr int C = 256; };
+template <> struct ChunkOf<double> { static constexpr int C = 128; };
+
+// Block group g owns tiles [16g, 16g + nt); warp w works on tile 16g + (w % nt)
+// and, when several warps share a tile, takes every nphase-th slice of cells.
 struct WarpWork {
     int tile, phase, nphase;
 };
-__device__ inline WarpWork warp_work(int group, int warp, int ntiles) {
-    const int t0 = group * kWarps;
-    const int nt = min(kWarps, ntiles - t0);
+__device__ inline WarpWork warp_work(int group, int warp, int nwarps, int ntiles) {
+    const int t0 = group * nwarps;
+    const int nt = min(nwarps, ntiles - t0);
     WarpWork w;
     w.tile = t0 + warp % nt;
     w.phase = warp / nt;
-    w.nphase = (kWarps - 1 - warp % nt) / nt + 1;
+    w.nphase = (nwarps - 1 - warp % nt) / nt + 1;
     return w;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
-                                                        const T *__restrict__ fields,
-                                                        const GramParams P, double *partial,
-                                                        int *status) {
-    constexpr int TM = TileShape<T>::TM, TN = TileShape<T>::TN, NV = TM * TN;
-    constexpr int PER_LANE = NV / 32;  // tile elements owned by a lane after the fold
+// FP32 tile step: a lane takes two adjacent cells; row operands are float2
+// (cell c, c+1) and the 8x8 accumulators are float2 (even-cell, odd-cell
+// partial sums) updated with packed FP32x2 FMAs.
+struct Fp32Tile {
+    static constexpr int TM = 8, TN = 8, NV = 64, WARPS = 8, CHUNK = 256;
+    float2 acc[TM][TN];
+    __device__ void zero() {
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[r][q] = make_float2(0.f, 0.f);
+    }
+    // rowG, rowA, rowB: staged chunk rows (G, first A row of the tile, first B row)
+    __device__ void step(const float *rowG, const float *rowA, const float *rowB, int c) {
+        const float2 g2 = *reinterpret_cast<const float2 *>(rowG + c);
+        float2 a2[TM], b2[TN];
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+            a2[r] = __fmul2_rn(g2, *reinterpret_cast<const float2 *>(rowA + r * CHUNK + c));
+#pragma unroll
+        for (int q = 0; q < TN; ++q) b2[q] = *reinterpret_cast<const float2 *>(rowB + q * CHUNK + c);
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[r][q] = __ffma2_rn(a2[r], b2[q], acc[r][q]);
+    }
+    __device__ void fold(double *acc64, int lane) {
+        float v[NV];
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) v[r * TN + q] = acc[r][q].x + acc[r][q].y;
+        TransposeReduce<float, NV, 16>::run(v, lane);
+        acc64[0] += (double)v[0];
+        acc64[1] += (double)v[1];
+        zero();
+    }
+};
+
+// FP64 tile step: one cell per lane, 8x4 accumulators in FP64.
+struct Fp64Tile {
+    static constexpr int TM = 8, TN = 4, NV = 32, WARPS = 16, CHUNK = 128;
+    double acc[TM][TN];
+    __device__ void zero() {
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[r][q] = 0.0;
+    }
+    __device__ void step(const double *rowG, const double *rowA, const double *rowB, int c) {
+        const double gv = rowG[c];
+        double av[TM], bv[TN];
+#pragma unroll
+        for (int r = 0; r < TM; ++r) av[r] = gv * rowA[r * CHUNK + c];
+#pragma unroll
+        for (int q = 0; q < TN; ++q) bv[q] = rowB[q * CHUNK + c];
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[r][q] = fma(av[r], bv[q], acc[r][q]);
+    }
+    __device__ void fold(double *acc64, int lane) {
+        double v[NV];
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) v[r * TN + q] = acc[r][q];
+        TransposeReduce<double, NV, 16>::run(v, lane);
+        acc64[0] += v[0];
+        zero();
+    }
+};
+
+template <typename T> struct TileOf;
+template <> struct TileOf<float> { using type = Fp32Tile; };
+template <> struct TileOf<double> { using type = Fp64Tile; };
+
+template <typename T, int NWARPS>
+__global__ void __launch_bounds__(NWARPS * 32, 1)
+    gram_kernel(const T *__restrict__ g, const T *__restrict__ fields, const GramParams P, double *partial,
+                int *status) {
+    using Tile = typename TileOf<T>::type;
+    constexpr int TM = Tile::TM, TN = Tile::TN, NV = Tile::NV, NW = Tile::WARPS, CHUNK = Tile::CHUNK;
+    constexpr int CPL = sizeof(T) == 4 ? 2 : 1;  // cells per lane per step
+    constexpr int PER_LANE = NV / 32;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kStages];
-    __shared__ __align__(8) uint64_t empty_bar[kStages];
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages];
+    __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
     __shared__ volatile int abort_flag;
-    const int nf = P.nunion + 1;  // staged rows: G then the union fields
-    const int64_t stage_elems = (int64_t)nf * P.chunk;
+    const int NST = P.nstages;
+    const int nf = P.nunion;  // staged rows (G, A rows, separate B rows), see run_gram
+    const int stage_elems = nf * CHUNK;
     T *const stage0 = reinterpret_cast<T *>(smem_raw);
 
     const int lane = threadIdx.x & 31;
@@ -143,63 +222,58 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
     const int group = blockIdx.x % P.ngroups;
     const int xr = blockIdx.x / P.ngroups;
     const int nxr = gridDim.x / P.ngroups;
-    const WarpWork ww = warp_work(group, warp, P.ntiles);
-    const int rt = ww.tile / P.ct;
-    const int cti = ww.tile % P.ct;
+    const WarpWork ww = warp_work(group, warp, NW, P.ntiles);
+    const int a_row = P.a_slot[(ww.tile / P.ct) * TM];   // first staged row of this tile's A rows
+    const int b_row = P.b_slot[(ww.tile % P.ct) * TN];   // first staged row of its B rows
 
-    int rs[TM], cs[TN];
-#pragma unroll
-    for (int r = 0; r < TM; ++r) rs[r] = P.a_slot[min(rt * TM + r, P.na - 1)] * P.chunk;
-#pragma unroll
-    for (int c = 0; c < TN; ++c) cs[c] = P.b_slot[min(cti * TN + c, P.nb - 1)] * P.chunk;
-
-    T acc[NV];
-#pragma unroll
-    for (int e = 0; e < NV; ++e) acc[e] = (T)0;
+    Tile tile;
+    tile.zero();
     double acc64[PER_LANE];
 #pragma unroll
     for (int e = 0; e < PER_LANE; ++e) acc64[e] = 0.0;
 
-    const int64_t first = (int64_t)xr * P.chunk;
-    const int64_t step = (int64_t)nxr * P.chunk;
+    const int64_t first = (int64_t)xr * CHUNK;
+    const int64_t step = (int64_t)nxr * CHUNK;
     const int nchunk = first < P.ncell ? (int)((P.ncell - first + step - 1) / step) : 0;
     const bool producer = threadIdx.x == 0;
 
     auto issue = [&](int k) {  // bulk copies of this block's k-th chunk
-        const int s = k % kStages;
+        const int s = k % NST;
         const int64_t c0 = first + (int64_t)k * step;
-        const int64_t valid = min((int64_t)P.chunk, P.ncell - c0);
+        const int64_t valid = min((int64_t)CHUNK, P.ncell - c0);
         const uint32_t bytes = (uint32_t)(valid * sizeof(T));
         T *dst = stage0 + s * stage_elems;
         fence_proxy_async();
-        mbar_expect_tx(&full_bar[s], bytes * (uint32_t)nf);
+        mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
         for (int u = 0; u < nf; ++u) {
-            const T *src = u == 0 ? g + c0 : fields + (int64_t)P.union_field[u - 1] * P.field_stride + c0;
-            bulk_g2s(dst + (int64_t)u * P.chunk, src, bytes, &full_bar[s]);
+            const int f = P.union_field[u];
+            if (f == -1) continue;  // padding row: never read into a kept output
+            const T *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
+            bulk_g2s(dst + u * CHUNK, src, bytes, &full_bar[s]);
         }
     };
 
     if (producer) {
         abort_flag = 0;
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < NST; ++s) {
             mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], kWarps);
+            mbar_init(&empty_bar[s], NW);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     int issued = 0;
     if (producer)
-        for (; issued < min(nchunk, kStages - 1); ++issued) issue(issued);
+        for (; issued < min(nchunk, NST - 1); ++issued) issue(issued);
 
     int since_flush = 0;
     int k = 0;
     for (; k < nchunk; ++k) {
-        const int s = k % kStages;
-        // producer: refill the stage freed by chunk k-1 with chunk k+kStages-1
+        const int s = k % NST;
         if (producer && issued < nchunk && !abort_flag) {
-            const int sp = issued % kStages;
-            if (issued >= kStages && !mbar_wait_bounded(&empty_bar[sp], (uint32_t)(((issued / kStages) - 1) & 1))) {
+            const int sp = issued % NST;
+            if (issued >= NST &&
+                !mbar_wait_bounded(&empty_bar[sp], (uint32_t)(((issued / NST) - 1) & 1))) {
                 abort_flag = 1;
                 atomicExch(status, (int)CNPC_ETIMEOUT);
             } else {
@@ -207,46 +281,30 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
                 ++issued;
             }
         }
-        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / kStages) & 1))) {
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / NST) & 1))) {
             abort_flag = 1;
             if (lane == 0) atomicExch(status, (int)CNPC_ETIMEOUT);
         }
         if (abort_flag) break;
         const T *sb = stage0 + s * stage_elems;
-        const int64_t valid = min((int64_t)P.chunk, P.ncell - (first + (int64_t)k * step));
-        const int cstep = 32 * ww.nphase;
-        for (int c = lane + 32 * ww.phase; c < (int)valid; c += cstep) {
-            const T gv = sb[c];
-            T av[TM], bv[TN];
-#pragma unroll
-            for (int r = 0; r < TM; ++r) av[r] = gv * sb[rs[r] + c];
-#pragma unroll
-            for (int q = 0; q < TN; ++q) bv[q] = sb[cs[q] + c];
-#pragma unroll
-            for (int r = 0; r < TM; ++r)
-#pragma unroll
-                for (int q = 0; q < TN; ++q) acc[r * TN + q] += av[r] * bv[q];
-        }
+        const int valid = (int)min((int64_t)CHUNK, P.ncell - (first + (int64_t)k * step));
+        const T *rowG = sb + P.g_row * CHUNK;
+        const T *rowA = sb + a_row * CHUNK;
+        const T *rowB = sb + b_row * CHUNK;
+        for (int c = CPL * (lane + 32 * ww.phase); c < valid; c += CPL * 32 * ww.nphase)
+            tile.step(rowG, rowA, rowB, c);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty_bar[s]);
-        if (sizeof(T) == 4 && ++since_flush == P.flush_chunks) {
+        if (++since_flush == P.flush_chunks) {
             since_flush = 0;
-            TransposeReduce<T, NV, 16>::run(acc, lane);
-#pragma unroll
-            for (int e = 0; e < PER_LANE; ++e) acc64[e] += (double)acc[e];
-#pragma unroll
-            for (int e = 0; e < NV; ++e) acc[e] = (T)0;
+            tile.fold(acc64, lane);
         }
     }
     if (abort_flag && producer) {
-        // drain the copies still in flight (bounded) before the block exits
-        for (int j = k; j < issued; ++j) mbar_wait_bounded(&full_bar[j % kStages], (uint32_t)((j / kStages) & 1));
+        for (int j = k; j < issued; ++j) mbar_wait_bounded(&full_bar[j % NST], (uint32_t)((j / NST) & 1));
     }
-    TransposeReduce<T, NV, 16>::run(acc, lane);
-#pragma unroll
-    for (int e = 0; e < PER_LANE; ++e) acc64[e] += (double)acc[e];
-    // per-warp partials: [block][warp][NV]
-    double *dst = partial + ((int64_t)blockIdx.x * kWarps + warp) * NV;
+    tile.fold(acc64, lane);
+    double *dst = partial + ((int64_t)blockIdx.x * NW + warp) * NV;
     const double nanv = __longlong_as_double(0x7ff8000000000000ll);
     const bool bad = abort_flag != 0;
 #pragma unroll
@@ -255,7 +313,7 @@ __global__ void __launch_bounds__(kThreads) gram_kernel(const T *__restrict__ g,
 
 // out[i, j] = sum over every block of the group owning tile(i, j) and every
 // warp of that block assigned to the tile, in a fixed order.
-template <int TM, int TN>
+template <int TM, int TN, int NW>
 __global__ void gram_reduce_kernel(const double *partial, int nblocks, int ngroups, int ntiles, int ct,
                                    int na, int nb, double *out) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,71 +321,81 @@ __global__ void gram_reduce_kernel(const double *partial, int nblocks, int ngrou
     const int i = o / nb, j = o % nb;
     const int tile = (i / TM) * ct + (j / TN);
     const int e = (i % TM) * TN + (j % TN);
-    const int group = tile / kWarps;
-    const int nt = min(kWarps, ntiles - group * kWarps);
-    const int local = tile - group * kWarps;
+    const int group = tile / NW;
+    const int nt = min(NW, ntiles - group * NW);
+    const int local = tile - group * NW;
     double s = 0.0;
     for (int b = group; b < nblocks; b += ngroups)
-        for (int w = local; w < kWarps; w += nt) s += partial[((int64_t)b * kWarps + w) * (TM * TN) + e];
+        for (int w = local; w < NW; w += nt) s += partial[((int64_t)b * NW + w) * (TM * TN) + e];
     out[o] = s;
 }
 
 template <typename T>
 static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, int64_t stride,
                     const int *a, int na, const int *b, int nb, double *out, cudaStream_t s) {
-    constexpr int TM = TileShape<T>::TM, TN = TileShape<T>::TN;
+    using Tile = typename TileOf<T>::type;
+    constexpr int TM = Tile::TM, TN = Tile::TN, NW = Tile::WARPS, CHUNK = Tile::CHUNK;
     GramParams P;
     std::memset(&P, 0, sizeof(P));
     P.na = na;
     P.nb = nb;
-    std::map<int, int> slot;
-    for (int i = 0; i < na; ++i) {
-        auto it = slot.find(a[i]);
-        if (it == slot.end()) it = slot.emplace(a[i], (int)slot.size()).first;
-        P.a_slot[i] = it->second + 1;  // slot 0 is G
+    // staged rows: [G][A rows padded to TM][B rows padded to TN unless B is a
+    // contiguous run of A], so each tile's rows are consecutive
+    const int na_pad = (na + TM - 1) / TM * TM;
+    const int nb_pad = (nb + TN - 1) / TN * TN;
+    int b_off = -1;
+    for (int off = 0; off + nb <= na && b_off < 0; ++off) {
+        bool same = true;
+        for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
+        // the padded columns must also stay inside the staged rows
+        if (same && off + nb_pad <= na_pad) b_off = off;
     }
-    for (int j = 0; j < nb; ++j) {
-        auto it = slot.find(b[j]);
-        if (it == slot.end()) it = slot.emplace(b[j], (int)slot.size()).first;
-        P.b_slot[j] = it->second + 1;
+    std::vector<int> rows;
+    rows.push_back(-2);  // G
+    for (int i = 0; i < na_pad; ++i) rows.push_back(i < na ? a[i] : -1);
+    int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
+    if (b_off < 0)
+        for (int j = 0; j < nb_pad; ++j) rows.push_back(j < nb ? b[j] : -1);
+    CNPC_REQUIRE(ctx, (int)rows.size() <= kMaxUnion, "too many staged rows (max 256)");
+    P.nunion = (int)rows.size();
+    P.ncopy = 0;
+    for (int u = 0; u < P.nunion; ++u) {
+        P.union_field[u] = rows[u];
+        if (rows[u] != -1) ++P.ncopy;
     }
-    CNPC_REQUIRE(ctx, (int)slot.size() <= kMaxUnion, "too many distinct fields (max 256)");
-    P.nunion = (int)slot.size();
-    for (auto &kv : slot) P.union_field[kv.second] = kv.first;
-    const int rtiles = (na + TM - 1) / TM;
-    P.ct = (nb + TN - 1) / TN;
+    P.g_row = 0;
+    for (int i = 0; i < na; ++i) P.a_slot[i] = 1 + i;
+    for (int j = 0; j < nb; ++j) P.b_slot[j] = b_base + j;
+    const int rtiles = na_pad / TM;
+    P.ct = nb_pad / TN;
     P.ntiles = rtiles * P.ct;
-    P.ngroups = (P.ntiles + kWarps - 1) / kWarps;
+    P.ngroups = (P.ntiles + NW - 1) / NW;
     P.ncell = ncell;
     P.field_stride = stride;
-    // bulk copies need 16-byte aligned sources and byte counts
     CNPC_REQUIRE(ctx, ((stride * sizeof(T)) % 16 == 0) && ((ncell * sizeof(T)) % 16 == 0) &&
                           ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0),
                  "contraction needs 16-byte aligned fields, field_stride and ncell");
-    // kStages x (G + union rows) x chunk in ~200 KB of shared memory (1 block/SM)
-    const size_t budget = 200 * 1024;
-    int chunk = (int)(budget / (kStages * (size_t)(P.nunion + 1) * sizeof(T)));
-    chunk = std::min(1024, chunk) / 32 * 32;
-    CNPC_REQUIRE(ctx, chunk >= 32, "too many distinct fields for the shared-memory stages");
-    P.chunk = chunk;
-    P.flush_chunks = std::max(1, 2048 / chunk);  // ~64 cells per lane per FP32 partial
-    const size_t smem = (size_t)kStages * (P.nunion + 1) * chunk * sizeof(T);
-    int st = check_cuda(ctx, cudaFuncSetAttribute(gram_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t row_bytes = (size_t)CHUNK * sizeof(T);
+    P.nstages = (int)std::min<size_t>(kMaxStages, (220 * 1024) / (P.nunion * row_bytes));
+    CNPC_REQUIRE(ctx, P.nstages >= 2, "too many staged rows for the shared-memory ring (max 110)");
+    const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
+    P.flush_chunks = sizeof(T) == 4 ? 8 : 1 << 30;  // FP32: ~64 cells per lane per partial
+    int st = check_cuda(ctx, cudaFuncSetAttribute(gram_kernel<T, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem), "gram smem attribute");
     if (st) return st;
-    const int64_t nchunks = (ncell + chunk - 1) / chunk;
+    const int64_t nchunks = (ncell + CHUNK - 1) / CHUNK;
     int64_t nxr = std::min<int64_t>(std::max<int64_t>(1, ctx->num_sms / P.ngroups), nchunks);
     const int nblocks = (int)(nxr * P.ngroups);
-    const size_t partial_bytes = (size_t)nblocks * kWarps * TM * TN * sizeof(double) + 256;
+    const size_t partial_bytes = (size_t)nblocks * NW * TM * TN * sizeof(double) + 256;
     st = ensure_scratch(ctx, partial_bytes, s);
     if (st) return st;
     int *status = reinterpret_cast<int *>(static_cast<char *>(ctx->scratch) + ctx->scratch_bytes - 256);
-    gram_kernel<T><<<(unsigned)nblocks, kThreads, smem, s>>>(g, fields, P, (double *)ctx->scratch, status);
+    gram_kernel<T, NW><<<(unsigned)nblocks, NW * 32, smem, s>>>(g, fields, P, (double *)ctx->scratch, status);
     st = check_launch(ctx, "gram_kernel");
     if (st) return st;
     const int nout = na * nb;
-    gram_reduce_kernel<TM, TN><<<(nout + 127) / 128, 128, 0, s>>>((const double *)ctx->scratch, nblocks,
-                                                                  P.ngroups, P.ntiles, P.ct, na, nb, out);
+    gram_reduce_kernel<TM, TN, NW><<<(nout + 127) / 128, 128, 0, s>>>(
+        (const double *)ctx->scratch, nblocks, P.ngroups, P.ntiles, P.ct, na, nb, out);
     return check_launch(ctx, "gram_reduce_kernel");
 }
 

@@ -198,8 +198,18 @@ class HostCopy:
         return self.host.numpy()
 
 
+def _staged_rows(nr, nc, shared):
+    pad = lambda x: (x + 7) // 8 * 8
+    return 1 + pad(nr) + (0 if shared else pad(nc))
+
+
 def contract(G, sf, rows, cols):
-    """Device tensor T[i, j] = sum_x G F_rows[i] F_cols[j] (FP64), enqueued only."""
+    """Device tensor T[i, j] = sum_x G F_rows[i] F_cols[j] (FP64), enqueued only.
+
+    One Gram launch stages G plus the row and column fields of a chunk of
+    cells; when the columns are a contiguous run of the rows they share the
+    staged rows.  Blocks of rows x columns are split so a launch stages at most
+    ~100 rows."""
     ctx = _lib.Context.get()
     ncell = sf.n ** 3
     dev = _device()
@@ -208,16 +218,26 @@ def contract(G, sf, rows, cols):
         return T
     ridx = [sf.slot[k] for k in rows]
     cidx = [sf.slot[k] for k in cols]
-    for r0 in range(0, len(ridx), 128):
-        for c0 in range(0, len(cidx), 128):
-            rr = ridx[r0:r0 + 128]
-            cc = cidx[c0:c0 + 128]
-            if r0 == 0 and c0 == 0 and len(rr) == len(ridx) and len(cc) == len(cidx):
-                ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, T)
-            else:
-                out = torch.empty((len(rr), len(cc)), dtype=torch.float64, device=dev)
-                ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
-                T[r0:r0 + len(rr), c0:c0 + len(cc)] = out
+
+    def shared(rr, cc):
+        for off in range(0, len(rr) - len(cc) + 1):
+            if rr[off:off + len(cc)] == cc:
+                return True
+        return False
+
+    if len(ridx) <= 128 and len(cidx) <= 128 and _staged_rows(len(ridx), len(cidx), shared(ridx, cidx)) <= 100:
+        blocks = [(0, len(ridx), 0, len(cidx))]
+    else:
+        blocks = [(r0, min(len(ridx), r0 + 48), c0, min(len(cidx), c0 + 48))
+                  for r0 in range(0, len(ridx), 48) for c0 in range(0, len(cidx), 48)]
+    for (r0, r1, c0, c1) in blocks:
+        rr, cc = ridx[r0:r1], cidx[c0:c1]
+        if (r1 - r0, c1 - c0) == (len(ridx), len(cidx)):
+            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, T)
+        else:
+            out = torch.empty((len(rr), len(cc)), dtype=torch.float64, device=dev)
+            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
+            T[r0:r1, c0:c1] = out
     return T
 
 
