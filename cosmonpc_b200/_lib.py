@@ -289,3 +289,4 @@ class Context:
         self._check(st, "cnpc_contract_gram")
         _count("gram")
         _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * _esz(dtype))
+        # (FP32 launches run on the tensor cores: gram_mma_kernel)

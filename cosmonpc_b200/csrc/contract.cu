@@ -123,45 +123,6 @@ __device__ inline WarpWork warp_work(int group, int warp, int nwarps, int ntiles
     return w;
 }
 
-// FP32 tile step: a lane takes two adjacent cells; row operands are float2
-// (cell c, c+1) and the 8x8 accumulators are float2 (even-cell, odd-cell
-// partial sums) updated with packed FP32x2 FMAs.
-struct Fp32Tile {
-    static constexpr int TM = 8, TN = 8, NV = 64, WARPS = 8, CHUNK = 256;
-    float2 acc[TM][TN];
-    __device__ void zero() {
-#pragma unroll
-        for (int r = 0; r < TM; ++r)
-#pragma unroll
-            for (int q = 0; q < TN; ++q) acc[r][q] = make_float2(0.f, 0.f);
-    }
-    // rowG, rowA, rowB: staged chunk rows (G, first A row of the tile, first B row)
-    __device__ void step(const float *rowG, const float *rowA, const float *rowB, int c) {
-        const float2 g2 = *reinterpret_cast<const float2 *>(rowG + c);
-        float2 a2[TM], b2[TN];
-#pragma unroll
-        for (int r = 0; r < TM; ++r)
-            a2[r] = __fmul2_rn(g2, *reinterpret_cast<const float2 *>(rowA + r * CHUNK + c));
-#pragma unroll
-        for (int q = 0; q < TN; ++q) b2[q] = *reinterpret_cast<const float2 *>(rowB + q * CHUNK + c);
-#pragma unroll
-        for (int r = 0; r < TM; ++r)
-#pragma unroll
-            for (int q = 0; q < TN; ++q) acc[r][q] = __ffma2_rn(a2[r], b2[q], acc[r][q]);
-    }
-    __device__ void fold(double *acc64, int lane) {
-        float v[NV];
-#pragma unroll
-        for (int r = 0; r < TM; ++r)
-#pragma unroll
-            for (int q = 0; q < TN; ++q) v[r * TN + q] = acc[r][q].x + acc[r][q].y;
-        TransposeReduce<float, NV, 16>::run(v, lane);
-        acc64[0] += (double)v[0];
-        acc64[1] += (double)v[1];
-        zero();
-    }
-};
-
 // FP64 tile step: one cell per lane, 8x4 accumulators in FP64.
 struct Fp64Tile {
     static constexpr int TM = 8, TN = 4, NV = 32, WARPS = 16, CHUNK = 128;
@@ -197,7 +158,6 @@ struct Fp64Tile {
 };
 
 template <typename T> struct TileOf;
-template <> struct TileOf<float> { using type = Fp32Tile; };
 template <> struct TileOf<double> { using type = Fp64Tile; };
 
 template <typename T, int NWARPS>
@@ -311,6 +271,264 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
     for (int e = 0; e < PER_LANE; ++e) dst[lane * PER_LANE + e] = bad ? nanv : acc64[e];
 }
 
+
+// ---------------------------------------------------------------------------
+// FP32 fields on the tensor cores.  The Gram is the GEMM
+//   C[a][b] = sum_k A[a][k] B[k][b],  A[a][k] = G(k) F_a(k),  B[k][b] = F_b(k)
+// with K = cells.  Each operand is split into two TF32 parts (x = hi + lo,
+// hi = rna_tf32(x), lo = rna_tf32(x - hi)) and C accumulates
+// Al*Bh + Ah*Bl + Ah*Bh with mma.sync m16n8k8 (FP32 accumulate): products
+// carry ~22 significant bits, as good as FP32 fields.  One warp owns the whole
+// (16 MT) x (8 NT) output for its 32 cells of every chunk; a dedicated producer
+// warp streams the chunks with cp.async.bulk into a ring guarded by full/empty
+// mbarriers.  The FP32 fragments are added into FP64 every 256 cells.
+constexpr int kMmaWarps = 8;               // consumer warps
+constexpr int kMmaChunk = 256;             // cells per staged row and chunk
+constexpr int kMmaStride = kMmaChunk + 4;  // padded row: conflict-free fragment loads
+constexpr int kMmaFlush = 8;               // chunks between FP64 folds
+
+__device__ inline uint32_t tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ inline void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - __uint_as_float(hi));
+}
+__device__ inline void mma_tf32(float *c, const uint32_t *a, const uint32_t *b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <int MT, int NT>
+__global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
+    gram_mma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
+                    double *partial, int *status) {
+    constexpr int MP = MT * 16, NP = NT * 8;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages];
+    __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
+    __shared__ volatile int abort_flag;
+    const int NST = P.nstages;
+    const int nf = P.nunion;
+    const int stage_elems = nf * kMmaStride;
+    float *const stage0 = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int64_t first = (int64_t)blockIdx.x * kMmaChunk;
+    const int64_t step = (int64_t)gridDim.x * kMmaChunk;
+    const int nchunk = first < P.ncell ? (int)((P.ncell - first + step - 1) / step) : 0;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < NST; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], kMmaWarps);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == kMmaWarps) {
+        // ---------------- producer warp: one lane issues every bulk copy
+        if (lane == 0) {
+            int issued = 0;
+            for (int k = 0; k < nchunk && !abort_flag; ++k) {
+                const int s = k % NST;
+                if (k >= NST && !mbar_wait_bounded(&empty_bar[s], (uint32_t)(((k / NST) - 1) & 1))) {
+                    abort_flag = 1;
+                    atomicExch(status, (int)CNPC_ETIMEOUT);
+                    break;
+                }
+                const int64_t c0 = first + (int64_t)k * step;
+                const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
+                const uint32_t bytes = (uint32_t)(valid * sizeof(float));
+                float *dst = stage0 + s * stage_elems;
+                fence_proxy_async();
+                mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
+                for (int u = 0; u < nf; ++u) {
+                    const int f = P.union_field[u];
+                    if (f == -1) continue;
+                    const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
+                    bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
+                }
+                issued = k + 1;
+            }
+            if (abort_flag) {
+                // drain this block's copies still in flight (bounded) before exit
+                for (int j = issued > NST ? issued - NST : 0; j < issued; ++j)
+                    mbar_wait_bounded(&full_bar[j % NST], (uint32_t)((j / NST) & 1));
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumer warps
+    const int gid = lane >> 2, tig = lane & 3;
+    const int a_row0 = P.a_slot[0];
+    const int b_row0 = P.b_slot[0];
+    float acc[MT][NT][4];
+    double acc64[MT][NT][4];
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                acc[m][n][e] = 0.f;
+                acc64[m][n][e] = 0.0;
+            }
+    int since_flush = 0;
+    for (int k = 0; k < nchunk; ++k) {
+        const int s = k % NST;
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / NST) & 1))) {
+            abort_flag = 1;
+            if (lane == 0) atomicExch(status, (int)CNPC_ETIMEOUT);
+        }
+        if (abort_flag) break;
+        const float *sb = stage0 + s * stage_elems;
+        const int valid = (int)min((int64_t)kMmaChunk, P.ncell - (first + (int64_t)k * step));
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int k0 = warp * 32 + ks * 8;
+            const bool v0 = k0 + tig < valid, v1 = k0 + tig + 4 < valid;
+            const float g0 = v0 ? sb[P.g_row * kMmaStride + k0 + tig] : 0.f;
+            const float g1 = v1 ? sb[P.g_row * kMmaStride + k0 + tig + 4] : 0.f;
+            uint32_t bh[NT][2], bl[NT][2];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                const float *rb = sb + (b_row0 + n * 8 + gid) * kMmaStride + k0 + tig;
+                split_tf32(v0 ? rb[0] : 0.f, bh[n][0], bl[n][0]);
+                split_tf32(v1 ? rb[4] : 0.f, bh[n][1], bl[n][1]);
+            }
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const float *ra = sb + (a_row0 + m * 16 + gid) * kMmaStride + k0 + tig;
+                uint32_t ah[4], al[4];
+                // cells past the end of a tail chunk were never copied: mask
+                // them (0 * garbage could be NaN)
+                split_tf32(v0 ? g0 * ra[0] : 0.f, ah[0], al[0]);
+                split_tf32(v0 ? g0 * ra[8 * kMmaStride] : 0.f, ah[1], al[1]);
+                split_tf32(v1 ? g1 * ra[4] : 0.f, ah[2], al[2]);
+                split_tf32(v1 ? g1 * ra[8 * kMmaStride + 4] : 0.f, ah[3], al[3]);
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    mma_tf32(acc[m][n], al, bh[n]);
+                    mma_tf32(acc[m][n], ah, bl[n]);
+                    mma_tf32(acc[m][n], ah, bh[n]);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty_bar[s]);
+        if (++since_flush == kMmaFlush) {
+            since_flush = 0;
+#pragma unroll
+            for (int m = 0; m < MT; ++m)
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        acc64[m][n][e] += (double)acc[m][n][e];
+                        acc[m][n][e] = 0.f;
+                    }
+        }
+    }
+    const bool bad = abort_flag != 0;
+    const double nanv = __longlong_as_double(0x7ff8000000000000ll);
+    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
+                const int col = n * 8 + 2 * tig + (e & 1);
+                dst[row * NP + col] = bad ? nanv : acc64[m][n][e] + (double)acc[m][n][e];
+            }
+}
+
+__global__ void gram_mma_reduce_kernel(const double *partial, int nparts, int mp, int np_, int na, int nb,
+                                       double *out) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= na * nb) return;
+    const int i = o / nb, j = o % nb;
+    double s = 0.0;
+    for (int p = 0; p < nparts; ++p) s += partial[(int64_t)p * mp * np_ + i * np_ + j];
+    out[o] = s;
+}
+
+static int run_gram_mma(cnpc_ctx *ctx, int64_t ncell, const float *g, const float *fields, int64_t stride,
+                        const int *a, int na, const int *b, int nb, double *out, cudaStream_t s) {
+    const int MT = (na + 15) / 16, NT = (nb + 7) / 8;
+    CNPC_REQUIRE(ctx, MT <= 3 && NT <= 3, "FP32 Gram launch covers at most 48 x 24 outputs");
+    GramParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.na = na;
+    P.nb = nb;
+    const int mp = MT * 16, np_ = NT * 8;
+    // staged rows: [G][A rows padded to 16 MT][B rows padded to 8 NT unless B is a
+    // contiguous run of A whose padding stays inside the A rows]
+    int b_off = -1;
+    for (int off = 0; off + nb <= na && b_off < 0; ++off) {
+        bool same = true;
+        for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
+        if (same && off + np_ <= mp) b_off = off;
+    }
+    std::vector<int> rows;
+    rows.push_back(-2);
+    for (int i = 0; i < mp; ++i) rows.push_back(i < na ? a[i] : -1);
+    const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
+    if (b_off < 0)
+        for (int j = 0; j < np_; ++j) rows.push_back(j < nb ? b[j] : -1);
+    CNPC_REQUIRE(ctx, (int)rows.size() <= kMaxUnion, "too many staged rows");
+    P.nunion = (int)rows.size();
+    for (int u = 0; u < P.nunion; ++u) {
+        P.union_field[u] = rows[u];
+        if (rows[u] != -1) ++P.ncopy;
+    }
+    P.g_row = 0;
+    P.a_slot[0] = 1;
+    P.b_slot[0] = b_base;
+    P.ncell = ncell;
+    P.field_stride = stride;
+    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && ((ncell * sizeof(float)) % 16 == 0) &&
+                          ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0),
+                 "contraction needs 16-byte aligned fields, field_stride and ncell");
+    const size_t row_bytes = (size_t)kMmaStride * sizeof(float);
+    P.nstages = (int)std::min<size_t>(kMaxStages, (220 * 1024) / (P.nunion * row_bytes));
+    CNPC_REQUIRE(ctx, P.nstages >= 2, "too many staged rows for the shared-memory ring");
+    const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
+    const int64_t nchunks = (ncell + kMmaChunk - 1) / kMmaChunk;
+    const int nblocks = (int)std::min<int64_t>(ctx->num_sms, nchunks);
+    const int nparts = nblocks * kMmaWarps;
+    int st = ensure_scratch(ctx, (size_t)nparts * mp * np_ * sizeof(double) + 256, s);
+    if (st) return st;
+    int *status = reinterpret_cast<int *>(static_cast<char *>(ctx->scratch) + ctx->scratch_bytes - 256);
+    double *part = (double *)ctx->scratch;
+#define CNPC_MMA_CASE(M_, N_)                                                                            \
+    if (MT == M_ && NT == N_) {                                                                          \
+        st = check_cuda(ctx, cudaFuncSetAttribute(gram_mma_kernel<M_, N_>,                               \
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
+                        "gram smem attribute");                                                          \
+        if (st) return st;                                                                               \
+        gram_mma_kernel<M_, N_><<<nblocks, (kMmaWarps + 1) * 32, smem, s>>>(g, fields, P, part, status); \
+    }
+    CNPC_MMA_CASE(1, 1) CNPC_MMA_CASE(1, 2) CNPC_MMA_CASE(1, 3) CNPC_MMA_CASE(2, 1) CNPC_MMA_CASE(2, 2)
+    CNPC_MMA_CASE(2, 3) CNPC_MMA_CASE(3, 1) CNPC_MMA_CASE(3, 2) CNPC_MMA_CASE(3, 3)
+#undef CNPC_MMA_CASE
+    st = check_launch(ctx, "gram_mma_kernel");
+    if (st) return st;
+    const int nout = na * nb;
+    gram_mma_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(part, nparts, mp, np_, na, nb, out);
+    return check_launch(ctx, "gram_mma_reduce_kernel");
+}
+
 // out[i, j] = sum over every block of the group owning tile(i, j) and every
 // warp of that block assigned to the tile, in a fixed order.
 template <int TM, int TN, int NW>
@@ -379,7 +597,7 @@ static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, i
     P.nstages = (int)std::min<size_t>(kMaxStages, (220 * 1024) / (P.nunion * row_bytes));
     CNPC_REQUIRE(ctx, P.nstages >= 2, "too many staged rows for the shared-memory ring (max 110)");
     const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
-    P.flush_chunks = sizeof(T) == 4 ? 8 : 1 << 30;  // FP32: ~64 cells per lane per partial
+    P.flush_chunks = 1 << 30;  // FP64 accumulators throughout
     int st = check_cuda(ctx, cudaFuncSetAttribute(gram_kernel<T, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem), "gram smem attribute");
     if (st) return st;
@@ -426,8 +644,8 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
     for (int j = 0; j < nb; ++j) CNPC_REQUIRE(ctx, h_b[j] >= 0, "negative field index");
     cudaStream_t s = (cudaStream_t)stream;
     if (dtype == CNPC_F32)
-        return run_gram<float>(ctx, ncell, (const float *)d_g, (const float *)d_fields, field_stride,
-                               h_a, na, h_b, nb, d_out, s);
+        return run_gram_mma(ctx, ncell, (const float *)d_g, (const float *)d_fields, field_stride, h_a, na,
+                            h_b, nb, d_out, s);
     return run_gram<double>(ctx, ncell, (const double *)d_g, (const double *)d_fields, field_stride,
                             h_a, na, h_b, nb, d_out, s);
 }

@@ -225,7 +225,15 @@ def contract(G, sf, rows, cols):
                 return True
         return False
 
-    if len(ridx) <= 128 and len(cidx) <= 128 and _staged_rows(len(ridx), len(cidx), shared(ridx, cidx)) <= 100:
+    if sf.precision == "f32":
+        # tensor-core launches cover at most 48 rows x 24 columns
+        rb, cb = 48, 24
+        if len(ridx) <= rb and len(cidx) <= cb:
+            blocks = [(0, len(ridx), 0, len(cidx))]
+        else:
+            blocks = [(r0, min(len(ridx), r0 + rb), c0, min(len(cidx), c0 + cb))
+                      for r0 in range(0, len(ridx), rb) for c0 in range(0, len(cidx), cb)]
+    elif len(ridx) <= 128 and len(cidx) <= 128 and _staged_rows(len(ridx), len(cidx), shared(ridx, cidx)) <= 100:
         blocks = [(0, len(ridx), 0, len(cidx))]
     else:
         blocks = [(r0, min(len(ridx), r0 + 48), c0, min(len(cidx), c0 + 48))
