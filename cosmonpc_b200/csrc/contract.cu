@@ -334,35 +334,43 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
     __syncthreads();
 
     if (warp == kMmaWarps) {
-        // ---------------- producer warp: one lane issues every bulk copy
-        if (lane == 0) {
-            int issued = 0;
-            for (int k = 0; k < nchunk && !abort_flag; ++k) {
-                const int s = k % NST;
-                if (k >= NST && !mbar_wait_bounded(&empty_bar[s], (uint32_t)(((k / NST) - 1) & 1))) {
+        // ---------------- producer warp: lane 0 posts the byte count of a
+        // stage, then the 32 lanes issue the row copies in parallel
+        int issued = 0;
+        for (int k = 0; k < nchunk; ++k) {
+            const int s = k % NST;
+            int ok = 1;
+            if (lane == 0) {
+                if (abort_flag ||
+                    (k >= NST && !mbar_wait_bounded(&empty_bar[s], (uint32_t)(((k / NST) - 1) & 1)))) {
+                    if (!abort_flag) atomicExch(status, (int)CNPC_ETIMEOUT);
                     abort_flag = 1;
-                    atomicExch(status, (int)CNPC_ETIMEOUT);
-                    break;
+                    ok = 0;
                 }
-                const int64_t c0 = first + (int64_t)k * step;
-                const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
-                const uint32_t bytes = (uint32_t)(valid * sizeof(float));
-                float *dst = stage0 + s * stage_elems;
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            const int64_t c0 = first + (int64_t)k * step;
+            const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
+            const uint32_t bytes = (uint32_t)(valid * sizeof(float));
+            float *dst = stage0 + s * stage_elems;
+            if (lane == 0) {
                 fence_proxy_async();
                 mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
-                for (int u = 0; u < nf; ++u) {
-                    const int f = P.union_field[u];
-                    if (f == -1) continue;
-                    const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
-                    bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
-                }
-                issued = k + 1;
             }
-            if (abort_flag) {
-                // drain this block's copies still in flight (bounded) before exit
-                for (int j = issued > NST ? issued - NST : 0; j < issued; ++j)
-                    mbar_wait_bounded(&full_bar[j % NST], (uint32_t)((j / NST) & 1));
+            __syncwarp();
+            for (int u = lane; u < nf; u += 32) {
+                const int f = P.union_field[u];
+                if (f == -1) continue;
+                const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
+                bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
             }
+            issued = k + 1;
+        }
+        if (abort_flag && lane == 0) {
+            // drain this block's copies still in flight (bounded) before exit
+            for (int j = issued > NST ? issued - NST : 0; j < issued; ++j)
+                mbar_wait_bounded(&full_bar[j % NST], (uint32_t)((j / NST) & 1));
         }
         return;
     }
