@@ -282,10 +282,10 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 // (16 MT) x (8 NT) output for its 32 cells of every chunk; a dedicated producer
 // warp streams the chunks with cp.async.bulk into a ring guarded by full/empty
 // mbarriers.  The FP32 fragments are added into FP64 every 256 cells.
-constexpr int kMmaWarps = 8;               // consumer warps
+constexpr int kMmaWarps = 16;              // consumer warps
 constexpr int kMmaChunk = 256;             // cells per staged row and chunk
 constexpr int kMmaStride = kMmaChunk + 4;  // padded row: conflict-free fragment loads
-constexpr int kMmaFlush = 8;               // chunks between FP64 folds
+constexpr int kMmaFlush = 8;               // chunks between FP64 folds (128 cells per lane)
 
 __device__ inline uint32_t tf32_rna(float x) {
     uint32_t r;
@@ -375,21 +375,36 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         return;
     }
 
-    // ---------------- consumer warps
+    // ---------------- consumer warps: warp w takes cells [16w, 16w + 16) of
+    // every chunk (two k-steps); FP32 fragments are folded into this warp's
+    // own FP64 partial in global memory every kMmaFlush chunks
     const int gid = lane >> 2, tig = lane & 3;
     const int a_row0 = P.a_slot[0];
     const int b_row0 = P.b_slot[0];
+    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
     float acc[MT][NT][4];
-    double acc64[MT][NT][4];
 #pragma unroll
     for (int m = 0; m < MT; ++m)
 #pragma unroll
         for (int n = 0; n < NT; ++n)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                acc[m][n][e] = 0.f;
-                acc64[m][n][e] = 0.0;
-            }
+            for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
+    bool stored = false;
+    auto fold = [&]() {
+#pragma unroll
+        for (int m = 0; m < MT; ++m)
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
+                    const int col = n * 8 + 2 * tig + (e & 1);
+                    double *p = dst + row * NP + col;
+                    *p = (stored ? *p : 0.0) + (double)acc[m][n][e];
+                    acc[m][n][e] = 0.f;
+                }
+        stored = true;
+    };
     int since_flush = 0;
     for (int k = 0; k < nchunk; ++k) {
         const int s = k % NST;
@@ -401,8 +416,8 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         const float *sb = stage0 + s * stage_elems;
         const int valid = (int)min((int64_t)kMmaChunk, P.ncell - (first + (int64_t)k * step));
 #pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            const int k0 = warp * 32 + ks * 8;
+        for (int ks = 0; ks < 2; ++ks) {
+            const int k0 = warp * 16 + ks * 8;
             const bool v0 = k0 + tig < valid, v1 = k0 + tig + 4 < valid;
             const float g0 = v0 ? sb[P.g_row * kMmaStride + k0 + tig] : 0.f;
             const float g1 = v1 ? sb[P.g_row * kMmaStride + k0 + tig + 4] : 0.f;
@@ -435,30 +450,20 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         if (lane == 0) mbar_arrive(&empty_bar[s]);
         if (++since_flush == kMmaFlush) {
             since_flush = 0;
-#pragma unroll
-            for (int m = 0; m < MT; ++m)
-#pragma unroll
-                for (int n = 0; n < NT; ++n)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        acc64[m][n][e] += (double)acc[m][n][e];
-                        acc[m][n][e] = 0.f;
-                    }
+            fold();
         }
     }
-    const bool bad = abort_flag != 0;
-    const double nanv = __longlong_as_double(0x7ff8000000000000ll);
-    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
+    fold();
+    if (abort_flag) {
+        const double nanv = __longlong_as_double(0x7ff8000000000000ll);
 #pragma unroll
-    for (int m = 0; m < MT; ++m)
+        for (int m = 0; m < MT; ++m)
 #pragma unroll
-        for (int n = 0; n < NT; ++n)
+            for (int n = 0; n < NT; ++n)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
-                const int col = n * 8 + 2 * tig + (e & 1);
-                dst[row * NP + col] = bad ? nanv : acc64[m][n][e] + (double)acc[m][n][e];
-            }
+                for (int e = 0; e < 4; ++e)
+                    dst[(m * 16 + gid + ((e & 2) ? 8 : 0)) * NP + n * 8 + 2 * tig + (e & 1)] = nanv;
+    }
 }
 
 __global__ void gram_mma_reduce_kernel(const double *partial, int nparts, int mp, int np_, int na, int nb,
