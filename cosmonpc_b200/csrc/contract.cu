@@ -94,6 +94,13 @@ __device__ inline void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+__device__ inline void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// arrive on the mbarrier once every cp.async this thread issued has landed
+__device__ inline void cp_async_arrive_noinc(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ inline void mbar_arrive(uint64_t *bar) {
@@ -326,7 +333,7 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < NST; ++s) {
-            mbar_init(&full_bar[s], 1);
+            mbar_init(&full_bar[s], 32);
             mbar_init(&empty_bar[s], kMmaWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -334,8 +341,9 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
     __syncthreads();
 
     if (warp == kMmaWarps) {
-        // ---------------- producer warp: lane 0 posts the byte count of a
-        // stage, then the 32 lanes issue the row copies in parallel
+        // ---------------- producer warp: the 32 lanes stream the chunk's rows
+        // with 16-byte cp.async; each lane's completion arrives on the stage's
+        // full barrier (count 32)
         int issued = 0;
         for (int k = 0; k < nchunk; ++k) {
             const int s = k % NST;
@@ -351,20 +359,17 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             const int64_t c0 = first + (int64_t)k * step;
-            const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
-            const uint32_t bytes = (uint32_t)(valid * sizeof(float));
+            const int valid = (int)min((int64_t)kMmaChunk, P.ncell - c0);
+            const int nvec = valid / 4;  // 16-byte pieces per row
             float *dst = stage0 + s * stage_elems;
-            if (lane == 0) {
-                fence_proxy_async();
-                mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
-            }
-            __syncwarp();
-            for (int u = lane; u < nf; u += 32) {
+            for (int idx = lane; idx < nf * (kMmaChunk / 4); idx += 32) {
+                const int u = idx / (kMmaChunk / 4), v = idx % (kMmaChunk / 4);
                 const int f = P.union_field[u];
-                if (f == -1) continue;
-                const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
-                bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
+                if (f == -1 || v >= nvec) continue;
+                const float *src = (f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0) + 4 * v;
+                cp_async16(dst + u * kMmaStride + 4 * v, src);
             }
+            cp_async_arrive_noinc(&full_bar[s]);
             issued = k + 1;
         }
         if (abort_flag && lane == 0) {
