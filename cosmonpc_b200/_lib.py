@@ -54,8 +54,8 @@ _SIGS = {
     "cnpc_status_string": [_i],
     "cnpc_version": [],
     "cnpc_paint": [_vp, _i, _vp, _vp, _i64, _i, _d, _i, _vp, _vp, _vp],
-    "cnpc_fft_r2c": [_vp, _i, _i, _i, _vp, _vp, _vp],
-    "cnpc_fft_c2r": [_vp, _i, _i, _i, _vp, _vp, _vp],
+    "cnpc_fft_r2c": [_vp, _i, _i, _i, _vp, _i64, _vp, _vp],
+    "cnpc_fft_c2r": [_vp, _i, _i, _i, _vp, _vp, _i64, _vp],
     "cnpc_forward_finish": [_vp, _i, _i, _d, _vp, _vp, _d, _i, _i, _d, _d, _vp],
     "cnpc_kbin_counts": [_vp, _i, _d, _dp, _i, _vp, _vp, _vp],
     "cnpc_pk_bins": [_vp, _i, _i, _d, _vp, _vp, _dp, _i, _ip, _i, _dp, _vp, _vp],
@@ -218,15 +218,15 @@ class Context:
         _tstop("paint", e0, pos.shape[0] * (24 + (8 if weight is not None else 0))
                + n ** 3 * _esz(dtype) * (2 if mesh_shifted is not None else 1))
 
-    def r2c(self, dtype, n, batch, real, spec):
+    def r2c(self, dtype, n, batch, real, spec, real_dist=0):
         e0 = _tstart()
-        self._check(self.lib.cnpc_fft_r2c(self.h, dtype, n, batch, _ptr(real), _ptr(spec), self.stream()),
+        self._check(self.lib.cnpc_fft_r2c(self.h, dtype, n, batch, _ptr(real), real_dist, _ptr(spec), self.stream()),
                     "cnpc_fft_r2c")
         _tstop("cufft_r2c", e0, batch * (n ** 3 + 2 * n * n * (n // 2 + 1)) * _esz(dtype))
 
-    def c2r(self, dtype, n, batch, spec, real):
+    def c2r(self, dtype, n, batch, spec, real, real_dist=0):
         e0 = _tstart()
-        self._check(self.lib.cnpc_fft_c2r(self.h, dtype, n, batch, _ptr(spec), _ptr(real), self.stream()),
+        self._check(self.lib.cnpc_fft_c2r(self.h, dtype, n, batch, _ptr(spec), _ptr(real), real_dist, self.stream()),
                     "cnpc_fft_c2r")
         _tstop("cufft_c2r", e0, batch * (n ** 3 + 2 * n * n * (n // 2 + 1)) * _esz(dtype))
 

@@ -41,8 +41,8 @@ int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream) {
     return CNPC_OK;
 }
 
-static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, cufftHandle *out) {
-    auto key = std::make_tuple((int)type, n, batch);
+static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long real_dist, cufftHandle *out) {
+    auto key = std::make_tuple((int)type, n, batch, real_dist);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) {
         *out = it->second;
@@ -50,7 +50,15 @@ static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, cufftHandle
     }
     cufftHandle h;
     int dims[3] = {n, n, n};
-    cufftResult r = cufftPlanMany(&h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch);
+    int real_embed[3] = {n, n, n};
+    int spec_embed[3] = {n, n, n / 2 + 1};
+    const long long spec_dist = (long long)n * n * (n / 2 + 1);
+    const bool forward = type == CUFFT_R2C || type == CUFFT_D2Z;
+    cufftResult r;
+    if (forward)
+        r = cufftPlanMany(&h, 3, dims, real_embed, 1, (int)real_dist, spec_embed, 1, (int)spec_dist, type, batch);
+    else
+        r = cufftPlanMany(&h, 3, dims, spec_embed, 1, (int)spec_dist, real_embed, 1, (int)real_dist, type, batch);
     if (r != CUFFT_SUCCESS) {
         if (r == CUFFT_ALLOC_FAILED)
             return fail(ctx, CNPC_ENOMEM, "cufftPlanMany: allocation failed");
@@ -116,14 +124,17 @@ int cnpc_ctx_destroy(cnpc_ctx *ctx) {
 
 const char *cnpc_ctx_last_error(cnpc_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
-int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real, void *d_spec,
-                 cnpc_stream_t stream) {
+int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real, int64_t real_dist,
+                 void *d_spec, cnpc_stream_t stream) {
     CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
     CNPC_REQUIRE(ctx, batch >= 1, "batch must be >= 1");
     CNPC_REQUIRE(ctx, d_real && d_spec, "null buffer");
     CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
     cufftHandle h;
-    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_R2C : CUFFT_D2Z, n, batch, &h);
+    const long long cells = (long long)n * n * n;
+    CNPC_REQUIRE(ctx, real_dist == 0 || real_dist >= cells, "real_dist must be 0 or >= n^3");
+    CNPC_REQUIRE(ctx, real_dist < (1ll << 31), "real_dist too large");
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_R2C : CUFFT_D2Z, n, batch, real_dist ? real_dist : cells, &h);
     if (st) return st;
     cufftSetStream(h, (cudaStream_t)stream);
     cufftResult r = dtype == CNPC_F32
@@ -133,14 +144,17 @@ int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real,
     return CNPC_OK;
 }
 
-int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec, void *d_real,
+int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec, void *d_real, int64_t real_dist,
                  cnpc_stream_t stream) {
     CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
     CNPC_REQUIRE(ctx, batch >= 1, "batch must be >= 1");
     CNPC_REQUIRE(ctx, d_real && d_spec, "null buffer");
     CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
     cufftHandle h;
-    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_C2R : CUFFT_Z2D, n, batch, &h);
+    const long long cells = (long long)n * n * n;
+    CNPC_REQUIRE(ctx, real_dist == 0 || real_dist >= cells, "real_dist must be 0 or >= n^3");
+    CNPC_REQUIRE(ctx, real_dist < (1ll << 31), "real_dist too large");
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_C2R : CUFFT_Z2D, n, batch, real_dist ? real_dist : cells, &h);
     if (st) return st;
     cufftSetStream(h, (cudaStream_t)stream);
     cufftResult r = dtype == CNPC_F32

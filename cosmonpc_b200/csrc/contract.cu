@@ -94,13 +94,6 @@ __device__ inline void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
-__device__ inline void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-// arrive on the mbarrier once every cp.async this thread issued has landed
-__device__ inline void cp_async_arrive_noinc(uint64_t *bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ inline void mbar_arrive(uint64_t *bar) {
@@ -289,10 +282,10 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 // (16 MT) x (8 NT) output for its 32 cells of every chunk; a dedicated producer
 // warp streams the chunks with cp.async.bulk into a ring guarded by full/empty
 // mbarriers.  The FP32 fragments are added into FP64 every 256 cells.
-constexpr int kMmaWarps = 16;              // consumer warps
+constexpr int kMmaWarps = 8;               // consumer warps
 constexpr int kMmaChunk = 256;             // cells per staged row and chunk
 constexpr int kMmaStride = kMmaChunk + 4;  // padded row: conflict-free fragment loads
-constexpr int kMmaFlush = 8;               // chunks between FP64 folds (128 cells per lane)
+constexpr int kMmaFlush = 8;               // chunks between FP64 folds
 
 __device__ inline uint32_t tf32_rna(float x) {
     uint32_t r;
@@ -333,7 +326,7 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < NST; ++s) {
-            mbar_init(&full_bar[s], 32);
+            mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], kMmaWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -341,9 +334,8 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
     __syncthreads();
 
     if (warp == kMmaWarps) {
-        // ---------------- producer warp: the 32 lanes stream the chunk's rows
-        // with 16-byte cp.async; each lane's completion arrives on the stage's
-        // full barrier (count 32)
+        // ---------------- producer warp: lane 0 posts the byte count of a
+        // stage, then the 32 lanes issue the row copies in parallel
         int issued = 0;
         for (int k = 0; k < nchunk; ++k) {
             const int s = k % NST;
@@ -359,17 +351,20 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             const int64_t c0 = first + (int64_t)k * step;
-            const int valid = (int)min((int64_t)kMmaChunk, P.ncell - c0);
-            const int nvec = valid / 4;  // 16-byte pieces per row
+            const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
+            const uint32_t bytes = (uint32_t)(valid * sizeof(float));
             float *dst = stage0 + s * stage_elems;
-            for (int idx = lane; idx < nf * (kMmaChunk / 4); idx += 32) {
-                const int u = idx / (kMmaChunk / 4), v = idx % (kMmaChunk / 4);
-                const int f = P.union_field[u];
-                if (f == -1 || v >= nvec) continue;
-                const float *src = (f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0) + 4 * v;
-                cp_async16(dst + u * kMmaStride + 4 * v, src);
+            if (lane == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
             }
-            cp_async_arrive_noinc(&full_bar[s]);
+            __syncwarp();
+            for (int u = lane; u < nf; u += 32) {
+                const int f = P.union_field[u];
+                if (f == -1) continue;
+                const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
+                bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
+            }
             issued = k + 1;
         }
         if (abort_flag && lane == 0) {
@@ -380,36 +375,21 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         return;
     }
 
-    // ---------------- consumer warps: warp w takes cells [16w, 16w + 16) of
-    // every chunk (two k-steps); FP32 fragments are folded into this warp's
-    // own FP64 partial in global memory every kMmaFlush chunks
+    // ---------------- consumer warps
     const int gid = lane >> 2, tig = lane & 3;
     const int a_row0 = P.a_slot[0];
     const int b_row0 = P.b_slot[0];
-    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
     float acc[MT][NT][4];
+    double acc64[MT][NT][4];
 #pragma unroll
     for (int m = 0; m < MT; ++m)
 #pragma unroll
         for (int n = 0; n < NT; ++n)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
-    bool stored = false;
-    auto fold = [&]() {
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int n = 0; n < NT; ++n)
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
-                    const int col = n * 8 + 2 * tig + (e & 1);
-                    double *p = dst + row * NP + col;
-                    *p = (stored ? *p : 0.0) + (double)acc[m][n][e];
-                    acc[m][n][e] = 0.f;
-                }
-        stored = true;
-    };
+            for (int e = 0; e < 4; ++e) {
+                acc[m][n][e] = 0.f;
+                acc64[m][n][e] = 0.0;
+            }
     int since_flush = 0;
     for (int k = 0; k < nchunk; ++k) {
         const int s = k % NST;
@@ -421,8 +401,8 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         const float *sb = stage0 + s * stage_elems;
         const int valid = (int)min((int64_t)kMmaChunk, P.ncell - (first + (int64_t)k * step));
 #pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-            const int k0 = warp * 16 + ks * 8;
+        for (int ks = 0; ks < 4; ++ks) {
+            const int k0 = warp * 32 + ks * 8;
             const bool v0 = k0 + tig < valid, v1 = k0 + tig + 4 < valid;
             const float g0 = v0 ? sb[P.g_row * kMmaStride + k0 + tig] : 0.f;
             const float g1 = v1 ? sb[P.g_row * kMmaStride + k0 + tig + 4] : 0.f;
@@ -455,20 +435,30 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
         if (lane == 0) mbar_arrive(&empty_bar[s]);
         if (++since_flush == kMmaFlush) {
             since_flush = 0;
-            fold();
+#pragma unroll
+            for (int m = 0; m < MT; ++m)
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        acc64[m][n][e] += (double)acc[m][n][e];
+                        acc[m][n][e] = 0.f;
+                    }
         }
     }
-    fold();
-    if (abort_flag) {
-        const double nanv = __longlong_as_double(0x7ff8000000000000ll);
+    const bool bad = abort_flag != 0;
+    const double nanv = __longlong_as_double(0x7ff8000000000000ll);
+    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
 #pragma unroll
-        for (int m = 0; m < MT; ++m)
+    for (int m = 0; m < MT; ++m)
 #pragma unroll
-            for (int n = 0; n < NT; ++n)
+        for (int n = 0; n < NT; ++n)
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    dst[(m * 16 + gid + ((e & 2) ? 8 : 0)) * NP + n * 8 + 2 * tig + (e & 1)] = nanv;
-    }
+            for (int e = 0; e < 4; ++e) {
+                const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
+                const int col = n * 8 + 2 * tig + (e & 1);
+                dst[row * NP + col] = bad ? nanv : acc64[m][n][e] + (double)acc[m][n][e];
+            }
 }
 
 __global__ void gram_mma_reduce_kernel(const double *partial, int nparts, int mp, int np_, int na, int nb,

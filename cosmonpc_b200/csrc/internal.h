@@ -13,8 +13,8 @@
 struct cnpc_ctx {
     int device = 0;
     std::string last_error;
-    // cuFFT plans keyed by (type, n, batch)
-    std::map<std::tuple<int, int, int>, cufftHandle> plans;
+    // cuFFT plans keyed by (type, n, batch, real-field distance)
+    std::map<std::tuple<int, int, int, long long>, cufftHandle> plans;
     // scratch for per-block partial sums of the x-space reductions
     void *scratch = nullptr;
     size_t scratch_bytes = 0;

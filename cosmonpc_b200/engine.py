@@ -98,6 +98,12 @@ def kbin_counts(n, boxsize, edges):
 
 
 # ------------------------------------------------------------ shell fields
+# Extra elements between consecutive shell fields.  An n^3 float field is a
+# power-of-two number of bytes; rows that far apart land on the same memory
+# channels when a contraction streams dozens of them at once.
+FIELD_PAD = 1088
+
+
 def leg_components(l, m):
     """Real component fields of the complex shell field of Y_lm (see header)."""
     if m == 0:
@@ -124,7 +130,9 @@ class ShellFields:
         self.racah = racah
         dev = _device()
         self.capacity = int(capacity)
-        self.fields = torch.empty((self.capacity, n * n * n), dtype=self.rdt, device=dev)
+        # rows padded off the 2^k-byte stride of an n^3 field (see FIELD_PAD)
+        self.stride = n * n * n + FIELD_PAD
+        self.fields = torch.empty((self.capacity, self.stride), dtype=self.rdt, device=dev)
         self.fft_batch = max(1, min(int(fft_batch), self.capacity))
         self.scratch = torch.empty((self.fft_batch, n, n, n // 2 + 1), dtype=self.cdt, device=dev)
         self.slot = {}
@@ -166,10 +174,11 @@ class ShellFields:
             slots = [self.free.pop() for _ in batch]
             # contiguous slots let one batched c2r write every field of the batch
             if slots == list(range(slots[0], slots[0] + len(slots))):
-                ctx.c2r(self.code, self.n, len(batch), self.scratch, self.fields[slots[0]:slots[0] + len(slots)])
+                ctx.c2r(self.code, self.n, len(batch), self.scratch, self.fields[slots[0]:slots[0] + len(slots)],
+                        self.stride)
             else:
                 for j, s in enumerate(slots):
-                    ctx.c2r(self.code, self.n, 1, self.scratch[j], self.fields[s])
+                    ctx.c2r(self.code, self.n, 1, self.scratch[j], self.fields[s], self.stride)
             for k, s in zip(batch, slots):
                 self.slot[k] = s
 
@@ -241,10 +250,10 @@ def contract(G, sf, rows, cols):
     for (r0, r1, c0, c1) in blocks:
         rr, cc = ridx[r0:r1], cidx[c0:c1]
         if (r1 - r0, c1 - c0) == (len(ridx), len(cidx)):
-            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, T)
+            ctx.gram(sf.code, ncell, G, sf.fields, sf.stride, rr, cc, T)
         else:
             out = torch.empty((len(rr), len(cc)), dtype=torch.float64, device=dev)
-            ctx.gram(sf.code, ncell, G, sf.fields, ncell, rr, cc, out)
+            ctx.gram(sf.code, ncell, G, sf.fields, sf.stride, rr, cc, out)
             T[r0:r1, c0:c1] = out
     return T
 

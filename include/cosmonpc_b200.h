@@ -104,12 +104,14 @@ int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_we
 
 /* --------------------------------------------------------------------- FFT
  * Replace RealField.r2c / ComplexField.c2r of pmesh.  Unnormalised cuFFT
- * transforms of `batch` contiguous fields; the 1/n^3 of pmesh's r2c is folded
- * into cnpc_forward_finish.  c2r may overwrite its input. */
+ * transforms of `batch` fields; the 1/n^3 of pmesh's r2c is folded into
+ * cnpc_forward_finish.  Spectra of a batch are contiguous; real field b starts
+ * at d_real + b * real_dist elements (real_dist 0 means n^3; a padded distance
+ * keeps batched fields off power-of-two strides).  c2r may overwrite its input. */
 int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real,
-                 void *d_spec, cnpc_stream_t stream);
+                 int64_t real_dist, void *d_spec, cnpc_stream_t stream);
 int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec,
-                 void *d_real, cnpc_stream_t stream);
+                 void *d_real, int64_t real_dist, cnpc_stream_t stream);
 
 /* Finishes the forward transform in place on d_spec:
  *   c = s1 / n^3                       (d_spec2 == NULL)
