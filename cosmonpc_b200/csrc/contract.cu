@@ -278,13 +278,16 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 // with K = cells.  Each operand is split into two TF32 parts (x = hi + lo,
 // hi = rna_tf32(x), lo = rna_tf32(x - hi)) and C accumulates
 // Al*Bh + Ah*Bl + Ah*Bh with mma.sync m16n8k8 (FP32 accumulate): products
-// carry ~22 significant bits, as good as FP32 fields.  One warp owns the whole
-// (16 MT) x (8 NT) output for its 32 cells of every chunk; a dedicated producer
-// warp streams the chunks with cp.async.bulk into a ring guarded by full/empty
-// mbarriers.  The FP32 fragments are added into FP64 every 256 cells.
-constexpr int kMmaWarps = 8;               // consumer warps
-constexpr int kMmaChunk = 256;             // cells per staged row and chunk
-constexpr int kMmaStride = kMmaChunk + 4;  // padded row: conflict-free fragment loads
+// carry ~22 significant bits, as good as FP32 fields.
+//
+// Every warp is independent: it owns the whole (16 MT) x (8 NT) output for a
+// 32-cell slab of each chunk, streams its slab of every staged row with 16-byte
+// cp.async into a private double-buffered shared-memory tile (padded rows, so
+// the fragment loads are bank-conflict free) while it contracts the previous
+// slab, and folds its FP32 fragments into FP64 registers every 8 chunks.
+constexpr int kMmaWarps = 8;
+constexpr int kMmaChunk = 256;             // cells per block chunk (32 per warp)
+constexpr int kMmaRow = 36;                // padded slab row (32 cells + 4)
 constexpr int kMmaFlush = 8;               // chunks between FP64 folds
 
 __device__ inline uint32_t tf32_rna(float x) {
@@ -303,79 +306,46 @@ __device__ inline void mma_tf32(float *c, const uint32_t *a, const uint32_t *b) 
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
+__device__ inline void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ inline void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 template <int MT, int NT>
-__global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
+__global__ void __launch_bounds__(kMmaWarps * 32, 1)
     gram_mma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
-                    double *partial, int *status) {
+                    double *partial) {
     constexpr int MP = MT * 16, NP = NT * 8;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kMaxStages];
-    __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
-    __shared__ volatile int abort_flag;
-    const int NST = P.nstages;
-    const int nf = P.nunion;
-    const int stage_elems = nf * kMmaStride;
-    float *const stage0 = reinterpret_cast<float *>(smem_raw);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int64_t first = (int64_t)blockIdx.x * kMmaChunk;
-    const int64_t step = (int64_t)gridDim.x * kMmaChunk;
-    const int nchunk = first < P.ncell ? (int)((P.ncell - first + step - 1) / step) : 0;
+    const int nrows = P.nunion;  // staged rows: G, A rows (padded), separate B rows (padded)
+    const int slab = nrows * kMmaRow;
+    float *const buf0 = reinterpret_cast<float *>(smem_raw) + (size_t)warp * 2 * slab;
+    const int64_t nchunk_all = (P.ncell + kMmaChunk - 1) / kMmaChunk;
+    const int nchunk = blockIdx.x < nchunk_all ? (int)((nchunk_all - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
-    if (threadIdx.x == 0) {
-        abort_flag = 0;
-        for (int s = 0; s < NST; ++s) {
-            mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], kMmaWarps);
+    // stream this warp's 32-cell slab of chunk k into buffer b
+    auto issue = [&](int k, int b) {
+        const int64_t c0 = ((int64_t)blockIdx.x + (int64_t)k * gridDim.x) * kMmaChunk + warp * 32;
+        float *dst = buf0 + b * slab;
+        for (int idx = lane; idx < nrows * 8; idx += 32) {
+            const int row = idx >> 3, part = idx & 7;
+            const int f = P.union_field[row];
+            if (f == -1) continue;  // padding row: only feeds discarded outputs
+            const int64_t cell = c0 + part * 4;
+            float *d = dst + row * kMmaRow + part * 4;
+            if (cell < P.ncell)  // ncell is a multiple of 4, so the 16 bytes are all valid
+                cp_async16(d, (f == -2 ? g : fields + (int64_t)f * P.field_stride) + cell);
+            else
+                *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
+        cp_async_commit();
+    };
 
-    if (warp == kMmaWarps) {
-        // ---------------- producer warp: lane 0 posts the byte count of a
-        // stage, then the 32 lanes issue the row copies in parallel
-        int issued = 0;
-        for (int k = 0; k < nchunk; ++k) {
-            const int s = k % NST;
-            int ok = 1;
-            if (lane == 0) {
-                if (abort_flag ||
-                    (k >= NST && !mbar_wait_bounded(&empty_bar[s], (uint32_t)(((k / NST) - 1) & 1)))) {
-                    if (!abort_flag) atomicExch(status, (int)CNPC_ETIMEOUT);
-                    abort_flag = 1;
-                    ok = 0;
-                }
-            }
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (!ok) break;
-            const int64_t c0 = first + (int64_t)k * step;
-            const int64_t valid = min((int64_t)kMmaChunk, P.ncell - c0);
-            const uint32_t bytes = (uint32_t)(valid * sizeof(float));
-            float *dst = stage0 + s * stage_elems;
-            if (lane == 0) {
-                fence_proxy_async();
-                mbar_expect_tx(&full_bar[s], bytes * (uint32_t)P.ncopy);
-            }
-            __syncwarp();
-            for (int u = lane; u < nf; u += 32) {
-                const int f = P.union_field[u];
-                if (f == -1) continue;
-                const float *src = f == -2 ? g + c0 : fields + (int64_t)f * P.field_stride + c0;
-                bulk_g2s(dst + u * kMmaStride, src, bytes, &full_bar[s]);
-            }
-            issued = k + 1;
-        }
-        if (abort_flag && lane == 0) {
-            // drain this block's copies still in flight (bounded) before exit
-            for (int j = issued > NST ? issued - NST : 0; j < issued; ++j)
-                mbar_wait_bounded(&full_bar[j % NST], (uint32_t)((j / NST) & 1));
-        }
-        return;
-    }
-
-    // ---------------- consumer warps
     const int gid = lane >> 2, tig = lane & 3;
     const int a_row0 = P.a_slot[0];
     const int b_row0 = P.b_slot[0];
@@ -390,39 +360,37 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
                 acc[m][n][e] = 0.f;
                 acc64[m][n][e] = 0.0;
             }
+    if (nchunk > 0) issue(0, 0);
     int since_flush = 0;
     for (int k = 0; k < nchunk; ++k) {
-        const int s = k % NST;
-        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / NST) & 1))) {
-            abort_flag = 1;
-            if (lane == 0) atomicExch(status, (int)CNPC_ETIMEOUT);
+        if (k + 1 < nchunk) {
+            issue(k + 1, (k + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
-        if (abort_flag) break;
-        const float *sb = stage0 + s * stage_elems;
-        const int valid = (int)min((int64_t)kMmaChunk, P.ncell - (first + (int64_t)k * step));
+        __syncwarp();
+        const float *sb = buf0 + (k & 1) * slab;
 #pragma unroll
         for (int ks = 0; ks < 4; ++ks) {
-            const int k0 = warp * 32 + ks * 8;
-            const bool v0 = k0 + tig < valid, v1 = k0 + tig + 4 < valid;
-            const float g0 = v0 ? sb[P.g_row * kMmaStride + k0 + tig] : 0.f;
-            const float g1 = v1 ? sb[P.g_row * kMmaStride + k0 + tig + 4] : 0.f;
+            const int k0 = ks * 8;
+            const float g0 = sb[P.g_row * kMmaRow + k0 + tig];
+            const float g1 = sb[P.g_row * kMmaRow + k0 + tig + 4];
             uint32_t bh[NT][2], bl[NT][2];
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
-                const float *rb = sb + (b_row0 + n * 8 + gid) * kMmaStride + k0 + tig;
-                split_tf32(v0 ? rb[0] : 0.f, bh[n][0], bl[n][0]);
-                split_tf32(v1 ? rb[4] : 0.f, bh[n][1], bl[n][1]);
+                const float *rb = sb + (b_row0 + n * 8 + gid) * kMmaRow + k0 + tig;
+                split_tf32(rb[0], bh[n][0], bl[n][0]);
+                split_tf32(rb[4], bh[n][1], bl[n][1]);
             }
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
-                const float *ra = sb + (a_row0 + m * 16 + gid) * kMmaStride + k0 + tig;
+                const float *ra = sb + (a_row0 + m * 16 + gid) * kMmaRow + k0 + tig;
                 uint32_t ah[4], al[4];
-                // cells past the end of a tail chunk were never copied: mask
-                // them (0 * garbage could be NaN)
-                split_tf32(v0 ? g0 * ra[0] : 0.f, ah[0], al[0]);
-                split_tf32(v0 ? g0 * ra[8 * kMmaStride] : 0.f, ah[1], al[1]);
-                split_tf32(v1 ? g1 * ra[4] : 0.f, ah[2], al[2]);
-                split_tf32(v1 ? g1 * ra[8 * kMmaStride + 4] : 0.f, ah[3], al[3]);
+                split_tf32(g0 * ra[0], ah[0], al[0]);
+                split_tf32(g0 * ra[8 * kMmaRow], ah[1], al[1]);
+                split_tf32(g1 * ra[4], ah[2], al[2]);
+                split_tf32(g1 * ra[8 * kMmaRow + 4], ah[3], al[3]);
 #pragma unroll
                 for (int n = 0; n < NT; ++n) {
                     mma_tf32(acc[m][n], al, bh[n]);
@@ -431,8 +399,7 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
                 }
             }
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty_bar[s]);
+        __syncwarp();  // the slab is refilled by the issue of iteration k + 1
         if (++since_flush == kMmaFlush) {
             since_flush = 0;
 #pragma unroll
@@ -446,8 +413,6 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
                     }
         }
     }
-    const bool bad = abort_flag != 0;
-    const double nanv = __longlong_as_double(0x7ff8000000000000ll);
     double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
 #pragma unroll
     for (int m = 0; m < MT; ++m)
@@ -457,7 +422,7 @@ __global__ void __launch_bounds__((kMmaWarps + 1) * 32, 1)
             for (int e = 0; e < 4; ++e) {
                 const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
                 const int col = n * 8 + 2 * tig + (e & 1);
-                dst[row * NP + col] = bad ? nanv : acc64[m][n][e] + (double)acc[m][n][e];
+                dst[row * NP + col] = acc64[m][n][e] + (double)acc[m][n][e];
             }
 }
 
@@ -496,28 +461,22 @@ static int run_gram_mma(cnpc_ctx *ctx, int64_t ncell, const float *g, const floa
         for (int j = 0; j < np_; ++j) rows.push_back(j < nb ? b[j] : -1);
     CNPC_REQUIRE(ctx, (int)rows.size() <= kMaxUnion, "too many staged rows");
     P.nunion = (int)rows.size();
-    for (int u = 0; u < P.nunion; ++u) {
-        P.union_field[u] = rows[u];
-        if (rows[u] != -1) ++P.ncopy;
-    }
+    for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
     P.g_row = 0;
     P.a_slot[0] = 1;
     P.b_slot[0] = b_base;
     P.ncell = ncell;
     P.field_stride = stride;
-    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && ((ncell * sizeof(float)) % 16 == 0) &&
+    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && (ncell % 4 == 0) &&
                           ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0),
                  "contraction needs 16-byte aligned fields, field_stride and ncell");
-    const size_t row_bytes = (size_t)kMmaStride * sizeof(float);
-    P.nstages = (int)std::min<size_t>(kMaxStages, (220 * 1024) / (P.nunion * row_bytes));
-    CNPC_REQUIRE(ctx, P.nstages >= 2, "too many staged rows for the shared-memory ring");
-    const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
+    const size_t smem = (size_t)kMmaWarps * 2 * P.nunion * kMmaRow * sizeof(float);
+    CNPC_REQUIRE(ctx, smem <= 220 * 1024, "too many staged rows for the warp slabs");
     const int64_t nchunks = (ncell + kMmaChunk - 1) / kMmaChunk;
     const int nblocks = (int)std::min<int64_t>(ctx->num_sms, nchunks);
     const int nparts = nblocks * kMmaWarps;
     int st = ensure_scratch(ctx, (size_t)nparts * mp * np_ * sizeof(double) + 256, s);
     if (st) return st;
-    int *status = reinterpret_cast<int *>(static_cast<char *>(ctx->scratch) + ctx->scratch_bytes - 256);
     double *part = (double *)ctx->scratch;
 #define CNPC_MMA_CASE(M_, N_)                                                                            \
     if (MT == M_ && NT == N_) {                                                                          \
@@ -525,7 +484,7 @@ static int run_gram_mma(cnpc_ctx *ctx, int64_t ncell, const float *g, const floa
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
                         "gram smem attribute");                                                          \
         if (st) return st;                                                                               \
-        gram_mma_kernel<M_, N_><<<nblocks, (kMmaWarps + 1) * 32, smem, s>>>(g, fields, P, part, status); \
+        gram_mma_kernel<M_, N_><<<nblocks, kMmaWarps * 32, smem, s>>>(g, fields, P, part);               \
     }
     CNPC_MMA_CASE(1, 1) CNPC_MMA_CASE(1, 2) CNPC_MMA_CASE(1, 3) CNPC_MMA_CASE(2, 1) CNPC_MMA_CASE(2, 2)
     CNPC_MMA_CASE(2, 3) CNPC_MMA_CASE(3, 1) CNPC_MMA_CASE(3, 2) CNPC_MMA_CASE(3, 3)

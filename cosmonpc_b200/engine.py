@@ -98,10 +98,9 @@ def kbin_counts(n, boxsize, edges):
 
 
 # ------------------------------------------------------------ shell fields
-# Extra elements between consecutive shell fields.  An n^3 float field is a
-# power-of-two number of bytes; rows that far apart land on the same memory
-# channels when a contraction streams dozens of them at once.
-FIELD_PAD = 1088
+# Extra elements between consecutive shell fields (0: contiguous batches,
+# which cuFFT writes fastest).
+FIELD_PAD = 0
 
 
 def leg_components(l, m):
