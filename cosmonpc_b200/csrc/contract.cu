@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 constexpr int kMmaWarps = 8;
 constexpr int kMmaChunk = 256;             // cells per block chunk (32 per warp)
 constexpr int kMmaRow = 36;                // padded slab row (32 cells + 4)
-constexpr int kMmaFlush = 8;               // chunks between FP64 folds
+constexpr int kMmaFlush = 1;               // chunks between FP64 folds (tensor-core FP32 sums are not round-to-nearest)
 
 __device__ inline uint32_t tf32_rna(float x) {
     uint32_t r;
