@@ -25,7 +25,7 @@ EXPORTED = (
     "cnpc_ctx_create", "cnpc_ctx_destroy", "cnpc_ctx_last_error", "cnpc_status_string",
     "cnpc_version", "cnpc_paint", "cnpc_fft_r2c", "cnpc_fft_c2r", "cnpc_forward_finish",
     "cnpc_kbin_counts", "cnpc_pk_bins", "cnpc_sn_bins", "cnpc_shell_spectra",
-    "cnpc_contract_gram",
+    "cnpc_contract_gram", "cnpc_contract_gram_noalloc",
 )
 
 
@@ -64,6 +64,7 @@ _SIGS = {
     "cnpc_shell_spectra": [_vp, _i, _i, _d, _vp, _vp, _dp, _i, ctypes.POINTER(Harmonic), _i,
                            ctypes.POINTER(ShellItem), _i, _vp, _vp],
     "cnpc_contract_gram": [_vp, _i, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
+    "cnpc_contract_gram_noalloc": [_i, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
 }
 
 _lib = None

@@ -618,3 +618,214 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free variant of cnpc_contract_gram.
+//
+// Some callers cannot let a library call cudaMalloc: an application that
+// hands the whole device to its own memory pool up front (so a library
+// allocation would fail or fragment the pool), or a pipeline that keeps other
+// streams busy and cannot afford the device-wide synchronisation that
+// cudaFree (and a growing cudaMalloc) may impose.  For them the per-block
+// partial sums of the contraction live in one fixed array in the library's
+// device memory instead of the context's scratch buffer.
+// ===========================================================================
+namespace cnpc {
+
+// 8 MiB of doubles per device: per-block partials plus a status word.  Every
+// GPU that loads the library holds this array until the process exits.
+constexpr size_t kNoAllocDoubles = (size_t)1 << 20;
+constexpr size_t kNoAllocStatusSlot = kNoAllocDoubles - 32;  // last 256 bytes
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[kNoAllocMaxDevices];
+static int g_noalloc_sms[kNoAllocMaxDevices];
+
+// Device address of the array for the current device.  The symbol's name in
+// host code is only a stand-in, so the address is fetched with
+// cudaGetSymbolAddress once per device (with that device current) and cached.
+static int noalloc_scratch(double **ptr, int *sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CNPC_ECUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return CNPC_EINVAL;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return CNPC_ECUDA;
+        }
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            return CNPC_ECUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+        g_noalloc_sms[dev] = n;
+    }
+    *ptr = g_noalloc_ptr[dev];
+    *sms = g_noalloc_sms[dev];
+    return CNPC_OK;
+}
+
+static int noalloc_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return CNPC_OK;
+    cudaGetLastError();
+    return CNPC_ECUDA;
+}
+
+static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, int64_t stride, const int *a,
+                            int na, const int *b, int nb, double *out, cudaStream_t s) {
+    const int MT = (na + 15) / 16, NT = (nb + 7) / 8;
+    if (MT > 3 || NT > 3) return CNPC_EINVAL;  // one launch: at most 48 x 24 outputs
+    if (((stride * sizeof(float)) % 16) || (ncell % 4) || ((uintptr_t)g % 16) || ((uintptr_t)fields % 16))
+        return CNPC_EINVAL;
+    double *scratch = nullptr;
+    int sms = 0;
+    int st = noalloc_scratch(&scratch, &sms);
+    if (st) return st;
+    GramParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.na = na;
+    P.nb = nb;
+    const int mp = MT * 16, np_ = NT * 8;
+    int b_off = -1;
+    for (int off = 0; off + nb <= na && b_off < 0; ++off) {
+        bool same = true;
+        for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
+        if (same && off + np_ <= mp) b_off = off;
+    }
+    std::vector<int> rows;
+    rows.push_back(-2);
+    for (int i = 0; i < mp; ++i) rows.push_back(i < na ? a[i] : -1);
+    const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
+    if (b_off < 0)
+        for (int j = 0; j < np_; ++j) rows.push_back(j < nb ? b[j] : -1);
+    P.nunion = (int)rows.size();
+    for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
+    P.g_row = 0;
+    P.a_slot[0] = 1;
+    P.b_slot[0] = b_base;
+    P.ncell = ncell;
+    P.field_stride = stride;
+    const size_t smem = (size_t)kMmaWarps * 2 * P.nunion * kMmaRow * sizeof(float);
+    if (smem > 220 * 1024) return CNPC_EINVAL;
+    // as many blocks as the fixed array can hold partials for
+    const size_t per_block = (size_t)kMmaWarps * mp * np_;
+    const int64_t nchunks = (ncell + kMmaChunk - 1) / kMmaChunk;
+    const int nblocks = (int)std::min<int64_t>(std::min<int64_t>(sms, nchunks), kNoAllocStatusSlot / per_block);
+    if (nblocks < 1) return CNPC_EINVAL;
+    const int nparts = nblocks * kMmaWarps;
+#define CNPC_NA_CASE(M_, N_)                                                                                  \
+    if (MT == M_ && NT == N_) {                                                                               \
+        st = noalloc_cuda(cudaFuncSetAttribute(gram_mma_kernel<M_, N_>,                                       \
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));      \
+        if (st) return st;                                                                                    \
+        gram_mma_kernel<M_, N_><<<nblocks, kMmaWarps * 32, smem, s>>>(g, fields, P, scratch);                 \
+    }
+    CNPC_NA_CASE(1, 1) CNPC_NA_CASE(1, 2) CNPC_NA_CASE(1, 3) CNPC_NA_CASE(2, 1) CNPC_NA_CASE(2, 2)
+    CNPC_NA_CASE(2, 3) CNPC_NA_CASE(3, 1) CNPC_NA_CASE(3, 2) CNPC_NA_CASE(3, 3)
+#undef CNPC_NA_CASE
+    st = noalloc_cuda(cudaGetLastError());
+    if (st) return st;
+    const int nout = na * nb;
+    gram_mma_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(scratch, nparts, mp, np_, na, nb, out);
+    return noalloc_cuda(cudaGetLastError());
+}
+
+static int noalloc_gram_f64(int64_t ncell, const double *g, const double *fields, int64_t stride, const int *a,
+                            int na, const int *b, int nb, double *out, cudaStream_t s) {
+    using Tile = Fp64Tile;
+    constexpr int TM = Tile::TM, TN = Tile::TN, NW = Tile::WARPS, CHUNK = Tile::CHUNK;
+    if (((stride * sizeof(double)) % 16) || ((ncell * sizeof(double)) % 16) || ((uintptr_t)g % 16) ||
+        ((uintptr_t)fields % 16))
+        return CNPC_EINVAL;
+    double *scratch = nullptr;
+    int sms = 0;
+    int st = noalloc_scratch(&scratch, &sms);
+    if (st) return st;
+    GramParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.na = na;
+    P.nb = nb;
+    const int na_pad = (na + TM - 1) / TM * TM;
+    const int nb_pad = (nb + TN - 1) / TN * TN;
+    int b_off = -1;
+    for (int off = 0; off + nb <= na && b_off < 0; ++off) {
+        bool same = true;
+        for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
+        if (same && off + nb_pad <= na_pad) b_off = off;
+    }
+    std::vector<int> rows;
+    rows.push_back(-2);
+    for (int i = 0; i < na_pad; ++i) rows.push_back(i < na ? a[i] : -1);
+    const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
+    if (b_off < 0)
+        for (int j = 0; j < nb_pad; ++j) rows.push_back(j < nb ? b[j] : -1);
+    if ((int)rows.size() > kMaxUnion) return CNPC_EINVAL;
+    P.nunion = (int)rows.size();
+    for (int u = 0; u < P.nunion; ++u) {
+        P.union_field[u] = rows[u];
+        if (rows[u] != -1) ++P.ncopy;
+    }
+    P.g_row = 0;
+    for (int i = 0; i < na; ++i) P.a_slot[i] = 1 + i;
+    for (int j = 0; j < nb; ++j) P.b_slot[j] = b_base + j;
+    P.ct = nb_pad / TN;
+    P.ntiles = (na_pad / TM) * P.ct;
+    P.ngroups = (P.ntiles + NW - 1) / NW;
+    P.ncell = ncell;
+    P.field_stride = stride;
+    const size_t row_bytes = (size_t)CHUNK * sizeof(double);
+    P.nstages = (int)std::min<size_t>(kMaxStages, (220 * 1024) / (P.nunion * row_bytes));
+    if (P.nstages < 2) return CNPC_EINVAL;
+    const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
+    P.flush_chunks = 1 << 30;
+    const size_t per_block = (size_t)NW * TM * TN;
+    const int64_t nchunks = (ncell + CHUNK - 1) / CHUNK;
+    int64_t nxr = std::min<int64_t>(std::max<int64_t>(1, sms / P.ngroups), nchunks);
+    nxr = std::min<int64_t>(nxr, (int64_t)(kNoAllocStatusSlot / per_block) / P.ngroups);
+    if (nxr < 1) return CNPC_EINVAL;
+    const int nblocks = (int)(nxr * P.ngroups);
+    int *status = reinterpret_cast<int *>(scratch + kNoAllocStatusSlot);
+    // the shared array keeps the previous call's contents: the bounded-wait
+    // status word must start at zero
+    st = noalloc_cuda(cudaMemsetAsync(status, 0, sizeof(int), s));
+    if (st) return st;
+    st = noalloc_cuda(
+        cudaFuncSetAttribute(gram_kernel<double, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (st) return st;
+    gram_kernel<double, NW><<<(unsigned)nblocks, NW * 32, smem, s>>>(g, fields, P, scratch, status);
+    st = noalloc_cuda(cudaGetLastError());
+    if (st) return st;
+    const int nout = na * nb;
+    gram_reduce_kernel<TM, TN, NW><<<(nout + 127) / 128, 128, 0, s>>>(scratch, nblocks, P.ngroups, P.ntiles, P.ct,
+                                                                      na, nb, out);
+    return noalloc_cuda(cudaGetLastError());
+}
+
+}  // namespace cnpc
+
+extern "C" int cnpc_contract_gram_noalloc(int dtype, int64_t ncell, const void *d_g, const void *d_fields,
+                                          int64_t field_stride, const int *h_a, int na, const int *h_b, int nb,
+                                          double *d_out, cnpc_stream_t stream) {
+    if (dtype != CNPC_F32 && dtype != CNPC_F64) return CNPC_EINVAL;
+    if (ncell < 1 || !d_g || !d_fields || !h_a || !h_b || !d_out || field_stride < ncell) return CNPC_EINVAL;
+    if (na < 1 || na > kMaxRows || nb < 1 || nb > kMaxRows) return CNPC_EINVAL;
+    for (int i = 0; i < na; ++i)
+        if (h_a[i] < 0) return CNPC_EINVAL;
+    for (int j = 0; j < nb; ++j)
+        if (h_b[j] < 0) return CNPC_EINVAL;
+    try {
+        cudaStream_t s = (cudaStream_t)stream;
+        if (dtype == CNPC_F32)
+            return noalloc_gram_f32(ncell, (const float *)d_g, (const float *)d_fields, field_stride, h_a, na, h_b,
+                                    nb, d_out, s);
+        return noalloc_gram_f64(ncell, (const double *)d_g, (const double *)d_fields, field_stride, h_a, na, h_b,
+                                nb, d_out, s);
+    } catch (...) {
+        return CNPC_EINVAL;
+    }
+}

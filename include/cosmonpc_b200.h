@@ -183,6 +183,29 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
                        const int *h_a, int na, const int *h_b, int nb, double *d_out,
                        cnpc_stream_t stream);
 
+/* Allocation-free form of cnpc_contract_gram.  It has no counterpart in the
+ * reference; it exists for callers that must not have a library allocate
+ * device memory, such as an application whose own pool owns the whole device,
+ * or one that cannot afford the device-wide synchronisation cudaFree may
+ * cause.  It takes no context and calls no cudaMalloc, cudaFree or allocating
+ * library routine: the per-block partial sums live in one fixed 8 MiB array in
+ * the library's device memory, which every GPU that loads the library holds
+ * until the process exits.  The caller still owns G, the fields and d_out.
+ *  - Limits per call: CNPC_F32 at most 48 rows x 24 columns (one tensor-core
+ *    launch); CNPC_F64 at most 128 x 128 with 1 + pad8(na) [+ pad4(nb) when
+ *    b is not a contiguous run of a] <= 110 staged rows.  Larger calls, or
+ *    misaligned fields (16-byte base, field_stride and ncell), return
+ *    CNPC_EINVAL.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) and caches it; make that first call before any
+ *    stream capture.
+ *  - All calls share the array, so calls whose work overlaps on the GPU (on
+ *    different streams, or from different threads) race and corrupt each
+ *    other's partial sums: serialise them. */
+int cnpc_contract_gram_noalloc(int dtype, int64_t ncell, const void *d_g, const void *d_fields,
+                               int64_t field_stride, const int *h_a, int na, const int *h_b, int nb,
+                               double *d_out, cnpc_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

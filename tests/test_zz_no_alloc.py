@@ -1,0 +1,65 @@
+"""The allocation-free contraction entry point against the regular one.
+
+cnpc_contract_gram_noalloc is for callers that cannot let the library call
+cudaMalloc (an application whose own memory pool owns the device, or one that
+cannot take the synchronisation cudaFree may cause); it keeps its partial sums
+in a fixed array in the library's device memory.  This file is collected last
+so that a run stopping at the first failure has already run every other test;
+it also passes alone in a fresh process.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": 1e-8, "f32": 1e-5}
+
+
+@pytest.mark.parametrize("precision,na,nb", [("f32", 40, 20), ("f32", 20, 20), ("f64", 40, 20), ("f64", 12, 7)])
+def test_noalloc_matches_gram_twice(precision, na, nb):
+    import torch
+
+    from cosmonpc_b200 import _lib, engine
+
+    code, rdt, _ = engine.PRECISION[precision]
+    ctx = _lib.Context.get()
+    lib = _lib.load()
+    n = 64
+    ncell = n ** 3
+    gen = torch.Generator(device="cuda").manual_seed(7 + na)
+    fields = torch.randn((48, ncell), dtype=rdt, device="cuda", generator=gen)
+    G = torch.randn(ncell, dtype=rdt, device="cuda", generator=gen)
+    a = list(range(na))
+    b = list(range(5, 5 + nb)) if na >= 5 + nb else list(range(nb))
+    ref = torch.empty((na, nb), dtype=torch.float64, device="cuda")
+    ctx.gram(code, ncell, G, fields, ncell, a, b, ref)
+    aa = (ctypes.c_int * na)(*a)
+    bb = (ctypes.c_int * nb)(*b)
+    stream = ctx.stream()
+    for _ in range(2):  # the shared array keeps the previous call's contents
+        out = torch.full((na, nb), float("nan"), dtype=torch.float64, device="cuda")
+        st = lib.cnpc_contract_gram_noalloc(code, ncell, ctypes.c_void_p(G.data_ptr()),
+                                            ctypes.c_void_p(fields.data_ptr()), ncell, aa, na, bb, nb,
+                                            ctypes.c_void_p(out.data_ptr()), stream)
+        assert st == _lib.CNPC_OK
+        torch.cuda.synchronize()
+        assert rel_err(out.cpu().numpy(), ref.cpu().numpy()) < TOL[precision]
+
+
+def test_noalloc_rejects_oversized_calls():
+    import torch
+
+    from cosmonpc_b200 import _lib
+
+    lib = _lib.load()
+    x = torch.zeros(1024, dtype=torch.float32, device="cuda")
+    out = torch.zeros(64 * 32, dtype=torch.float64, device="cuda")
+    a = (ctypes.c_int * 64)(*([0] * 64))
+    b = (ctypes.c_int * 32)(*([0] * 32))
+    st = lib.cnpc_contract_gram_noalloc(_lib.F32, 1024, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(x.data_ptr()),
+                                        1024, a, 64, b, 32, ctypes.c_void_p(out.data_ptr()), None)
+    assert st == _lib.CNPC_EINVAL
