@@ -273,39 +273,19 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 
 
 // ---------------------------------------------------------------------------
-// FP32 fields on the tensor cores.  The Gram is the GEMM
-//   C[a][b] = sum_k A[a][k] B[k][b],  A[a][k] = G(k) F_a(k),  B[k][b] = F_b(k)
-// with K = cells.  Each operand is split into two TF32 parts (x = hi + lo,
-// hi = rna_tf32(x), lo = rna_tf32(x - hi)) and C accumulates
-// Al*Bh + Ah*Bl + Ah*Bh with mma.sync m16n8k8 (FP32 accumulate): products
-// carry ~22 significant bits, as good as FP32 fields.
-//
-// Every warp is independent: it owns the whole (16 MT) x (8 NT) output for a
-// 32-cell slab of each chunk, streams its slab of every staged row with 16-byte
-// cp.async into a private double-buffered shared-memory tile (padded rows, so
-// the fragment loads are bank-conflict free) while it contracts the previous
-// slab, and folds its FP32 fragments into FP64 registers every 8 chunks.
-constexpr int kMmaWarps = 8;
-constexpr int kMmaChunk = 256;             // cells per block chunk (32 per warp)
-constexpr int kMmaRow = 36;                // padded slab row (32 cells + 4)
-constexpr int kMmaFlush = 1;               // chunks between FP64 folds (tensor-core FP32 sums are not round-to-nearest)
+// FP32 fields.  Every warp is independent: it owns a (8 RB) x (4 CB) output
+// window for a 32-cell slab of each block chunk, streams that slab of every
+// staged row with 16-byte cp.async into a private double-buffered shared-memory
+// tile (rows padded to 36 floats), and contracts the previous slab meanwhile.
+// Lane (g, h) = (lane / 4, lane % 4) owns rows g + 8 r and columns h + 4 q, so a
+// shared-memory load of one row is either a broadcast or hits 8 distinct
+// banks.  Two adjacent cells are read per 8-byte load and accumulated with
+// packed FP32x2 FMAs (even and odd cell partial sums); the FP32 partials are
+// folded into FP64 registers after every chunk (32 cells per lane).
+constexpr int kFfWarps = 8;
+constexpr int kFfChunk = 256;  // cells per block chunk (32 per warp)
+constexpr int kFfRow = 36;     // padded slab row (32 cells + 4)
 
-__device__ inline uint32_t tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-__device__ inline void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
-    hi = tf32_rna(x);
-    lo = tf32_rna(x - __uint_as_float(hi));
-}
-__device__ inline void mma_tf32(float *c, const uint32_t *a, const uint32_t *b) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 __device__ inline void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -314,30 +294,30 @@ template <int N> __device__ inline void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int MT, int NT>
-__global__ void __launch_bounds__(kMmaWarps * 32, 1)
-    gram_mma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
-                    double *partial) {
-    constexpr int MP = MT * 16, NP = NT * 8;
+template <int RB, int CB>
+__global__ void __launch_bounds__(kFfWarps * 32, 1)
+    gram_ffma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
+                     double *partial) {
+    constexpr int WR = 8 * RB, WC = 4 * CB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int nrows = P.nunion;  // staged rows: G, A rows (padded), separate B rows (padded)
-    const int slab = nrows * kMmaRow;
+    const int nrows = P.nunion;  // staged rows: G, A window, separate B window
+    const int slab = nrows * kFfRow;
     float *const buf0 = reinterpret_cast<float *>(smem_raw) + (size_t)warp * 2 * slab;
-    const int64_t nchunk_all = (P.ncell + kMmaChunk - 1) / kMmaChunk;
+    const int64_t nchunk_all = (P.ncell + kFfChunk - 1) / kFfChunk;
     const int nchunk = blockIdx.x < nchunk_all ? (int)((nchunk_all - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
     // stream this warp's 32-cell slab of chunk k into buffer b
     auto issue = [&](int k, int b) {
-        const int64_t c0 = ((int64_t)blockIdx.x + (int64_t)k * gridDim.x) * kMmaChunk + warp * 32;
+        const int64_t c0 = ((int64_t)blockIdx.x + (int64_t)k * gridDim.x) * kFfChunk + warp * 32;
         float *dst = buf0 + b * slab;
         for (int idx = lane; idx < nrows * 8; idx += 32) {
             const int row = idx >> 3, part = idx & 7;
             const int f = P.union_field[row];
             if (f == -1) continue;  // padding row: only feeds discarded outputs
             const int64_t cell = c0 + part * 4;
-            float *d = dst + row * kMmaRow + part * 4;
+            float *d = dst + row * kFfRow + part * 4;
             if (cell < P.ncell)  // ncell is a multiple of 4, so the 16 bytes are all valid
                 cp_async16(d, (f == -2 ? g : fields + (int64_t)f * P.field_stride) + cell);
             else
@@ -346,22 +326,19 @@ __global__ void __launch_bounds__(kMmaWarps * 32, 1)
         cp_async_commit();
     };
 
-    const int gid = lane >> 2, tig = lane & 3;
-    const int a_row0 = P.a_slot[0];
-    const int b_row0 = P.b_slot[0];
-    float acc[MT][NT][4];
-    double acc64[MT][NT][4];
+    const int gl = lane >> 2, hl = lane & 3;
+    const int a_row = P.a_slot[0] + gl;  // rows a_row + 8 r
+    const int b_row = P.b_slot[0] + hl;  // rows b_row + 4 q
+    float2 acc[RB][CB];
+    double acc64[RB][CB];
 #pragma unroll
-    for (int m = 0; m < MT; ++m)
+    for (int r = 0; r < RB; ++r)
 #pragma unroll
-        for (int n = 0; n < NT; ++n)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                acc[m][n][e] = 0.f;
-                acc64[m][n][e] = 0.0;
-            }
+        for (int q = 0; q < CB; ++q) {
+            acc[r][q] = make_float2(0.f, 0.f);
+            acc64[r][q] = 0.0;
+        }
     if (nchunk > 0) issue(0, 0);
-    int since_flush = 0;
     for (int k = 0; k < nchunk; ++k) {
         if (k + 1 < nchunk) {
             issue(k + 1, (k + 1) & 1);
@@ -371,95 +348,81 @@ __global__ void __launch_bounds__(kMmaWarps * 32, 1)
         }
         __syncwarp();
         const float *sb = buf0 + (k & 1) * slab;
+        const float *rg = sb + P.g_row * kFfRow;
+        const float *ra = sb + a_row * kFfRow;
+        const float *rb = sb + b_row * kFfRow;
 #pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            const int k0 = ks * 8;
-            const float g0 = sb[P.g_row * kMmaRow + k0 + tig];
-            const float g1 = sb[P.g_row * kMmaRow + k0 + tig + 4];
-            uint32_t bh[NT][2], bl[NT][2];
+        for (int c = 0; c < 32; c += 2) {
+            const float2 g2 = *reinterpret_cast<const float2 *>(rg + c);
+            float2 a2[RB], b2[CB];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                const float *rb = sb + (b_row0 + n * 8 + gid) * kMmaRow + k0 + tig;
-                split_tf32(rb[0], bh[n][0], bl[n][0]);
-                split_tf32(rb[4], bh[n][1], bl[n][1]);
-            }
+            for (int r = 0; r < RB; ++r)
+                a2[r] = __fmul2_rn(g2, *reinterpret_cast<const float2 *>(ra + 8 * r * kFfRow + c));
 #pragma unroll
-            for (int m = 0; m < MT; ++m) {
-                const float *ra = sb + (a_row0 + m * 16 + gid) * kMmaRow + k0 + tig;
-                uint32_t ah[4], al[4];
-                split_tf32(g0 * ra[0], ah[0], al[0]);
-                split_tf32(g0 * ra[8 * kMmaRow], ah[1], al[1]);
-                split_tf32(g1 * ra[4], ah[2], al[2]);
-                split_tf32(g1 * ra[8 * kMmaRow + 4], ah[3], al[3]);
+            for (int q = 0; q < CB; ++q) b2[q] = *reinterpret_cast<const float2 *>(rb + 4 * q * kFfRow + c);
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    mma_tf32(acc[m][n], al, bh[n]);
-                    mma_tf32(acc[m][n], ah, bl[n]);
-                    mma_tf32(acc[m][n], ah, bh[n]);
-                }
-            }
+            for (int r = 0; r < RB; ++r)
+#pragma unroll
+                for (int q = 0; q < CB; ++q) acc[r][q] = __ffma2_rn(a2[r], b2[q], acc[r][q]);
         }
         __syncwarp();  // the slab is refilled by the issue of iteration k + 1
-        if (++since_flush == kMmaFlush) {
-            since_flush = 0;
 #pragma unroll
-            for (int m = 0; m < MT; ++m)
+        for (int r = 0; r < RB; ++r)
 #pragma unroll
-                for (int n = 0; n < NT; ++n)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        acc64[m][n][e] += (double)acc[m][n][e];
-                        acc[m][n][e] = 0.f;
-                    }
-        }
-    }
-    double *dst = partial + ((int64_t)blockIdx.x * kMmaWarps + warp) * (MP * NP);
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < NT; ++n)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int row = m * 16 + gid + ((e & 2) ? 8 : 0);
-                const int col = n * 8 + 2 * tig + (e & 1);
-                dst[row * NP + col] = acc64[m][n][e] + (double)acc[m][n][e];
+            for (int q = 0; q < CB; ++q) {
+                acc64[r][q] += (double)acc[r][q].x + (double)acc[r][q].y;
+                acc[r][q] = make_float2(0.f, 0.f);
             }
+    }
+    double *dst = partial + ((int64_t)blockIdx.x * kFfWarps + warp) * (WR * WC);
+#pragma unroll
+    for (int r = 0; r < RB; ++r)
+#pragma unroll
+        for (int q = 0; q < CB; ++q) dst[(gl + 8 * r) * WC + hl + 4 * q] = acc64[r][q];
 }
 
-__global__ void gram_mma_reduce_kernel(const double *partial, int nparts, int mp, int np_, int na, int nb,
-                                       double *out) {
+__global__ void gram_window_reduce_kernel(const double *partial, int nparts, int wr, int wc, int na, int nb,
+                                          double *out) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= na * nb) return;
     const int i = o / nb, j = o % nb;
     double s = 0.0;
-    for (int p = 0; p < nparts; ++p) s += partial[(int64_t)p * mp * np_ + i * np_ + j];
+    for (int p = 0; p < nparts; ++p) s += partial[(int64_t)p * wr * wc + i * wc + j];
     out[o] = s;
 }
 
-static int run_gram_mma(cnpc_ctx *ctx, int64_t ncell, const float *g, const float *fields, int64_t stride,
-                        const int *a, int na, const int *b, int nb, double *out, cudaStream_t s) {
-    const int MT = (na + 15) / 16, NT = (nb + 7) / 8;
-    CNPC_REQUIRE(ctx, MT <= 3 && NT <= 3, "FP32 Gram launch covers at most 48 x 24 outputs");
+// Staged rows and window of an FP32 Gram launch (na <= 48, nb <= 24).
+struct FfPlan {
     GramParams P;
+    int RB, CB, wr, wc;
+    size_t smem;
+};
+
+static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const int *b, int nb, FfPlan *pl) {
+    GramParams &P = pl->P;
     std::memset(&P, 0, sizeof(P));
+    pl->RB = (na + 7) / 8;
+    pl->CB = (nb + 3) / 4;
+    if (pl->RB > 6 || pl->CB > 6) return false;
+    pl->wr = 8 * pl->RB;
+    pl->wc = 4 * pl->CB;
     P.na = na;
     P.nb = nb;
-    const int mp = MT * 16, np_ = NT * 8;
-    // staged rows: [G][A rows padded to 16 MT][B rows padded to 8 NT unless B is a
-    // contiguous run of A whose padding stays inside the A rows]
+    // staged rows: [G][A window][B window unless B is a contiguous run of A whose
+    // window stays inside the A window]
     int b_off = -1;
     for (int off = 0; off + nb <= na && b_off < 0; ++off) {
         bool same = true;
         for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
-        if (same && off + np_ <= mp) b_off = off;
+        if (same && off + pl->wc <= pl->wr) b_off = off;
     }
     std::vector<int> rows;
     rows.push_back(-2);
-    for (int i = 0; i < mp; ++i) rows.push_back(i < na ? a[i] : -1);
+    for (int i = 0; i < pl->wr; ++i) rows.push_back(i < na ? a[i] : -1);
     const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
     if (b_off < 0)
-        for (int j = 0; j < np_; ++j) rows.push_back(j < nb ? b[j] : -1);
-    CNPC_REQUIRE(ctx, (int)rows.size() <= kMaxUnion, "too many staged rows");
+        for (int j = 0; j < pl->wc; ++j) rows.push_back(j < nb ? b[j] : -1);
+    if ((int)rows.size() > kMaxUnion) return false;
     P.nunion = (int)rows.size();
     for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
     P.g_row = 0;
@@ -467,33 +430,48 @@ static int run_gram_mma(cnpc_ctx *ctx, int64_t ncell, const float *g, const floa
     P.b_slot[0] = b_base;
     P.ncell = ncell;
     P.field_stride = stride;
-    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && (ncell % 4 == 0) &&
-                          ((uintptr_t)g % 16 == 0) && ((uintptr_t)fields % 16 == 0),
+    pl->smem = (size_t)kFfWarps * 2 * P.nunion * kFfRow * sizeof(float);
+    return pl->smem <= 220 * 1024;
+}
+
+static cudaError_t ff_launch(const FfPlan &pl, int nblocks, const float *g, const float *fields, double *part,
+                             cudaStream_t s) {
+    cudaError_t e = cudaErrorInvalidValue;
+#define CNPC_FF_CASE(R_, C_)                                                                                  \
+    if (pl.RB == R_ && pl.CB == C_) {                                                                         \
+        e = cudaFuncSetAttribute(gram_ffma_kernel<R_, C_>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                 (int)pl.smem);                                                               \
+        if (e != cudaSuccess) return e;                                                                       \
+        gram_ffma_kernel<R_, C_><<<nblocks, kFfWarps * 32, pl.smem, s>>>(g, fields, pl.P, part);              \
+        return cudaGetLastError();                                                                            \
+    }
+#define CNPC_FF_ROW(R_) \
+    CNPC_FF_CASE(R_, 1) CNPC_FF_CASE(R_, 2) CNPC_FF_CASE(R_, 3) CNPC_FF_CASE(R_, 4) CNPC_FF_CASE(R_, 5) CNPC_FF_CASE(R_, 6)
+    CNPC_FF_ROW(1) CNPC_FF_ROW(2) CNPC_FF_ROW(3) CNPC_FF_ROW(4) CNPC_FF_ROW(5) CNPC_FF_ROW(6)
+#undef CNPC_FF_ROW
+#undef CNPC_FF_CASE
+    return e;
+}
+
+static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const float *fields, int64_t stride,
+                         const int *a, int na, const int *b, int nb, double *out, cudaStream_t s) {
+    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && (ncell % 4 == 0) && ((uintptr_t)g % 16 == 0) &&
+                          ((uintptr_t)fields % 16 == 0),
                  "contraction needs 16-byte aligned fields, field_stride and ncell");
-    const size_t smem = (size_t)kMmaWarps * 2 * P.nunion * kMmaRow * sizeof(float);
-    CNPC_REQUIRE(ctx, smem <= 220 * 1024, "too many staged rows for the warp slabs");
-    const int64_t nchunks = (ncell + kMmaChunk - 1) / kMmaChunk;
+    FfPlan pl;
+    CNPC_REQUIRE(ctx, ff_plan(ncell, stride, a, na, b, nb, &pl),
+                 "FP32 Gram launch covers at most 48 x 24 outputs");
+    const int64_t nchunks = (ncell + kFfChunk - 1) / kFfChunk;
     const int nblocks = (int)std::min<int64_t>(ctx->num_sms, nchunks);
-    const int nparts = nblocks * kMmaWarps;
-    int st = ensure_scratch(ctx, (size_t)nparts * mp * np_ * sizeof(double) + 256, s);
+    const int nparts = nblocks * kFfWarps;
+    int st = ensure_scratch(ctx, (size_t)nparts * pl.wr * pl.wc * sizeof(double) + 256, s);
     if (st) return st;
     double *part = (double *)ctx->scratch;
-#define CNPC_MMA_CASE(M_, N_)                                                                            \
-    if (MT == M_ && NT == N_) {                                                                          \
-        st = check_cuda(ctx, cudaFuncSetAttribute(gram_mma_kernel<M_, N_>,                               \
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
-                        "gram smem attribute");                                                          \
-        if (st) return st;                                                                               \
-        gram_mma_kernel<M_, N_><<<nblocks, kMmaWarps * 32, smem, s>>>(g, fields, P, part);               \
-    }
-    CNPC_MMA_CASE(1, 1) CNPC_MMA_CASE(1, 2) CNPC_MMA_CASE(1, 3) CNPC_MMA_CASE(2, 1) CNPC_MMA_CASE(2, 2)
-    CNPC_MMA_CASE(2, 3) CNPC_MMA_CASE(3, 1) CNPC_MMA_CASE(3, 2) CNPC_MMA_CASE(3, 3)
-#undef CNPC_MMA_CASE
-    st = check_launch(ctx, "gram_mma_kernel");
+    st = check_cuda(ctx, ff_launch(pl, nblocks, g, fields, part, s), "gram_ffma_kernel");
     if (st) return st;
     const int nout = na * nb;
-    gram_mma_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(part, nparts, mp, np_, na, nb, out);
-    return check_launch(ctx, "gram_mma_reduce_kernel");
+    gram_window_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
+    return check_launch(ctx, "gram_window_reduce_kernel");
 }
 
 // out[i, j] = sum over every block of the group owning tile(i, j) and every
@@ -611,8 +589,8 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
     for (int j = 0; j < nb; ++j) CNPC_REQUIRE(ctx, h_b[j] >= 0, "negative field index");
     cudaStream_t s = (cudaStream_t)stream;
     if (dtype == CNPC_F32)
-        return run_gram_mma(ctx, ncell, (const float *)d_g, (const float *)d_fields, field_stride, h_a, na,
-                            h_b, nb, d_out, s);
+        return run_gram_ffma(ctx, ncell, (const float *)d_g, (const float *)d_fields, field_stride, h_a, na,
+                             h_b, nb, d_out, s);
     return run_gram<double>(ctx, ncell, (const double *)d_g, (const double *)d_fields, field_stride,
                             h_a, na, h_b, nb, d_out, s);
 }
@@ -678,60 +656,24 @@ static int noalloc_cuda(cudaError_t e) {
 
 static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, int64_t stride, const int *a,
                             int na, const int *b, int nb, double *out, cudaStream_t s) {
-    const int MT = (na + 15) / 16, NT = (nb + 7) / 8;
-    if (MT > 3 || NT > 3) return CNPC_EINVAL;  // one launch: at most 48 x 24 outputs
     if (((stride * sizeof(float)) % 16) || (ncell % 4) || ((uintptr_t)g % 16) || ((uintptr_t)fields % 16))
         return CNPC_EINVAL;
+    FfPlan pl;
+    if (!ff_plan(ncell, stride, a, na, b, nb, &pl)) return CNPC_EINVAL;  // one launch: at most 48 x 24
     double *scratch = nullptr;
     int sms = 0;
     int st = noalloc_scratch(&scratch, &sms);
     if (st) return st;
-    GramParams P;
-    std::memset(&P, 0, sizeof(P));
-    P.na = na;
-    P.nb = nb;
-    const int mp = MT * 16, np_ = NT * 8;
-    int b_off = -1;
-    for (int off = 0; off + nb <= na && b_off < 0; ++off) {
-        bool same = true;
-        for (int j = 0; j < nb && same; ++j) same = a[off + j] == b[j];
-        if (same && off + np_ <= mp) b_off = off;
-    }
-    std::vector<int> rows;
-    rows.push_back(-2);
-    for (int i = 0; i < mp; ++i) rows.push_back(i < na ? a[i] : -1);
-    const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
-    if (b_off < 0)
-        for (int j = 0; j < np_; ++j) rows.push_back(j < nb ? b[j] : -1);
-    P.nunion = (int)rows.size();
-    for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
-    P.g_row = 0;
-    P.a_slot[0] = 1;
-    P.b_slot[0] = b_base;
-    P.ncell = ncell;
-    P.field_stride = stride;
-    const size_t smem = (size_t)kMmaWarps * 2 * P.nunion * kMmaRow * sizeof(float);
-    if (smem > 220 * 1024) return CNPC_EINVAL;
     // as many blocks as the fixed array can hold partials for
-    const size_t per_block = (size_t)kMmaWarps * mp * np_;
-    const int64_t nchunks = (ncell + kMmaChunk - 1) / kMmaChunk;
+    const size_t per_block = (size_t)kFfWarps * pl.wr * pl.wc;
+    const int64_t nchunks = (ncell + kFfChunk - 1) / kFfChunk;
     const int nblocks = (int)std::min<int64_t>(std::min<int64_t>(sms, nchunks), kNoAllocStatusSlot / per_block);
     if (nblocks < 1) return CNPC_EINVAL;
-    const int nparts = nblocks * kMmaWarps;
-#define CNPC_NA_CASE(M_, N_)                                                                                  \
-    if (MT == M_ && NT == N_) {                                                                               \
-        st = noalloc_cuda(cudaFuncSetAttribute(gram_mma_kernel<M_, N_>,                                       \
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));      \
-        if (st) return st;                                                                                    \
-        gram_mma_kernel<M_, N_><<<nblocks, kMmaWarps * 32, smem, s>>>(g, fields, P, scratch);                 \
-    }
-    CNPC_NA_CASE(1, 1) CNPC_NA_CASE(1, 2) CNPC_NA_CASE(1, 3) CNPC_NA_CASE(2, 1) CNPC_NA_CASE(2, 2)
-    CNPC_NA_CASE(2, 3) CNPC_NA_CASE(3, 1) CNPC_NA_CASE(3, 2) CNPC_NA_CASE(3, 3)
-#undef CNPC_NA_CASE
-    st = noalloc_cuda(cudaGetLastError());
+    st = noalloc_cuda(ff_launch(pl, nblocks, g, fields, scratch, s));
     if (st) return st;
     const int nout = na * nb;
-    gram_mma_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(scratch, nparts, mp, np_, na, nb, out);
+    gram_window_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na,
+                                                                 nb, out);
     return noalloc_cuda(cudaGetLastError());
 }
 
