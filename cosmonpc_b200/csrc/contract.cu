@@ -294,7 +294,7 @@ template <int N> __device__ inline void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int RB, int CB>
+template <int RB, int CB, int NBUF>
 __global__ void __launch_bounds__(kFfWarps * 32, 1)
     gram_ffma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
                      double *partial) {
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
     const int warp = threadIdx.x >> 5;
     const int nrows = P.nunion;  // staged rows: G, A window, separate B window
     const int slab = nrows * kFfRow;
-    float *const buf0 = reinterpret_cast<float *>(smem_raw) + (size_t)warp * 2 * slab;
+    float *const buf0 = reinterpret_cast<float *>(smem_raw) + (size_t)warp * NBUF * slab;
     const int64_t nchunk_all = (P.ncell + kFfChunk - 1) / kFfChunk;
     const int nchunk = blockIdx.x < nchunk_all ? (int)((nchunk_all - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
@@ -338,16 +338,19 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
             acc[r][q] = make_float2(0.f, 0.f);
             acc64[r][q] = 0.0;
         }
-    if (nchunk > 0) issue(0, 0);
+    // NBUF-deep ring per warp: chunks k+1 .. k+NBUF-1 stream in while chunk k
+    // is contracted; an empty commit keeps one cp.async group per chunk slot
+    for (int j = 0; j < NBUF - 1; ++j) {
+        if (j < nchunk) issue(j, j);
+        else cp_async_commit();
+    }
     for (int k = 0; k < nchunk; ++k) {
-        if (k + 1 < nchunk) {
-            issue(k + 1, (k + 1) & 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        const int kn = k + NBUF - 1;
+        if (kn < nchunk) issue(kn, kn % NBUF);
+        else cp_async_commit();
+        cp_async_wait<NBUF - 1>();  // the group of chunk k has landed
         __syncwarp();
-        const float *sb = buf0 + (k & 1) * slab;
+        const float *sb = buf0 + (k % NBUF) * slab;
         const float *rg = sb + P.g_row * kFfRow;
         const float *ra = sb + a_row * kFfRow;
         const float *rb = sb + b_row * kFfRow;
@@ -365,7 +368,7 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
 #pragma unroll
                 for (int q = 0; q < CB; ++q) acc[r][q] = __ffma2_rn(a2[r], b2[q], acc[r][q]);
         }
-        __syncwarp();  // the slab is refilled by the issue of iteration k + 1
+        __syncwarp();  // this slot is refilled by the issue of iteration k + 1
 #pragma unroll
         for (int r = 0; r < RB; ++r)
 #pragma unroll
@@ -394,7 +397,7 @@ __global__ void gram_window_reduce_kernel(const double *partial, int nparts, int
 // Staged rows and window of an FP32 Gram launch (na <= 48, nb <= 24).
 struct FfPlan {
     GramParams P;
-    int RB, CB, wr, wc;
+    int RB, CB, wr, wc, nbuf;
     size_t smem;
 };
 
@@ -430,27 +433,39 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
     P.b_slot[0] = b_base;
     P.ncell = ncell;
     P.field_stride = stride;
-    pl->smem = (size_t)kFfWarps * 2 * P.nunion * kFfRow * sizeof(float);
-    return pl->smem <= 220 * 1024;
+    const size_t per_buf = (size_t)kFfWarps * P.nunion * kFfRow * sizeof(float);
+    pl->nbuf = (int)std::min<size_t>(4, (220 * 1024) / per_buf);
+    pl->smem = pl->nbuf * per_buf;
+    return pl->nbuf >= 2;
+}
+
+template <int R_, int C_>
+static cudaError_t ff_launch_rc(const FfPlan &pl, int nblocks, const float *g, const float *fields, double *part,
+                                cudaStream_t s) {
+    cudaError_t e;
+#define CNPC_FF_NB(NB_)                                                                                       \
+    if (pl.nbuf == NB_) {                                                                                     \
+        e = cudaFuncSetAttribute(gram_ffma_kernel<R_, C_, NB_>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                 (int)pl.smem);                                                               \
+        if (e != cudaSuccess) return e;                                                                       \
+        gram_ffma_kernel<R_, C_, NB_><<<nblocks, kFfWarps * 32, pl.smem, s>>>(g, fields, pl.P, part);         \
+        return cudaGetLastError();                                                                            \
+    }
+    CNPC_FF_NB(2) CNPC_FF_NB(3) CNPC_FF_NB(4)
+#undef CNPC_FF_NB
+    return cudaErrorInvalidValue;
 }
 
 static cudaError_t ff_launch(const FfPlan &pl, int nblocks, const float *g, const float *fields, double *part,
                              cudaStream_t s) {
-    cudaError_t e = cudaErrorInvalidValue;
-#define CNPC_FF_CASE(R_, C_)                                                                                  \
-    if (pl.RB == R_ && pl.CB == C_) {                                                                         \
-        e = cudaFuncSetAttribute(gram_ffma_kernel<R_, C_>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
-                                 (int)pl.smem);                                                               \
-        if (e != cudaSuccess) return e;                                                                       \
-        gram_ffma_kernel<R_, C_><<<nblocks, kFfWarps * 32, pl.smem, s>>>(g, fields, pl.P, part);              \
-        return cudaGetLastError();                                                                            \
-    }
+#define CNPC_FF_CASE(R_, C_) \
+    if (pl.RB == R_ && pl.CB == C_) return ff_launch_rc<R_, C_>(pl, nblocks, g, fields, part, s);
 #define CNPC_FF_ROW(R_) \
     CNPC_FF_CASE(R_, 1) CNPC_FF_CASE(R_, 2) CNPC_FF_CASE(R_, 3) CNPC_FF_CASE(R_, 4) CNPC_FF_CASE(R_, 5) CNPC_FF_CASE(R_, 6)
     CNPC_FF_ROW(1) CNPC_FF_ROW(2) CNPC_FF_ROW(3) CNPC_FF_ROW(4) CNPC_FF_ROW(5) CNPC_FF_ROW(6)
 #undef CNPC_FF_ROW
 #undef CNPC_FF_CASE
-    return e;
+    return cudaErrorInvalidValue;
 }
 
 static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const float *fields, int64_t stride,
