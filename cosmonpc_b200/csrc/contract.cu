@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 constexpr int kFfWarps = 8;
 constexpr int kFfChunk = 256;  // cells per block chunk (32 per warp)
 constexpr int kFfRow = 36;     // padded slab row (32 cells + 4)
+constexpr int kFfFold = 4;     // chunks per FP32 partial (128 cells per lane)
 
 __device__ inline void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
@@ -295,7 +296,7 @@ template <int N> __device__ inline void cp_async_wait() {
 }
 
 template <int RB, int CB, int NBUF>
-__global__ void __launch_bounds__(kFfWarps * 32, 1)
+__global__ void __launch_bounds__(kFfWarps * 32, 2)
     gram_ffma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
                      double *partial) {
     constexpr int WR = 8 * RB, WC = 4 * CB;
@@ -329,15 +330,26 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
     const int gl = lane >> 2, hl = lane & 3;
     const int a_row = P.a_slot[0] + gl;  // rows a_row + 8 r
     const int b_row = P.b_slot[0] + hl;  // rows b_row + 4 q
+    // FP32 partials are folded every kFfFold chunks into this warp's own FP64
+    // partial in global memory (L2 resident), keeping registers for the tile
+    double *dst = partial + ((int64_t)blockIdx.x * kFfWarps + warp) * (WR * WC);
     float2 acc[RB][CB];
-    double acc64[RB][CB];
 #pragma unroll
     for (int r = 0; r < RB; ++r)
 #pragma unroll
-        for (int q = 0; q < CB; ++q) {
-            acc[r][q] = make_float2(0.f, 0.f);
-            acc64[r][q] = 0.0;
-        }
+        for (int q = 0; q < CB; ++q) acc[r][q] = make_float2(0.f, 0.f);
+    bool stored = false;
+    auto fold = [&]() {
+#pragma unroll
+        for (int r = 0; r < RB; ++r)
+#pragma unroll
+            for (int q = 0; q < CB; ++q) {
+                double *p = dst + (gl + 8 * r) * WC + hl + 4 * q;
+                *p = (stored ? *p : 0.0) + ((double)acc[r][q].x + (double)acc[r][q].y);
+                acc[r][q] = make_float2(0.f, 0.f);
+            }
+        stored = true;
+    };
     // NBUF-deep ring per warp: chunks k+1 .. k+NBUF-1 stream in while chunk k
     // is contracted; an empty commit keeps one cp.async group per chunk slot
     for (int j = 0; j < NBUF - 1; ++j) {
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
         const float *rg = sb + P.g_row * kFfRow;
         const float *ra = sb + a_row * kFfRow;
         const float *rb = sb + b_row * kFfRow;
-#pragma unroll
+#pragma unroll 4
         for (int c = 0; c < 32; c += 2) {
             const float2 g2 = *reinterpret_cast<const float2 *>(rg + c);
             float2 a2[RB], b2[CB];
@@ -369,19 +381,9 @@ __global__ void __launch_bounds__(kFfWarps * 32, 1)
                 for (int q = 0; q < CB; ++q) acc[r][q] = __ffma2_rn(a2[r], b2[q], acc[r][q]);
         }
         __syncwarp();  // this slot is refilled by the issue of iteration k + 1
-#pragma unroll
-        for (int r = 0; r < RB; ++r)
-#pragma unroll
-            for (int q = 0; q < CB; ++q) {
-                acc64[r][q] += (double)acc[r][q].x + (double)acc[r][q].y;
-                acc[r][q] = make_float2(0.f, 0.f);
-            }
+        if ((k + 1) % kFfFold == 0) fold();
     }
-    double *dst = partial + ((int64_t)blockIdx.x * kFfWarps + warp) * (WR * WC);
-#pragma unroll
-    for (int r = 0; r < RB; ++r)
-#pragma unroll
-        for (int q = 0; q < CB; ++q) dst[(gl + 8 * r) * WC + hl + 4 * q] = acc64[r][q];
+    fold();  // also defines the partial of a warp that had no chunk
 }
 
 __global__ void gram_window_reduce_kernel(const double *partial, int nparts, int wr, int wc, int na, int nb,
@@ -433,8 +435,9 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
     P.b_slot[0] = b_base;
     P.ncell = ncell;
     P.field_stride = stride;
+    // two blocks per SM: ~110 KB of slabs each
     const size_t per_buf = (size_t)kFfWarps * P.nunion * kFfRow * sizeof(float);
-    pl->nbuf = (int)std::min<size_t>(4, (220 * 1024) / per_buf);
+    pl->nbuf = (int)std::min<size_t>(4, (110 * 1024) / per_buf);
     pl->smem = pl->nbuf * per_buf;
     return pl->nbuf >= 2;
 }
@@ -477,7 +480,7 @@ static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const flo
     CNPC_REQUIRE(ctx, ff_plan(ncell, stride, a, na, b, nb, &pl),
                  "FP32 Gram launch covers at most 48 x 24 outputs");
     const int64_t nchunks = (ncell + kFfChunk - 1) / kFfChunk;
-    const int nblocks = (int)std::min<int64_t>(ctx->num_sms, nchunks);
+    const int nblocks = (int)std::min<int64_t>(2 * ctx->num_sms, nchunks);
     const int nparts = nblocks * kFfWarps;
     int st = ensure_scratch(ctx, (size_t)nparts * pl.wr * pl.wc * sizeof(double) + 256, s);
     if (st) return st;
@@ -682,7 +685,8 @@ static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, 
     // as many blocks as the fixed array can hold partials for
     const size_t per_block = (size_t)kFfWarps * pl.wr * pl.wc;
     const int64_t nchunks = (ncell + kFfChunk - 1) / kFfChunk;
-    const int nblocks = (int)std::min<int64_t>(std::min<int64_t>(sms, nchunks), kNoAllocStatusSlot / per_block);
+    const int nblocks =
+        (int)std::min<int64_t>(std::min<int64_t>(2 * sms, nchunks), kNoAllocStatusSlot / per_block);
     if (nblocks < 1) return CNPC_EINVAL;
     st = noalloc_cuda(ff_launch(pl, nblocks, g, fields, scratch, s));
     if (st) return st;
