@@ -49,6 +49,11 @@ __device__ inline double kcomp(int n_int, double boxsize) {
 
 // |k| = sqrt((kx^2 + ky^2) + kz^2) with every operation rounded separately
 // (no FMA contraction), which reproduces numpy's value bit for bit.
+__device__ inline double knorm_from(double kx, double ky, double kz) {
+    double s = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+    return __dsqrt_rn(s);
+}
+
 __device__ inline double knorm_exact(const Mode &m, double boxsize, double *kx, double *ky,
                                      double *kz) {
     *kx = kcomp(m.nx, boxsize);
@@ -59,13 +64,28 @@ __device__ inline double knorm_exact(const Mode &m, double boxsize, double *kx, 
 }
 
 // Bin b with e[b] <= v < e[b+1], or -1 (searchsorted(..., "right") - 1 on the
-// valid range [e[0], e[last])).
+// valid range [e[0], e[last])).  The guess from an even spacing is corrected
+// against the actual edges, so any increasing edges give the exact answer.
 __device__ inline int find_bin(double v, const double *e, int nedges) {
     if (!(v >= e[0]) || !(v < e[nedges - 1])) return -1;
-    int b = 0;
-    for (int i = 1; i < nedges - 1; ++i) b += (v >= e[i]) ? 1 : 0;
+    const int nb = nedges - 1;
+    int b = (int)((v - e[0]) * nb / (e[nb] - e[0]));
+    b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+    while (b > 0 && v < e[b]) --b;
+    while (b < nb - 1 && v >= e[b + 1]) ++b;
     return b;
 }
+
+// Per-axis values shared by every mode of a block: the exact wave numbers
+// k(j) for integer j in [-n/2, n/2] and, optionally, the per-axis factor of a
+// separable window compensation.  Filled cooperatively at kernel start.
+struct AxisTable {
+    double *k;   // k[j + n/2]
+    double *cf;  // cf[j + n/2] or nullptr
+    int half;
+    __device__ double kx(int j) const { return k[j + half]; }
+    __device__ double f(int j) const { return cf[j + half]; }
+};
 
 // sinc(w / 2) = sin(w/2) / (w/2), 1 at w = 0 (np.sinc(0.5 w / pi)).
 __device__ inline double sinc_half(double w) {
@@ -86,6 +106,37 @@ __device__ inline double cwin(int p, double s) {
     if (p == 3) return 1.0 - s + 2.0 / 15 * s * s;
     if (p == 4) return 1.0 - 4.0 / 3.0 * s + 2.0 / 5.0 * s * s - 4.0 / 315.0 * s * s * s;
     return 1.0;
+}
+
+// One axis's factor of the separable compensation (comp_factor = product of
+// the three axes' factors).
+__device__ inline double comp_axis(int kind, int p, double w) {
+    if (kind == CNPC_COMP_SINC) return 1.0 / ipow(sinc_half(w), p);
+    if (p == 1) return 1.0;
+    if (kind == CNPC_COMP_SHOTNOISE) {
+        const double s = sin(0.5 * w);
+        return 1.0 / sqrt(cwin(p, s * s));
+    }
+    if (kind == CNPC_COMP_BKNOISE) {
+        const double s = sin(0.5 * w);
+        const double t = ipow(sinc_half(w), p);
+        return cwin(p, s * s) / (t * t);
+    }
+    return 1.0;
+}
+
+// Fill an AxisTable in shared memory (all threads of the block call this,
+// then __syncthreads()).
+__device__ inline void fill_axis_table(AxisTable &t, double *smem, int n, double boxsize, int kind, int p) {
+    t.half = n / 2;
+    t.k = smem;
+    t.cf = kind == CNPC_COMP_NONE ? nullptr : smem + (n + 1);
+    const double H = boxsize / n;
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+        const double k = kcomp(i - n / 2, boxsize);
+        t.k[i] = k;
+        if (t.cf) t.cf[i] = comp_axis(kind, p, k * H);
+    }
 }
 
 // Multiplicative compensation factor at circular coordinates w = k H.

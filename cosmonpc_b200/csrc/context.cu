@@ -24,21 +24,25 @@ int check_launch(cnpc_ctx *ctx, const char *what) {
     return check_cuda(ctx, cudaGetLastError(), what);
 }
 
-int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream) {
-    if (ctx->scratch_bytes >= bytes) return CNPC_OK;
-    if (ctx->scratch) {
-        // the previous scratch may still be read by work queued on `stream`
+int ensure_buffer(cnpc_ctx *ctx, void **buf, size_t *have, size_t bytes, cudaStream_t stream) {
+    if (*have >= bytes) return CNPC_OK;
+    if (*buf) {
+        // the previous buffer may still be in use by work queued on `stream`
         cudaError_t e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) return check_cuda(ctx, e, "scratch sync");
-        cudaFree(ctx->scratch);
-        ctx->scratch = nullptr;
-        ctx->scratch_bytes = 0;
+        if (e != cudaSuccess) return check_cuda(ctx, e, "workspace sync");
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
     }
     size_t want = bytes < (size_t)(1 << 20) ? (size_t)(1 << 20) : bytes;
-    cudaError_t e = cudaMalloc(&ctx->scratch, want);
-    if (e != cudaSuccess) return check_cuda(ctx, e, "scratch alloc");
-    ctx->scratch_bytes = want;
+    cudaError_t e = cudaMalloc(buf, want);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "workspace alloc");
+    *have = want;
     return CNPC_OK;
+}
+
+int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream) {
+    return ensure_buffer(ctx, &ctx->scratch, &ctx->scratch_bytes, bytes, stream);
 }
 
 static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long real_dist, cufftHandle *out) {
@@ -118,6 +122,7 @@ int cnpc_ctx_destroy(cnpc_ctx *ctx) {
     if (!ctx) return CNPC_OK;
     for (auto &kv : ctx->plans) cufftDestroy(kv.second);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->paint_ws) cudaFree(ctx->paint_ws);
     delete ctx;
     return CNPC_OK;
 }

@@ -18,6 +18,9 @@ struct cnpc_ctx {
     // scratch for per-block partial sums of the x-space reductions
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    // workspace of the tiled paint (tile counts, offsets, sorted particles)
+    void *paint_ws = nullptr;
+    size_t paint_ws_bytes = 0;
     int num_sms = 148;
 };
 
@@ -27,6 +30,7 @@ int fail(cnpc_ctx *ctx, int status, const std::string &msg);
 int check_cuda(cnpc_ctx *ctx, cudaError_t e, const char *what);
 int check_launch(cnpc_ctx *ctx, const char *what);
 int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream);
+int ensure_buffer(cnpc_ctx *ctx, void **buf, size_t *have, size_t bytes, cudaStream_t stream);
 
 }  // namespace cnpc
 

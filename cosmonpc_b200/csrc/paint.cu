@@ -1,6 +1,7 @@
 // Mass assignment (pmesh ParticleMesh.paint restated): B-spline windows of
 // order p = 1..4 on nodes at integer grid coordinates, periodic wrap; the
 // interlaced +1/2-cell mesh is painted in the same pass.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -84,6 +85,190 @@ static int launch_paint(cnpc_ctx *ctx, const double *pos, const double *w, int64
     return check_launch(ctx, "paint_kernel");
 }
 
+// ------------------------------------------------------------ tiled paint
+// Particles are counting-sorted by the 16^3-cell tile of their base node
+// floor(g); a block then deposits one tile's particles into a (16+4)^3
+// shared-memory region per mesh (every node a particle of the tile can reach,
+// for both the plain and the +1/2-shifted grid and every window order) with
+// shared atomics, and adds the region to the mesh with one global atomic per
+// node.  Node selection and weights are those of the per-particle kernel.
+constexpr int kTile = 16;
+constexpr int kRegion = kTile + 4;  // nodes [b - 1, b + 3] of a base node b in the tile
+constexpr int kRegionCells = kRegion * kRegion * kRegion;
+
+__device__ inline void grid_coords(const double *pos, int64_t i, double scale, double *g) {
+    g[0] = __dmul_rn(pos[3 * i + 0], scale);
+    g[1] = __dmul_rn(pos[3 * i + 1], scale);
+    g[2] = __dmul_rn(pos[3 * i + 2], scale);
+}
+
+__device__ inline int wrapi(int64_t v, int n) {
+    int r = (int)(v % n);
+    return r < 0 ? r + n : r;
+}
+
+__global__ void tile_count_kernel(const double *__restrict__ pos, int64_t np, int n, double scale, int tpa,
+                                  int *count, int *tile_of) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+        double g[3];
+        grid_coords(pos, i, scale, g);
+        int tid = 0;
+        for (int d = 0; d < 3; ++d) tid = tid * tpa + wrapi((int64_t)floor(g[d]), n) / kTile;
+        tile_of[i] = tid;
+        atomicAdd(&count[tid], 1);
+    }
+}
+
+// exclusive scan of count[0..nt) into offset[0..nt] and cursor (one block)
+__global__ void tile_scan_kernel(const int *count, int nt, int *offset, int *cursor) {
+    __shared__ long long part[1024];
+    const int per = (nt + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(nt, b + per);
+    long long s = 0;
+    for (int i = b; i < e; ++i) s += count[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long run = 0;
+        for (int i = 0; i < (int)blockDim.x; ++i) {
+            const long long v = part[i];
+            part[i] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    long long run = part[threadIdx.x];
+    for (int i = b; i < e; ++i) {
+        offset[i] = (int)run;
+        cursor[i] = (int)run;
+        run += count[i];
+    }
+    if (e == nt && b < e) offset[nt] = (int)run;
+    if (nt == 0 && threadIdx.x == 0) offset[0] = 0;
+}
+
+__global__ void tile_scatter_kernel(const double *__restrict__ pos, const double *__restrict__ weight,
+                                    int64_t np, double scale, const int *tile_of, int *cursor, double4 *sorted) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+        double g[3];
+        grid_coords(pos, i, scale, g);
+        const int slot = atomicAdd(&cursor[tile_of[i]], 1);
+        sorted[slot] = make_double4(g[0], g[1], g[2], weight ? weight[i] : 1.0);
+    }
+}
+
+template <typename T, int P>
+__device__ inline void deposit_region(float *reg, const int *org, double gx, double gy, double gz, double mass) {
+    int ix[P], iy[P], iz[P];
+    double wx[P], wy[P], wz[P];
+    axis_weights<P>(gx, 1 << 30, ix, wx);  // ix: unwrapped node indices (no mod with a huge n)
+    axis_weights<P>(gy, 1 << 30, iy, wy);
+    axis_weights<P>(gz, 1 << 30, iz, wz);
+    // axis_weights wrapped with n = 2^30: recover the unwrapped node
+    const int bx = (P % 2 == 0) ? (int)floor(gx) - (P / 2 - 1) : (int)floor(__dadd_rn(gx, 0.5)) - (P - 1) / 2;
+    const int by = (P % 2 == 0) ? (int)floor(gy) - (P / 2 - 1) : (int)floor(__dadd_rn(gy, 0.5)) - (P - 1) / 2;
+    const int bz = (P % 2 == 0) ? (int)floor(gz) - (P / 2 - 1) : (int)floor(__dadd_rn(gz, 0.5)) - (P - 1) / 2;
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+#pragma unroll
+        for (int b = 0; b < P; ++b) {
+            const double wab = mass * wx[a] * wy[b];
+            const int row = ((bx + a - org[0]) * kRegion + (by + b - org[1])) * kRegion;
+#pragma unroll
+            for (int c = 0; c < P; ++c) atomicAdd(reg + row + (bz + c - org[2]), (float)(T)(wab * wz[c]));
+        }
+    }
+}
+
+// Region origin (unwrapped node of region index 0) for a particle at g:
+// its base node b = floor(g) minus the offset of b inside its tile, minus 1.
+__device__ inline int region_origin(double g, int n) {
+    const int64_t b = (int64_t)floor(g);
+    const int cw = wrapi(b, n);
+    return (int)(b - (cw % kTile)) - 1;
+}
+
+template <typename T, int P>
+__global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int *__restrict__ offset, int ntiles,
+                                  int tpa, int n, T *mesh, T *mesh_shifted) {
+    extern __shared__ float reg[];  // [2][kRegionCells]
+    const int nreg = mesh_shifted ? 2 : 1;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int p0 = offset[tile], p1 = offset[tile + 1];
+        if (p0 == p1) continue;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0.f;
+        __syncthreads();
+        for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+            const double4 q = sorted[i];
+            int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};
+            deposit_region<T, P>(reg, org, q.x, q.y, q.z, q.w);
+            if (mesh_shifted)
+                deposit_region<T, P>(reg + kRegionCells, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5),
+                                     __dadd_rn(q.z, 0.5), q.w);
+        }
+        __syncthreads();
+        // wrapped origin of the region: tile origin - 1
+        const int tz = tile % tpa, ty = (tile / tpa) % tpa, tx = tile / (tpa * tpa);
+        const int ox = tx * kTile - 1, oy = ty * kTile - 1, oz = tz * kTile - 1;
+        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
+            const float v = reg[i];
+            if (v == 0.f) continue;
+            const int r = i % kRegionCells;
+            const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
+            const size_t cell = ((size_t)wrapi(ox + rx, n) * n + wrapi(oy + ry, n)) * n + wrapi(oz + rz, n);
+            atomicAdd((i < kRegionCells ? mesh : mesh_shifted) + cell, (T)v);
+        }
+    }
+}
+
+template <typename T>
+static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n, double scale,
+                        int window, T *m1, T *m2, cudaStream_t s) {
+    const int tpa = (n + kTile - 1) / kTile;
+    const int nt = tpa * tpa * tpa;
+    const size_t off_counts = 0, off_offset = off_counts + sizeof(int) * nt,
+                 off_cursor = off_offset + sizeof(int) * (nt + 1), off_tile = off_cursor + sizeof(int) * nt;
+    size_t off_sorted = off_tile + sizeof(int) * (size_t)np;
+    off_sorted = (off_sorted + 255) / 256 * 256;
+    const size_t bytes = off_sorted + sizeof(double4) * (size_t)np;
+    int st = ensure_buffer(ctx, &ctx->paint_ws, &ctx->paint_ws_bytes, bytes, s);
+    if (st) return st;
+    char *ws = static_cast<char *>(ctx->paint_ws);
+    int *count = reinterpret_cast<int *>(ws + off_counts);
+    int *offset = reinterpret_cast<int *>(ws + off_offset);
+    int *cursor = reinterpret_cast<int *>(ws + off_cursor);
+    int *tile_of = reinterpret_cast<int *>(ws + off_tile);
+    double4 *sorted = reinterpret_cast<double4 *>(ws + off_sorted);
+    st = check_cuda(ctx, cudaMemsetAsync(count, 0, sizeof(int) * nt, s), "memset tile counts");
+    if (st) return st;
+    const int threads = 256;
+    const int pblocks = (int)std::min<int64_t>((np + threads - 1) / threads, (int64_t)ctx->num_sms * 16);
+    tile_count_kernel<<<pblocks, threads, 0, s>>>(pos, np, n, scale, tpa, count, tile_of);
+    tile_scan_kernel<<<1, 1024, 0, s>>>(count, nt, offset, cursor);
+    tile_scatter_kernel<<<pblocks, threads, 0, s>>>(pos, w, np, scale, tile_of, cursor, sorted);
+    st = check_launch(ctx, "tile sort");
+    if (st) return st;
+    const size_t smem = sizeof(float) * kRegionCells * (m2 ? 2 : 1);
+    const int tblocks = (int)std::min<int64_t>(nt, (int64_t)ctx->num_sms * 8);
+    switch (window) {
+#define CNPC_TP(P_)                                                                                        \
+    case P_:                                                                                               \
+        st = check_cuda(ctx, cudaFuncSetAttribute(tile_paint_kernel<T, P_>,                                \
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
+                        "tile paint smem");                                                                \
+        if (st) return st;                                                                                 \
+        tile_paint_kernel<T, P_><<<tblocks, 256, smem, s>>>(sorted, offset, nt, tpa, n, m1, m2);           \
+        break;
+        CNPC_TP(1) CNPC_TP(2) CNPC_TP(3) CNPC_TP(4)
+#undef CNPC_TP
+        default: return fail(ctx, CNPC_EINVAL, "window must be 1..4");
+    }
+    return check_launch(ctx, "tile_paint_kernel");
+}
+
 }  // namespace cnpc
 
 using namespace cnpc;
@@ -110,9 +295,16 @@ extern "C" int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const d
     }
     if (np == 0) return CNPC_OK;
     const double scale = (double)n / boxsize;
-    if (dtype == CNPC_F32)
+    // the tiled deposit pays off once tiles hold many particles; its FP32
+    // shared-memory region would round FP64 meshes, so FP64 stays per particle
+    const bool tiled = dtype == CNPC_F32 && n >= 2 * kTile && np >= 8 * (int64_t)n * n * n / 64;
+    if (dtype == CNPC_F32) {
+        if (tiled)
+            return launch_tiled<float>(ctx, d_pos, d_weight, np, n, scale, window, (float *)d_mesh,
+                                       (float *)d_mesh_shifted, s);
         return launch_paint<float>(ctx, d_pos, d_weight, np, n, scale, window, (float *)d_mesh,
                                    (float *)d_mesh_shifted, s);
+    }
     return launch_paint<double>(ctx, d_pos, d_weight, np, n, scale, window, (double *)d_mesh,
                                 (double *)d_mesh_shifted, s);
 }

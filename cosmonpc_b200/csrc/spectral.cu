@@ -51,12 +51,16 @@ template <typename T>
 __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int n, double L,
                                       double inv_n3, double scale, int comp, int p, double k0,
                                       double band, int64_t nh) {
+    extern __shared__ double tbl[];
+    AxisTable ax;
+    fill_axis_table(ax, tbl, n, L, comp, p);
+    __syncthreads();
     const double H = L / n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
-        Mode m = mode_of(t, n);
-        double kx, ky, kz;
-        const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+        const Mode m = mode_of(t, n);
+        const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
+        const double kn = knorm_from(kx, ky, kz);
         double re = (double)spec[t].x * inv_n3, im = (double)spec[t].y * inv_n3;
         if (spec2) {
             const double ph = 0.5 * ((kx * H + ky * H) + kz * H);
@@ -66,7 +70,8 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
             re = 0.5 * re + 0.5 * (r2 * cp - i2 * sp);
             im = 0.5 * im + 0.5 * (r2 * sp + i2 * cp);
         }
-        const double f = scale * comp_factor(comp, p, kx * H, ky * H, kz * H);
+        double f = scale;
+        if (ax.cf) f *= ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz);
         re *= f;
         im *= f;
         if (t == 0) {
@@ -82,8 +87,11 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
 __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *counts, double *ksum,
                                    int64_t nh) {
     extern __shared__ double sm[];
+    AxisTable ax;
+    fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
+    double *bins = sm + (n + 1);
     const int nb = edges.n - 1;
-    for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) sm[i] = 0.0;
+    for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
@@ -93,19 +101,18 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
         int bin = -1;
         double kn = 0.0, mult = 0.0;
         if (t < nh) {
-            Mode m = mode_of(t, n);
-            double kx, ky, kz;
-            kn = knorm_exact(m, L, &kx, &ky, &kz);
+            const Mode m = mode_of(t, n);
+            kn = knorm_from(ax.kx(m.nx), ax.kx(m.ny), ax.kx(m.nz));
             bin = find_bin(kn, edges.e, edges.n);
             mult = m.mult;
         }
-        warp_bin_add(sm, bin, mult);
-        warp_bin_add(sm + nb, bin, mult * kn);
+        warp_bin_add(bins, bin, mult);
+        warp_bin_add(bins + nb, bin, mult * kn);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-        if (sm[i] != 0.0) atomicAdd(&counts[i], sm[i]);
-        if (sm[nb + i] != 0.0) atomicAdd(&ksum[i], sm[nb + i]);
+        if (bins[i] != 0.0) atomicAdd(&counts[i], bins[i]);
+        if (bins[nb + i] != 0.0) atomicAdd(&ksum[i], bins[nb + i]);
     }
 }
 
@@ -120,8 +127,11 @@ template <typename T>
 __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, EdgeSet edges,
                                PoleSet poles, double *sums, int64_t nh) {
     extern __shared__ double sm[];
+    AxisTable ax;
+    fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
+    double *bins = sm + (n + 1);
     const int nb = edges.n - 1;
-    for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x) sm[i] = 0.0;
+    for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
@@ -131,9 +141,9 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
         int bin = -1;
         double pv = 0.0, mu = 0.0;
         if (t < nh) {
-            Mode m = mode_of(t, n);
-            double kx, ky, kz;
-            const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+            const Mode m = mode_of(t, n);
+            const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
+            const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, edges.e, edges.n);
             if (bin >= 0) {
                 const cpx_t<T> va = a[t], vb = b[t];
@@ -152,12 +162,12 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                 p0 = p1;
                 p1 = pl;
             }
-            warp_bin_add(sm + q * nb, bin, pv * pl);
+            warp_bin_add(bins + q * nb, bin, pv * pl);
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x)
-        if (sm[i] != 0.0) atomicAdd(&sums[i], sm[i]);
+        if (bins[i] != 0.0) atomicAdd(&sums[i], bins[i]);
 }
 
 // ------------------------------------------------------- shot-noise sums
@@ -166,10 +176,12 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                                double sn0, int p, int use_y, cnpc_harmonic yl0, EdgeSet edges,
                                double *sums, cpx_t<T> *source, double band, int64_t nh) {
     extern __shared__ double sm[];
+    AxisTable ax;
+    fill_axis_table(ax, sm, n, L, sn0 != 0.0 ? CNPC_COMP_BKNOISE : CNPC_COMP_NONE, p);
+    double *bins = sm + 2 * (n + 1);
     const int nb = edges.n - 1;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) sm[i] = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
-    const double H = L / n;
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
@@ -178,33 +190,35 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
         int bin = -1;
         double val = 0.0;
         if (t < nh) {
-            Mode m = mode_of(t, n);
-            double kx, ky, kz;
-            const double kn = knorm_exact(m, L, &kx, &ky, &kz);
-            const cpx_t<T> va = a[t], vb = b[t];
-            double pr = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
-            const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
-            if (sn0 != 0.0) pr -= sn0 * comp_factor(CNPC_COMP_BKNOISE, p, kx * H, ky * H, kz * H);
-            if (source) {
-                const bool keep = !(band > 0.0) || kn < band;
-                source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
-            }
+            const Mode m = mode_of(t, n);
+            const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
+            const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, edges.e, edges.n);
-            if (bin >= 0) {
-                double y = 1.0;
-                if (use_y) {
-                    const bool origin = kn == 0.0;
-                    const double ik = origin ? 0.0 : 1.0 / kn;
-                    y = harmonic_eval<double>(yl0, kx * ik, ky * ik, kz * ik, origin).x;
+            const bool keep = !(band > 0.0) || kn < band;
+            if (bin >= 0 || (source && keep)) {
+                const cpx_t<T> va = a[t], vb = b[t];
+                double pr = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+                const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
+                if (sn0 != 0.0) pr -= sn0 * (ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz));
+                if (source) source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+                if (bin >= 0) {
+                    double y = 1.0;
+                    if (use_y) {
+                        const bool origin = kn == 0.0;
+                        const double ik = origin ? 0.0 : 1.0 / kn;
+                        y = harmonic_eval<double>(yl0, kx * ik, ky * ik, kz * ik, origin).x;
+                    }
+                    val = m.mult * pr * y;
                 }
-                val = m.mult * pr * y;
+            } else if (source) {
+                source[t] = mk<T>((T)0, (T)0);
             }
         }
-        warp_bin_add(sm, bin, val);
+        warp_bin_add(bins, bin, val);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x)
-        if (sm[i] != 0.0) atomicAdd(&sums[2 * i], sm[i]);
+        if (bins[i] != 0.0) atomicAdd(&sums[2 * i], bins[i]);
 }
 
 // --------------------------------------------------------- shell spectra
@@ -212,12 +226,16 @@ template <typename T>
 __global__ void shell_spectra_kernel(const cpx_t<T> *A, const cpx_t<T> *B, int n, double L,
                                      EdgeSet edges, HarmTable harm, ItemTable items,
                                      cpx_t<T> *out, int64_t nh) {
+    extern __shared__ double tbl[];
+    AxisTable ax;
+    fill_axis_table(ax, tbl, n, L, CNPC_COMP_NONE, 1);
+    __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const cpx_t<T> zero = mk<T>((T)0, (T)0);
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
-        Mode m = mode_of(t, n);
-        double kx, ky, kz;
-        const double kn = knorm_exact(m, L, &kx, &ky, &kz);
+        const Mode m = mode_of(t, n);
+        const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
+        const double kn = knorm_from(kx, ky, kz);
         const int bin = find_bin(kn, edges.e, edges.n);
         if (bin < 0) {
             for (int j = 0; j < items.n; ++j) out[(int64_t)j * nh + t] = zero;
@@ -292,12 +310,13 @@ int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d
     cudaStream_t s = (cudaStream_t)stream;
     const int threads = 256;
     const int blocks = grid_for(ctx, nh, threads);
+    const size_t tsm = 2 * sizeof(double) * (n + 1);
     if (dtype == CNPC_F32)
-        forward_finish_kernel<float><<<blocks, threads, 0, s>>>(
+        forward_finish_kernel<float><<<blocks, threads, tsm, s>>>(
             (float2 *)d_spec, (const float2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
             k0_value, band_kmax, nh);
     else
-        forward_finish_kernel<double><<<blocks, threads, 0, s>>>(
+        forward_finish_kernel<double><<<blocks, threads, tsm, s>>>(
             (double2 *)d_spec, (const double2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
             k0_value, band_kmax, nh);
     return check_launch(ctx, "forward_finish_kernel");
@@ -319,7 +338,7 @@ int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges
     if (st) return st;
     const int64_t nh = half_modes(n);
     const int threads = 256;
-    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, 2 * nb * sizeof(double), s>>>(
+    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, (n + 1 + 2 * nb) * sizeof(double), s>>>(
         n, boxsize, es, d_counts, d_ksum, nh);
     return check_launch(ctx, "kbin_counts_kernel");
 }
@@ -347,7 +366,7 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     if (st) return st;
     const int64_t nh = half_modes(n);
     const int threads = 256;
-    const size_t smem = sizeof(double) * nb * npoles;
+    const size_t smem = sizeof(double) * (n + 1 + nb * npoles);
     if (dtype == CNPC_F32)
         pk_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ps, d_sums, nh);
@@ -380,7 +399,7 @@ int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     if (st) return st;
     const int64_t nh = half_modes(n);
     const int threads = 256;
-    const size_t smem = sizeof(double) * nb;
+    const size_t smem = sizeof(double) * (2 * (n + 1) + nb);
     if (dtype == CNPC_F32)
         sn_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, volume_sq, sn0, window,
@@ -429,11 +448,11 @@ int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize, const vo
     const int threads = 256;
     cudaStream_t s = (cudaStream_t)stream;
     if (dtype == CNPC_F32)
-        shell_spectra_kernel<float><<<grid_for(ctx, nh, threads), threads, 0, s>>>(
+        shell_spectra_kernel<float><<<grid_for(ctx, nh, threads), threads, (n + 1) * sizeof(double), s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ht, itab,
             (float2 *)d_out, nh);
     else
-        shell_spectra_kernel<double><<<grid_for(ctx, nh, threads), threads, 0, s>>>(
+        shell_spectra_kernel<double><<<grid_for(ctx, nh, threads), threads, (n + 1) * sizeof(double), s>>>(
             (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ht, itab,
             (double2 *)d_out, nh);
     return check_launch(ctx, "shell_spectra_kernel");

@@ -49,19 +49,22 @@ def test_golden_case(name, precision, tmp_path):
     assert res["nmesh"] == cfg["nmesh"] and "nyquist_freq" in res
 
 
+@pytest.mark.parametrize("n,npart", [(24, 5000), (40, 20000)])
 @pytest.mark.parametrize("window", [1, 2, 3, 4])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_paint_matches_oracle(window, precision):
+def test_paint_matches_oracle(window, precision, n, npart):
+    """Per-particle paint (small n) and the tiled shared-memory paint (FP32,
+    n >= 32 with enough particles; n = 40 also has a partial edge tile)."""
     import torch
     from cosmonpc_b200 import _lib, engine
     from oracle.pmesh_lite import paint_mass
 
-    n, L = 24, 300.0
+    L = 300.0
     rng = np.random.default_rng(window)
-    pos = rng.random((5000, 3)) * L
+    pos = rng.random((npart, 3)) * L
     pos[:7] = [[0, 0, 0], [L * (1 - 1e-16), 1, 2], [L / n * 3, L / n * 5.5, 0.5 * L], [1e-9, 299.9, 150],
                [L / 2, L / 2, L / 2], [L / n * 7.25, 0.0, L / n * 11.75], [L - 1e-7, L - 1e-7, L - 1e-7]]
-    w = 0.5 + rng.random(5000)
+    w = 0.5 + rng.random(npart)
     ctx = _lib.Context.get()
     code, rdt, _ = engine.PRECISION[precision]
     mesh = torch.empty((2, n, n, n), dtype=rdt, device="cuda")
