@@ -116,7 +116,9 @@ __global__ void tile_count_kernel(const double *__restrict__ pos, int64_t np, in
         int tid = 0;
         for (int d = 0; d < 3; ++d) tid = tid * tpa + wrapi((int64_t)floor(g[d]), n) / kTile;
         tile_of[i] = tid;
-        atomicAdd(&count[tid], 1);
+        // clustered catalogs put many lanes of a warp in one tile: one atomic per tile
+        const unsigned same = __match_any_sync(__activemask(), tid);
+        if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&count[tid], __popc(same));
     }
 }
 
@@ -154,7 +156,15 @@ __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
         double g[3];
         grid_coords(pos, i, scale, g);
-        const int slot = atomicAdd(&cursor[tile_of[i]], 1);
+        const int tid = tile_of[i];
+        // reserve the slots of every lane in the same tile with one atomic
+        const unsigned same = __match_any_sync(__activemask(), tid);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(same) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&cursor[tid], __popc(same));
+        base = __shfl_sync(same, base, leader);
+        const int slot = base + __popc(same & ((1u << lane) - 1));
         sorted[slot] = make_double4(g[0], g[1], g[2], weight ? weight[i] : 1.0);
     }
 }
