@@ -386,14 +386,19 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
     fold();  // also defines the partial of a warp that had no chunk
 }
 
+// One warp per output: lane l sums partials l, l+32, ... and a fixed shuffle
+// tree combines the lanes, so the result is bitwise reproducible.
 __global__ void gram_window_reduce_kernel(const double *partial, int nparts, int wr, int wc, int na, int nb,
                                           double *out) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (o >= na * nb) return;
     const int i = o / nb, j = o % nb;
     double s = 0.0;
-    for (int p = 0; p < nparts; ++p) s += partial[(int64_t)p * wr * wc + i * wc + j];
-    out[o] = s;
+    for (int p = lane; p < nparts; p += 32) s += partial[(int64_t)p * wr * wc + i * wc + j];
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[o] = s;
 }
 
 // Staged rows and window of an FP32 Gram launch (na <= 48, nb <= 24).
@@ -488,7 +493,7 @@ static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const flo
     st = check_cuda(ctx, ff_launch(pl, nblocks, g, fields, part, s), "gram_ffma_kernel");
     if (st) return st;
     const int nout = na * nb;
-    gram_window_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
+    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
     return check_launch(ctx, "gram_window_reduce_kernel");
 }
 
@@ -497,7 +502,8 @@ static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const flo
 template <int TM, int TN, int NW>
 __global__ void gram_reduce_kernel(const double *partial, int nblocks, int ngroups, int ntiles, int ct,
                                    int na, int nb, double *out) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (o >= na * nb) return;
     const int i = o / nb, j = o % nb;
     const int tile = (i / TM) * ct + (j / TN);
@@ -505,10 +511,17 @@ __global__ void gram_reduce_kernel(const double *partial, int nblocks, int ngrou
     const int group = tile / NW;
     const int nt = min(NW, ntiles - group * NW);
     const int local = tile - group * NW;
+    const int per_block = (NW - 1 - local) / nt + 1;  // warps of a block assigned to this tile
+    const int nblk = (nblocks - group + ngroups - 1) / ngroups;
     double s = 0.0;
-    for (int b = group; b < nblocks; b += ngroups)
-        for (int w = local; w < NW; w += nt) s += partial[((int64_t)b * NW + w) * (TM * TN) + e];
-    out[o] = s;
+    for (int q = lane; q < nblk * per_block; q += 32) {
+        const int b = group + (q / per_block) * ngroups;
+        const int w = local + (q % per_block) * nt;
+        s += partial[((int64_t)b * NW + w) * (TM * TN) + e];
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[o] = s;
 }
 
 template <typename T>
@@ -575,7 +588,7 @@ static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, i
     st = check_launch(ctx, "gram_kernel");
     if (st) return st;
     const int nout = na * nb;
-    gram_reduce_kernel<TM, TN, NW><<<(nout + 127) / 128, 128, 0, s>>>(
+    gram_reduce_kernel<TM, TN, NW><<<(nout + 7) / 8, 256, 0, s>>>(
         (const double *)ctx->scratch, nblocks, P.ngroups, P.ntiles, P.ct, na, nb, out);
     return check_launch(ctx, "gram_reduce_kernel");
 }
@@ -691,8 +704,8 @@ static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, 
     st = noalloc_cuda(ff_launch(pl, nblocks, g, fields, scratch, s));
     if (st) return st;
     const int nout = na * nb;
-    gram_window_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na,
-                                                                 nb, out);
+    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na, nb,
+                                                             out);
     return noalloc_cuda(cudaGetLastError());
 }
 
@@ -762,8 +775,8 @@ static int noalloc_gram_f64(int64_t ncell, const double *g, const double *fields
     st = noalloc_cuda(cudaGetLastError());
     if (st) return st;
     const int nout = na * nb;
-    gram_reduce_kernel<TM, TN, NW><<<(nout + 127) / 128, 128, 0, s>>>(scratch, nblocks, P.ngroups, P.ntiles, P.ct,
-                                                                      na, nb, out);
+    gram_reduce_kernel<TM, TN, NW><<<(nout + 7) / 8, 256, 0, s>>>(scratch, nblocks, P.ngroups, P.ntiles, P.ct, na,
+                                                                  nb, out);
     return noalloc_cuda(cudaGetLastError());
 }
 

@@ -169,25 +169,34 @@ __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double
     }
 }
 
-template <typename T, int P>
-__device__ inline void deposit_region(float *reg, const int *org, double gx, double gy, double gz, double mass) {
-    int ix[P], iy[P], iz[P];
-    double wx[P], wy[P], wz[P];
-    axis_weights<P>(gx, 1 << 30, ix, wx);  // ix: unwrapped node indices (no mod with a huge n)
-    axis_weights<P>(gy, 1 << 30, iy, wy);
-    axis_weights<P>(gz, 1 << 30, iz, wz);
-    // axis_weights wrapped with n = 2^30: recover the unwrapped node
-    const int bx = (P % 2 == 0) ? (int)floor(gx) - (P / 2 - 1) : (int)floor(__dadd_rn(gx, 0.5)) - (P - 1) / 2;
-    const int by = (P % 2 == 0) ? (int)floor(gy) - (P / 2 - 1) : (int)floor(__dadd_rn(gy, 0.5)) - (P - 1) / 2;
-    const int bz = (P % 2 == 0) ? (int)floor(gz) - (P / 2 - 1) : (int)floor(__dadd_rn(gz, 0.5)) - (P - 1) / 2;
+__device__ inline void red_shared_add(float *addr, float v) {
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "f"(v) : "memory");
+}
+
+// 1-D window of one axis: first (unwrapped) node and the P weights, computed
+// exactly as axis_weights does.
+template <int P> __device__ inline int axis_first(double g, float *w) {
+    const int base = (P % 2 == 0) ? (int)floor(g) - (P / 2 - 1) : (int)floor(__dadd_rn(g, 0.5)) - (P - 1) / 2;
+#pragma unroll
+    for (int o = 0; o < P; ++o) w[o] = (float)bspline<P>(__dsub_rn((double)(base + o), g));
+    return base;
+}
+
+// Deposit into a shared region whose index 0 is the unwrapped node org.
+template <int P>
+__device__ inline void deposit_region(float *reg, const int *org, double gx, double gy, double gz, float mass) {
+    float wx[P], wy[P], wz[P];
+    const int bx = axis_first<P>(gx, wx) - org[0];
+    const int by = axis_first<P>(gy, wy) - org[1];
+    const int bz = axis_first<P>(gz, wz) - org[2];
+    float *base = reg + (bx * kRegion + by) * kRegion + bz;
 #pragma unroll
     for (int a = 0; a < P; ++a) {
 #pragma unroll
         for (int b = 0; b < P; ++b) {
-            const double wab = mass * wx[a] * wy[b];
-            const int row = ((bx + a - org[0]) * kRegion + (by + b - org[1])) * kRegion;
+            const float wab = mass * wx[a] * wy[b];
 #pragma unroll
-            for (int c = 0; c < P; ++c) atomicAdd(reg + row + (bz + c - org[2]), (float)(T)(wab * wz[c]));
+            for (int c = 0; c < P; ++c) red_shared_add(base + (a * kRegion + b) * kRegion + c, wab * wz[c]);
         }
     }
 }
@@ -214,10 +223,10 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
             const double4 q = sorted[i];
             int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};
-            deposit_region<T, P>(reg, org, q.x, q.y, q.z, q.w);
+            deposit_region<P>(reg, org, q.x, q.y, q.z, (float)q.w);
             if (mesh_shifted)
-                deposit_region<T, P>(reg + kRegionCells, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5),
-                                     __dadd_rn(q.z, 0.5), q.w);
+                deposit_region<P>(reg + kRegionCells, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5),
+                                  __dadd_rn(q.z, 0.5), (float)q.w);
         }
         __syncthreads();
         // wrapped origin of the region: tile origin - 1
