@@ -10,7 +10,8 @@ and ``h5py``; none is installed here, so this module places stand-ins in
   caller's frame (the form ``sympy.lambdify(..., "numexpr")`` emits).
 * ``pmesh.pm.ParticleMesh``: ``oracle.pmesh_lite`` (restated pmesh behaviour).
 * ``astropy.cosmology.FlatLambdaCDM``: comoving distance by ``scipy.integrate.quad``.
-* ``fitsio`` / ``h5py``: placeholders (box ``.npy`` workloads never reach them).
+* ``fitsio.FITS``: this repository's FITS binary-table reader (``cosmonpc_b200.fits``).
+* ``h5py``: a placeholder (no workload here reads HDF5).
 """
 from __future__ import annotations
 
@@ -119,6 +120,10 @@ def _install_pmesh():
 def _install_astropy():
     from scipy.integrate import quad
 
+    # the real astropy imports numpy.lib.recfunctions, which the reference's
+    # add_completeness_weight reaches as np.lib.recfunctions
+    import numpy.lib.recfunctions  # noqa: F401
+
     astropy = types.ModuleType("astropy")
     cosmo = types.ModuleType("astropy.cosmology")
     units = types.ModuleType("astropy.units")
@@ -168,6 +173,49 @@ def _install_astropy():
     sys.modules["astropy.units"] = units
 
 
+def _install_fitsio():
+    """``fitsio.FITS`` over this repository's FITS binary-table reader."""
+    sys.path.insert(0, _REPO)
+    from cosmonpc_b200 import fits as _fits
+
+    fitsio = types.ModuleType("fitsio")
+
+    class _HDU:
+        def __init__(self, table):
+            self._t = table
+
+        def get_nrows(self):
+            return self._t.nrows
+
+        def get_colnames(self):
+            return self._t.colnames()
+
+        def read(self, rows=None, columns=None):
+            cols = self._t.colnames() if columns is None else list(columns)
+            sel = None if rows is None else np.asarray(list(rows), dtype=np.int64)
+            return self._t.read_columns(cols, rows=sel)
+
+    class FITS:
+        def __init__(self, path, mode="r"):
+            self._path = path
+            self._n = len(_fits.hdu_list(path))
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def __len__(self):
+            return self._n
+
+        def __getitem__(self, i):
+            return _HDU(_fits.open_table(self._path))
+
+    fitsio.FITS = FITS
+    sys.modules["fitsio"] = fitsio
+
+
 def _install_placeholders():
     for name in ("fitsio", "h5py"):
         sys.modules.setdefault(name, types.ModuleType(name))
@@ -179,6 +227,7 @@ def import_reference():
     _install_numexpr()
     _install_pmesh()
     _install_astropy()
+    _install_fitsio()
     _install_placeholders()
     if REFERENCE_SRC not in sys.path:
         sys.path.insert(0, REFERENCE_SRC)
