@@ -123,6 +123,7 @@ int cnpc_ctx_destroy(cnpc_ctx *ctx) {
     for (auto &kv : ctx->plans) cufftDestroy(kv.second);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->paint_ws) cudaFree(ctx->paint_ws);
+    if (ctx->aux) cudaFree(ctx->aux);
     delete ctx;
     return CNPC_OK;
 }

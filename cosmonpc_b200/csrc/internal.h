@@ -21,6 +21,9 @@ struct cnpc_ctx {
     // workspace of the tiled paint (tile counts, offsets, sorted particles)
     void *paint_ws = nullptr;
     size_t paint_ws_bytes = 0;
+    // workspace of the catalog and survey reductions (block counts, partials)
+    void *aux = nullptr;
+    size_t aux_bytes = 0;
     int num_sms = 148;
 };
 

@@ -51,17 +51,36 @@ __device__ inline void deposit(T *mesh, int n, double gx, double gy, double gz, 
     }
 }
 
+// Painting frame: grid coordinate g = (x - origin) * scale with each
+// operation rounded separately (no FMA contraction), so grid coordinates match
+// Position - boxcenter (mesh_generator.py:182-183) followed by the restated
+// pmesh affine transform bit for bit; x - 0 is exact, so a zero origin is the
+// plain transform.  Masses are weight * mass_scale.
+struct Frame {
+    double ox, oy, oz;
+    double scale;
+    double mass_scale;
+};
+
+__device__ inline void grid_coords(const double *pos, int64_t i, const Frame &f, double *g) {
+    g[0] = __dmul_rn(__dsub_rn(pos[3 * i + 0], f.ox), f.scale);
+    g[1] = __dmul_rn(__dsub_rn(pos[3 * i + 1], f.oy), f.scale);
+    g[2] = __dmul_rn(__dsub_rn(pos[3 * i + 2], f.oz), f.scale);
+}
+
+__device__ inline double mass_of(const double *weight, int64_t i, const Frame &f) {
+    return weight ? __dmul_rn(weight[i], f.mass_scale) : f.mass_scale;
+}
+
 template <typename T, int P>
 __global__ void paint_kernel(const double *__restrict__ pos, const double *__restrict__ weight,
-                             int64_t np, int n, double scale, T *mesh, T *mesh_shifted) {
+                             int64_t np, int n, Frame f, T *mesh, T *mesh_shifted) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
-        // separately rounded products and sums (no FMA contraction), so grid
-        // coordinates match the restated pmesh affine transform bit for bit
-        const double gx = __dmul_rn(pos[3 * i + 0], scale);
-        const double gy = __dmul_rn(pos[3 * i + 1], scale);
-        const double gz = __dmul_rn(pos[3 * i + 2], scale);
-        const double mass = weight ? weight[i] : 1.0;
+        double g[3];
+        grid_coords(pos, i, f, g);
+        const double gx = g[0], gy = g[1], gz = g[2];
+        const double mass = mass_of(weight, i, f);
         deposit<T, P>(mesh, n, gx, gy, gz, mass);
         if (mesh_shifted)
             deposit<T, P>(mesh_shifted, n, __dadd_rn(gx, 0.5), __dadd_rn(gy, 0.5), __dadd_rn(gz, 0.5), mass);
@@ -70,7 +89,7 @@ __global__ void paint_kernel(const double *__restrict__ pos, const double *__res
 
 template <typename T>
 static int launch_paint(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n,
-                        double scale, int window, T *m1, T *m2, cudaStream_t s) {
+                        const Frame &scale, int window, T *m1, T *m2, cudaStream_t s) {
     const int threads = 256;
     int64_t want = (np + threads - 1) / threads;
     int64_t cap = (int64_t)ctx->num_sms * 16;
@@ -96,18 +115,12 @@ constexpr int kTile = 16;
 constexpr int kRegion = kTile + 4;  // nodes [b - 1, b + 3] of a base node b in the tile
 constexpr int kRegionCells = kRegion * kRegion * kRegion;
 
-__device__ inline void grid_coords(const double *pos, int64_t i, double scale, double *g) {
-    g[0] = __dmul_rn(pos[3 * i + 0], scale);
-    g[1] = __dmul_rn(pos[3 * i + 1], scale);
-    g[2] = __dmul_rn(pos[3 * i + 2], scale);
-}
-
 __device__ inline int wrapi(int64_t v, int n) {
     int r = (int)(v % n);
     return r < 0 ? r + n : r;
 }
 
-__global__ void tile_count_kernel(const double *__restrict__ pos, int64_t np, int n, double scale, int tpa,
+__global__ void tile_count_kernel(const double *__restrict__ pos, int64_t np, int n, Frame scale, int tpa,
                                   int *count, int *tile_of) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
@@ -151,7 +164,7 @@ __global__ void tile_scan_kernel(const int *count, int nt, int *offset, int *cur
 }
 
 __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double *__restrict__ weight,
-                                    int64_t np, double scale, const int *tile_of, int *cursor, double4 *sorted) {
+                                    int64_t np, Frame scale, const int *tile_of, int *cursor, double4 *sorted) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
         double g[3];
@@ -165,7 +178,7 @@ __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double
         if (lane == leader) base = atomicAdd(&cursor[tid], __popc(same));
         base = __shfl_sync(same, base, leader);
         const int slot = base + __popc(same & ((1u << lane) - 1));
-        sorted[slot] = make_double4(g[0], g[1], g[2], weight ? weight[i] : 1.0);
+        sorted[slot] = make_double4(g[0], g[1], g[2], mass_of(weight, i, scale));
     }
 }
 
@@ -244,7 +257,7 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
 }
 
 template <typename T>
-static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n, double scale,
+static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n, const Frame &scale,
                         int window, T *m1, T *m2, cudaStream_t s) {
     const int tpa = (n + kTile - 1) / kTile;
     const int nt = tpa * tpa * tpa;
@@ -292,9 +305,10 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
 
 using namespace cnpc;
 
-extern "C" int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_weight,
-                          int64_t np, int n, double boxsize, int window, void *d_mesh,
-                          void *d_mesh_shifted, cnpc_stream_t stream) {
+extern "C" int cnpc_paint_ex(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_weight,
+                             int64_t np, int n, double boxsize, int window, const double *h_origin,
+                             double mass_scale, int accumulate, void *d_mesh, void *d_mesh_shifted,
+                             cnpc_stream_t stream) {
     CNPC_REQUIRE(ctx, ctx != nullptr, "null context");
     CNPC_REQUIRE(ctx, n >= 2 && n <= 2048, "n out of range");
     CNPC_REQUIRE(ctx, boxsize > 0.0, "boxsize must be positive");
@@ -306,24 +320,39 @@ extern "C" int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const d
     cudaStream_t s = (cudaStream_t)stream;
     const size_t cells = (size_t)n * n * n;
     const size_t esz = dtype == CNPC_F32 ? sizeof(float) : sizeof(double);
-    int st = check_cuda(ctx, cudaMemsetAsync(d_mesh, 0, cells * esz, s), "memset mesh");
-    if (st) return st;
-    if (d_mesh_shifted) {
-        st = check_cuda(ctx, cudaMemsetAsync(d_mesh_shifted, 0, cells * esz, s), "memset mesh");
+    int st;
+    if (!accumulate) {
+        st = check_cuda(ctx, cudaMemsetAsync(d_mesh, 0, cells * esz, s), "memset mesh");
         if (st) return st;
+        if (d_mesh_shifted) {
+            st = check_cuda(ctx, cudaMemsetAsync(d_mesh_shifted, 0, cells * esz, s), "memset mesh");
+            if (st) return st;
+        }
     }
     if (np == 0) return CNPC_OK;
-    const double scale = (double)n / boxsize;
+    Frame f;
+    f.ox = h_origin ? h_origin[0] : 0.0;
+    f.oy = h_origin ? h_origin[1] : 0.0;
+    f.oz = h_origin ? h_origin[2] : 0.0;
+    f.scale = (double)n / boxsize;
+    f.mass_scale = mass_scale;
     // the tiled deposit pays off once tiles hold many particles; its FP32
     // shared-memory region would round FP64 meshes, so FP64 stays per particle
     const bool tiled = dtype == CNPC_F32 && n >= 2 * kTile && np >= 8 * (int64_t)n * n * n / 64;
     if (dtype == CNPC_F32) {
         if (tiled)
-            return launch_tiled<float>(ctx, d_pos, d_weight, np, n, scale, window, (float *)d_mesh,
+            return launch_tiled<float>(ctx, d_pos, d_weight, np, n, f, window, (float *)d_mesh,
                                        (float *)d_mesh_shifted, s);
-        return launch_paint<float>(ctx, d_pos, d_weight, np, n, scale, window, (float *)d_mesh,
+        return launch_paint<float>(ctx, d_pos, d_weight, np, n, f, window, (float *)d_mesh,
                                    (float *)d_mesh_shifted, s);
     }
-    return launch_paint<double>(ctx, d_pos, d_weight, np, n, scale, window, (double *)d_mesh,
+    return launch_paint<double>(ctx, d_pos, d_weight, np, n, f, window, (double *)d_mesh,
                                 (double *)d_mesh_shifted, s);
+}
+
+extern "C" int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_weight,
+                          int64_t np, int n, double boxsize, int window, void *d_mesh,
+                          void *d_mesh_shifted, cnpc_stream_t stream) {
+    return cnpc_paint_ex(ctx, dtype, d_pos, d_weight, np, n, boxsize, window, nullptr, 1.0, 0, d_mesh,
+                         d_mesh_shifted, stream);
 }

@@ -102,6 +102,18 @@ int cnpc_paint(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_we
                int64_t np, int n, double boxsize, int window,
                void *d_mesh, void *d_mesh_shifted, cnpc_stream_t stream);
 
+/* cnpc_paint in a shifted frame, with scaled masses, optionally accumulating:
+ * grid coordinates (x - h_origin) * n / L (h_origin: 3 host doubles or NULL),
+ * masses weight * mass_scale, and the meshes are zeroed first unless
+ * `accumulate`.  Replaces pm_painter's Position - boxcenter
+ * (mesh_generator.py:182-183) and the x-space scalings of the painted survey
+ * fields (mesh_generator.py:449-454, :666-668, :1117-1120), which are linear
+ * in the masses. */
+int cnpc_paint_ex(cnpc_ctx *ctx, int dtype, const double *d_pos, const double *d_weight,
+                  int64_t np, int n, double boxsize, int window, const double *h_origin,
+                  double mass_scale, int accumulate, void *d_mesh, void *d_mesh_shifted,
+                  cnpc_stream_t stream);
+
 /* --------------------------------------------------------------------- FFT
  * Replace RealField.r2c / ComplexField.c2r of pmesh.  Unnormalised cuFFT
  * transforms of `batch` fields; the 1/n^3 of pmesh's r2c is folded into
@@ -120,7 +132,8 @@ int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec,
  *   c *= scale, then the compensation `comp` of window order `window`
  *   (clustering_estimator.py:599-603, :815-816), and the k = 0 mode is set to
  *   k0_value (the reference clears it for pk, ce:634-636, and it equals
- *   (sum w / n^3)/dV - NZ for the bk overdensity, ce:808-816).
+ *   (sum w / n^3)/dV - NZ for the bk overdensity, ce:808-816); k0_value NaN
+ *   keeps the computed k = 0 mode (survey fields, ce:590-603, ce:1625-1627).
  *   band_kmax > 0 zeroes modes with |k| >= band_kmax. */
 int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
                         const void *d_spec2, double scale, int comp, int window,
@@ -170,6 +183,129 @@ int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize,
                        const cnpc_harmonic *h_harmonics, int nharmonics,
                        const cnpc_shell_item *h_items, int nitems, void *d_out,
                        cnpc_stream_t stream);
+
+/* ------------------------------------------------------------ survey path
+ * Survey catalogs arrive as the raw big-endian rows of a FITS binary table
+ * (catalog_processor.py:128-183 reads them with fitsio); one call decodes the
+ * columns the reference uses on the device. */
+enum cnpc_coltype {
+    CNPC_CT_ABSENT = 0, CNPC_CT_F64 = 1, CNPC_CT_F32 = 2, CNPC_CT_I16 = 3,
+    CNPC_CT_I32 = 4, CNPC_CT_I64 = 5, CNPC_CT_U8 = 6, CNPC_CT_BOOL = 7
+};
+/* one scalar FITS column: value = zero + scale * raw (TZEROn / TSCALn) */
+typedef struct cnpc_column {
+    int type;    /* cnpc_coltype                     */
+    int offset;  /* byte offset of the column in a row */
+    double scale;
+    double zero;
+} cnpc_column;
+enum cnpc_colid {
+    CNPC_COL_RA = 0, CNPC_COL_DEC, CNPC_COL_Z, CNPC_COL_WEIGHT, CNPC_COL_SYSTOT,
+    CNPC_COL_NOZ, CNPC_COL_CP, CNPC_COL_FKP, CNPC_COL_NZ, CNPC_NCOLS
+};
+/* completeness weight (add_completeness_weight, catalog_processor.py:186-290):
+ * COLUMN: the WEIGHT slot (an existing WEIGHT column or the alias column);
+ * ONE: 1; BOSS: SYSTOT (NOZ + CP - 1); EBOSS: SYSTOT NOZ CP */
+enum cnpc_weight_rule { CNPC_W_COLUMN = 0, CNPC_W_ONE = 1, CNPC_W_BOSS = 2, CNPC_W_EBOSS = 3 };
+typedef struct cnpc_catalog_spec {
+    int64_t row_bytes;
+    cnpc_column col[CNPC_NCOLS]; /* NZ slot: the NZ or NX column, or absent (NZ = 1) */
+    int weight_rule;
+    int has_zrange;              /* keep rows with z_min < Z < z_max (cp:506-508) */
+    double z_min, z_max;
+    double h, omega_m;           /* flat LCDM, no radiation (cp:617-632)          */
+} cnpc_catalog_spec;
+
+/* Decode, z-cut and convert a survey catalog: catalog_reader's survey branch
+ * (catalog_processor.py:493-586) with ra_dec_z_to_xyz (cp:589-645).
+ * Kept rows are written in file order to d_pos (n, 3), d_weight, d_wfkp, d_nz;
+ * the buffers must hold nrows entries.  Positions are D_C(z) h (cos d cos a,
+ * cos d sin a, sin d) in Mpc/h with D_C from 16-point Gauss-Legendre panels.
+ * The call waits for the stream to return the kept count in *h_kept. */
+int cnpc_catalog_decode(cnpc_ctx *ctx, const void *d_rows, int64_t nrows,
+                        const cnpc_catalog_spec *h_spec, double *d_pos, double *d_weight,
+                        double *d_wfkp, double *d_nz, int64_t *h_kept, cnpc_stream_t stream);
+
+/* Per-particle sums of compute_particle_sums_pk / _bk (mesh_generator.py:1131-1268)
+ * and the position range of catalog_reader's boxcenter (cp:564-574).  d_out:
+ *   [0] sum w wfkp   [1] sum w   [2] sum w nz wfkp^2   [3] sum (w wfkp)^2
+ *   [4] sum nz^2 w^2 wfkp^3,
+ *   [5 + 2q], [6 + 2q]: re, im of sum (w wfkp)^3 conj(Y_q(x/|x|)) for the
+ *   nharm harmonics h_ylm (S_LM), then min x, y, z and max x, y, z. */
+#define CNPC_PSUM_COUNT 5
+int cnpc_particle_sums(cnpc_ctx *ctx, int64_t np, const double *d_pos, const double *d_weight,
+                       const double *d_wfkp, const double *d_nz, const cnpc_harmonic *h_ylm,
+                       int nharm, double *d_out, cnpc_stream_t stream);
+
+/* d_out[i] = (w[i] wfkp[i])^power, power 1 (paint weights, mg:422-445) or 2
+ * (the N-field weights of get_N_field, mg:1082-1083). */
+int cnpc_catalog_weights(cnpc_ctx *ctx, int64_t np, const double *d_weight, const double *d_wfkp,
+                         int power, double *d_out, cnpc_stream_t stream);
+
+/* The reference holds an interlaced painted field as the complex-to-complex
+ * c2r of c = s1/2 + s2/2 e^{i k.H/2} (mesh_generator.py:207-219); on the
+ * Nyquist planes c is not Hermitian, so the field has an imaginary part.
+ * This writes, from the raw R2C spectra s1, s2 (s1 / n^3 is pmesh's r2c),
+ *   d_herm = scale * (c(k) + conj c(-k)) / 2        (c2r -> Re field)
+ *   d_anti = scale * (-i) (c(k) - conj c(-k)) / 2   (c2r -> Im field)
+ * with the reference's index convention (index i >= n/2 is k = (i - n) 2pi/L
+ * on every axis).  d_spec2 NULL: d_herm = scale * s1 / n^3, d_anti unused.
+ * accumulate adds to d_herm / d_anti; in place (d_herm == d_spec,
+ * d_anti == d_spec2) is allowed without accumulate. */
+int cnpc_interlace_split(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec,
+                         const void *d_spec2, double scale, int accumulate, void *d_herm,
+                         void *d_anti, cnpc_stream_t stream);
+
+/* x-space harmonic weighting of a complex field F = re + i im (im may be NULL):
+ *   out_re + i out_im = scale * F(x) * Y(xhat)   (conj: conj(Y))
+ * at the cell positions of get_xgrid (math_evaluator.py:25-32): the node
+ * coordinate i L / n wrapped into [-L/2, L/2), plus L / (2 n) + boxcenter.
+ * Replaces rfield * Y_lm(xgrid) in ce:3118-3124, ce:1700-1703, ce:2262, ce:2346,
+ * ce:2496.  d_out_im may be NULL when the product is known to be real. */
+int cnpc_xspace_harmonic(cnpc_ctx *ctx, int dtype, int n, double boxsize, const double *h_boxcenter,
+                         const void *d_re, const void *d_im, const cnpc_harmonic *h_y, int conj,
+                         double scale, void *d_out_re, void *d_out_im, cnpc_stream_t stream);
+
+/* A spectral operand of the survey sums: Hermitian half spectrum p (q NULL),
+ * or X = P + i Q for the non-Hermitian FFT of a complex field whose real and
+ * imaginary parts have half spectra P and Q (X(-k) = conj P + i conj Q).
+ * The operand's value is scale * comp(k) * (p or X). */
+typedef struct cnpc_operand {
+    const void *p;
+    const void *q;
+    double scale;
+    int comp;
+} cnpc_operand;
+
+/* Complex shell sums over full k-space, d_sums[2 b + {0, 1}]:
+ *   sum_{k in bin b} weight * (U(k) conj V(k) - sbar W_bknoise(k)) * Z(khat)
+ * Z = Y of h_z (conj_z: conj Y; NULL: 1; Y(-khat) = (-1)^l Y(khat)).
+ * Replaces radial_binning of the survey terms: a conj G_l (ce:456-468 with
+ * get_G_ell ce:3104-3134), the S1 field (ce:2254-2296) and Q_L (ce:2338-2385). */
+int cnpc_survey_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window,
+                     const cnpc_operand *u, const cnpc_operand *v, double sbar_re, double sbar_im,
+                     const cnpc_harmonic *h_z, int conj_z, double weight, const double *h_edges,
+                     int nedges, double *d_sums, cnpc_stream_t stream);
+
+/* The S3-FFT source spectrum src = U conj V - sbar W_bknoise (ce:2484-2511)
+ * split like cnpc_interlace_split into its Hermitian part (d_herm, c2r ->
+ * Re src) and -i times its anti-Hermitian part (d_anti, c2r -> Im src),
+ * zero at |k| >= band_kmax when band_kmax > 0. */
+int cnpc_survey_source(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window,
+                       const cnpc_operand *u, const cnpc_operand *v, double sbar_re, double sbar_im,
+                       double band_kmax, void *d_herm, void *d_anti, cnpc_stream_t stream);
+
+/* d_out[0] + i d_out[1] = sum_x prod_{j < nf} (re_j(x) + i im_j(x)), nf 1..3,
+ * h_re / h_im: host arrays of nf device pointers (h_im or its entries may be
+ * NULL).  Replaces the normalisation sums np.sum(D * R) and friends
+ * (mesh_generator.py:503-519, :829-830, :903-905, :961-990). */
+int cnpc_field_product_sum(cnpc_ctx *ctx, int dtype, int64_t ncell, int nf, const void *const *h_re,
+                           const void *const *h_im, double *d_out, cnpc_stream_t stream);
+
+/* d_out = a x + b y over ncell real cells (d_y may be NULL); the x-space
+ * combinations rfield_data - alpha rfield_randoms (mg:449-454, :666-668). */
+int cnpc_field_axpby(cnpc_ctx *ctx, int dtype, int64_t ncell, double a, const void *d_x, double b,
+                     const void *d_y, void *d_out, cnpc_stream_t stream);
 
 /* ------------------------------------------------------ x-space reductions
  * Replaces np.sum(G * F1 * F2) of clustering_estimator.py:972, :1051, :1257,

@@ -95,6 +95,96 @@ CASES = [
 ]
 
 
+# Survey-like cases (FITS catalogs, RA/DEC/Z columns).  Catalog spec per tracer:
+# (seed, n_data, n_randoms, boss_weights); the survey occupies RA 150-180 deg,
+# DEC 10-35 deg, 0.4 < z < 0.6, inside a 1000 Mpc/h box.
+_SURVEY_BASE = dict(
+    geometry="survey-like",
+    column_names=["RA", "DEC", "Z", "WEIGHT_FKP", "WEIGHT_SYSTOT", "WEIGHT_NOZ", "WEIGHT_CP", "NZ"],
+    cosmology={"h": 0.6766, "Omega0": 0.31},
+    compensation=True,
+    nmesh=[32] * 3,
+    boxsize=[1000.0] * 3,
+    z_range=[0.42, 0.58],
+    comp_weight_plan={"scheme": "boss", "name_alias": None},
+    alpha_scheme="pypower",
+)
+_SA = {"a": (41, 20000, 100000, True)}
+_SAB = {"a": (41, 20000, 100000, True), "b": (42, 15000, 80000, True)}
+_SABC = {"a": (41, 20000, 100000, True), "b": (42, 15000, 80000, True), "c": (43, 12000, 70000, True)}
+
+SURVEY_CASES = [
+    ("sv_pk_auto_tsc_particle", dict(statistic="pk", correlation_mode="auto", sampler="tsc",
+                                     interlaced=True, k_min=0.0, k_max=0.09, k_bins=9, poles=[0, 2, 4],
+                                     normalization_scheme="particle"), _SA),
+    ("sv_pk_cross_cic_mixed", dict(statistic="pk", correlation_mode="cross", sampler="cic",
+                                   interlaced=False, k_min=0.005, k_max=0.085, k_bins=8, poles=[0, 1, 2],
+                                   normalization_scheme="mixed-mesh", alpha_scheme="nbodykit",
+                                   z_range=None, comp_weight_plan={"scheme": None, "name_alias": None}),
+     _SAB),
+    ("sv_pk_auto_pcs_compare", dict(statistic="pk", correlation_mode="auto", sampler="pcs",
+                                    interlaced=True, k_min=0.0, k_max=0.09, k_bins=6, poles=[0, 2, 4, 6, 8],
+                                    normalization_scheme="mixed-mesh", high_order_mode="compare",
+                                    comp_weight_plan={"scheme": "eboss", "name_alias": None}), _SA),
+    ("sv_pk_auto_ngp_fast", dict(statistic="pk", correlation_mode="auto", sampler="ngp",
+                                 interlaced=True, k_min=0.0, k_max=0.09, k_bins=6, poles=[0, 2, 4],
+                                 normalization_scheme="particle", high_order_mode="fast"), _SA),
+    ("sv_bk_000_diag_tsc", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                                sampler="tsc", interlaced=True, k_min=0.005, k_max=0.045, k_bins=4,
+                                angu_config=[0, 0, 0], data_vector_mode="diagonal", shotnoise_mode="both",
+                                normalization_scheme="particle"), _SA),
+    ("sv_bk_202_full_pcs_mixed", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                                      sampler="pcs", interlaced=True, k_min=0.005, k_max=0.045, k_bins=4,
+                                      angu_config=[2, 0, 2], data_vector_mode="full", shotnoise_mode="both",
+                                      block_size=2, normalization_scheme="mixed-mesh"), _SA),
+    ("sv_bk_110_diag_cic_mesh", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                                     sampler="cic", interlaced=False, k_min=0.005, k_max=0.045, k_bins=4,
+                                     angu_config=[1, 1, 0], data_vector_mode="diagonal",
+                                     shotnoise_mode="fft", normalization_scheme="mesh"), _SA),
+    ("sv_bk_112_full_ngp", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                                sampler="ngp", interlaced=True, k_min=0.005, k_max=0.045, k_bins=3,
+                                angu_config=[1, 1, 2], data_vector_mode="full", shotnoise_mode="both",
+                                normalization_scheme="particle", alpha_scheme="nbodykit"), _SA),
+    ("sv_bk_aab_000_full", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="aab",
+                                sampler="tsc", interlaced=True, k_min=0.005, k_max=0.045, k_bins=3,
+                                angu_config=[0, 0, 0], data_vector_mode="full", shotnoise_mode="both",
+                                normalization_scheme="mixed-mesh"), _SAB),
+    ("sv_bk_abb_202_diag", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="abb",
+                                sampler="cic", interlaced=True, k_min=0.005, k_max=0.045, k_bins=4,
+                                angu_config=[2, 0, 2], data_vector_mode="diagonal", shotnoise_mode="ana",
+                                normalization_scheme="mixed-mesh"), _SAB),
+    ("sv_bk_abc_000_diag", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="abc",
+                                sampler="tsc", interlaced=False, k_min=0.005, k_max=0.045, k_bins=4,
+                                angu_config=[0, 0, 0], data_vector_mode="diagonal", shotnoise_mode="ana",
+                                normalization_scheme="mixed-mesh"), _SABC),
+]
+
+
+def build_survey_case(name, workdir):
+    """Write the survey case's FITS catalogs under ``workdir``; return (config, checksums)."""
+    from cosmonpc_b200 import mocks
+
+    for cname, over, cats in SURVEY_CASES:
+        if cname != name:
+            continue
+        cfg = copy.deepcopy(_SURVEY_BASE)
+        cfg.update(copy.deepcopy(over))
+        catalogs = {"data_a": None, "randoms_a": None, "data_b": None, "randoms_b": None}
+        sums = {}
+        os.makedirs(workdir, exist_ok=True)
+        for letter, (seed, nd, nr, boss) in cats.items():
+            d, r = mocks.survey_catalogs(nd, nr, seed, boss_weights=boss)
+            for kind, cols in (("data", d), ("randoms", r)):
+                path = os.path.join(workdir, "%s_%s_%s.fits" % (name, kind, letter))
+                mocks.write_fits_catalog(path, cols)
+                catalogs["%s_%s" % (kind, letter)] = path
+                sums["%s_%s" % (kind, letter)] = float(sum(np.sum(v) for v in cols.values()))
+        cfg["catalogs"] = catalogs
+        cfg["output_dir"] = os.path.join(workdir, "out_" + name)
+        return cfg, sums
+    raise KeyError(name)
+
+
 def catalog_positions(seed, n_particles, boxsize):
     from cosmonpc_b200.mocks import lognormal_box
 
@@ -108,6 +198,8 @@ def catalog_weights(seed, n):
 
 def build_case(name, workdir):
     """Write the case's catalogs under ``workdir`` and return (config, checksums)."""
+    if name.startswith("sv_"):
+        return build_survey_case(name, workdir)
     for cname, over, cats in CASES:
         if cname != name:
             continue
@@ -135,6 +227,10 @@ def build_case(name, workdir):
     raise KeyError(name)
 
 
+# survey-only result / attribute keys kept in the fixtures
+SURVEY_KEYS = ("P4b", "P6b", "P8b", "N0", "I_rand", "I_data", "I_mesh", "boxcenter")
+
+
 def flatten_result(res):
     """Numeric keys of a result dict as a flat {name: ndarray} mapping."""
     out = {}
@@ -144,5 +240,7 @@ def flatten_result(res):
                 out["SN_terms." + kk] = np.asarray(vv)
         elif k in ("B_sugi", "Bk_raw", "Shot_noise", "I_norm", "k_eff", "nmodes", "k_num",
                    "P_shot") or (k.startswith("P") and k[1:].isdigit()):
+            out[k] = np.asarray(v)
+        elif (k in SURVEY_KEYS or k.startswith(("alpha_", "I_33_", "S_LM_"))) and not isinstance(v, str):
             out[k] = np.asarray(v)
     return out

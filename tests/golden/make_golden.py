@@ -26,7 +26,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
-from cases import CASES, build_case, flatten_result  # noqa: E402
+from cases import CASES, SURVEY_CASES, build_case, flatten_result  # noqa: E402
 from ref_shims import import_reference  # noqa: E402
 
 
@@ -36,7 +36,7 @@ def main(names=None):
     # catalogs live in a folder named "golden": the bispectrum output file name
     # carries the catalog's parent folder name (task_executor.py:305-309)
     work = os.path.join(tempfile.mkdtemp(prefix="cnpc_golden_"), "golden")
-    for name, _, _ in CASES:
+    for name, _, _ in CASES + SURVEY_CASES:
         if names and name not in names:
             continue
         cfg, sums = build_case(name, work)
