@@ -25,8 +25,18 @@ EXPORTED = (
     "cnpc_ctx_create", "cnpc_ctx_destroy", "cnpc_ctx_last_error", "cnpc_status_string",
     "cnpc_version", "cnpc_paint", "cnpc_fft_r2c", "cnpc_fft_c2r", "cnpc_forward_finish",
     "cnpc_kbin_counts", "cnpc_pk_bins", "cnpc_sn_bins", "cnpc_shell_spectra",
-    "cnpc_contract_gram", "cnpc_contract_gram_noalloc",
+    "cnpc_contract_gram", "cnpc_contract_gram_noalloc", "cnpc_paint_ex", "cnpc_catalog_decode",
+    "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
+    "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
+    "cnpc_survey_hermitian_accumulate",
 )
+
+# survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
+COL_RA, COL_DEC, COL_Z, COL_WEIGHT, COL_SYSTOT, COL_NOZ, COL_CP, COL_FKP, COL_NZ, NCOLS = range(10)
+CT_ABSENT, CT_F64, CT_F32, CT_I16, CT_I32, CT_I64, CT_U8, CT_BOOL = range(8)
+CT_OF_FITS = {"D": CT_F64, "E": CT_F32, "I": CT_I16, "J": CT_I32, "K": CT_I64, "B": CT_U8, "L": CT_BOOL}
+W_COLUMN, W_ONE, W_BOSS, W_EBOSS = range(4)
+PSUM_COUNT = 5
 
 
 class CnpcError(RuntimeError):
@@ -38,6 +48,28 @@ class ShellItem(ctypes.Structure):
 
     _fields_ = [("bin", ctypes.c_int), ("harmonic", ctypes.c_int), ("component", ctypes.c_int),
                 ("source", ctypes.c_int), ("conj", ctypes.c_int)]
+
+
+class Column(ctypes.Structure):
+    """Mirror of ``cnpc_column``."""
+
+    _fields_ = [("type", ctypes.c_int), ("offset", ctypes.c_int), ("scale", ctypes.c_double),
+                ("zero", ctypes.c_double)]
+
+
+class CatalogSpec(ctypes.Structure):
+    """Mirror of ``cnpc_catalog_spec``."""
+
+    _fields_ = [("row_bytes", ctypes.c_int64), ("col", Column * 9), ("weight_rule", ctypes.c_int),
+                ("has_zrange", ctypes.c_int), ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("h", ctypes.c_double), ("omega_m", ctypes.c_double)]
+
+
+class Operand(ctypes.Structure):
+    """Mirror of ``cnpc_operand``."""
+
+    _fields_ = [("p", ctypes.c_void_p), ("q", ctypes.c_void_p), ("scale", ctypes.c_double),
+                ("comp", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p
@@ -65,6 +97,22 @@ _SIGS = {
                            ctypes.POINTER(ShellItem), _i, _vp, _vp],
     "cnpc_contract_gram": [_vp, _i, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
     "cnpc_contract_gram_noalloc": [_i, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
+    "cnpc_paint_ex": [_vp, _i, _vp, _vp, _i64, _i, _d, _i, _dp, _d, _i, _vp, _vp, _vp],
+    "cnpc_catalog_decode": [_vp, _vp, _i64, ctypes.POINTER(CatalogSpec), _vp, _vp, _vp, _vp,
+                            ctypes.POINTER(_i64), _vp],
+    "cnpc_particle_sums": [_vp, _i64, _vp, _vp, _vp, _vp, ctypes.POINTER(Harmonic), _i, _vp, _vp],
+    "cnpc_catalog_weights": [_vp, _i64, _vp, _vp, _i, _vp, _vp],
+    "cnpc_interlace_split": [_vp, _i, _i, _d, _vp, _vp, _d, _i, _vp, _vp, _vp],
+    "cnpc_xspace_harmonic": [_vp, _i, _i, _d, _dp, _vp, _vp, ctypes.POINTER(Harmonic), _i, _d, _vp, _vp,
+                             _vp],
+    "cnpc_survey_bins": [_vp, _i, _i, _d, _i, ctypes.POINTER(Operand), ctypes.POINTER(Operand), _d, _d,
+                         ctypes.POINTER(Harmonic), _i, _d, _dp, _i, _vp, _vp],
+    "cnpc_survey_source": [_vp, _i, _i, _d, _i, ctypes.POINTER(Operand), ctypes.POINTER(Operand), _d, _d,
+                           _d, _vp, _vp, _vp],
+    "cnpc_field_product_sum": [_vp, _i, _i64, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _vp],
+    "cnpc_field_axpby": [_vp, _i, _i64, _d, _vp, _d, _vp, _vp, _vp],
+    "cnpc_survey_hermitian_accumulate": [_vp, _i, _i, _d, _i, ctypes.POINTER(Operand),
+                                         ctypes.POINTER(Harmonic), _d, _vp, _vp],
 }
 
 _lib = None
@@ -104,7 +152,10 @@ def _ptr(t):
 
 # kernels each entry point launches (cuFFT's own kernels are not counted)
 KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins": 1, "sn_bins": 1,
-                    "shell_spectra": 1, "gram": 2}
+                    "shell_spectra": 1, "gram": 2, "catalog_decode": 3, "particle_sums": 2,
+                    "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
+                    "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
+                    "hermitian_accumulate": 1}
 launch_count = 0
 
 
@@ -290,4 +341,103 @@ class Context:
         self._check(st, "cnpc_contract_gram")
         _count("gram")
         _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * _esz(dtype))
-        # (FP32 launches run on the tensor cores: gram_mma_kernel)
+
+    # ------------------------------------------------------ survey path
+    def paint_ex(self, dtype, pos, weight, n, boxsize, window, origin, mass_scale, accumulate, mesh,
+                 mesh_shifted):
+        o, op = _darr(origin if origin is not None else [0.0, 0.0, 0.0])
+        e0 = _tstart()
+        st = self.lib.cnpc_paint_ex(self.h, dtype, _ptr(pos), _ptr(weight), pos.shape[0], n, boxsize,
+                                    window, op, float(mass_scale), int(bool(accumulate)), _ptr(mesh),
+                                    _ptr(mesh_shifted), self.stream())
+        self._check(st, "cnpc_paint_ex")
+        _count("paint")
+        _tstop("paint", e0, pos.shape[0] * (24 + (8 if weight is not None else 0))
+               + n ** 3 * _esz(dtype) * (2 if mesh_shifted is not None else 1))
+
+    def catalog_decode(self, rows, nrows, spec, pos, w, wfkp, nz):
+        kept = _i64(0)
+        st = self.lib.cnpc_catalog_decode(self.h, _ptr(rows), nrows, ctypes.byref(spec), _ptr(pos), _ptr(w),
+                                          _ptr(wfkp), _ptr(nz), ctypes.byref(kept), self.stream())
+        self._check(st, "cnpc_catalog_decode")
+        _count("catalog_decode")
+        return int(kept.value)
+
+    def particle_sums(self, np_, pos, w, wfkp, nz, harmonics, out):
+        harr = (Harmonic * max(1, len(harmonics)))(*harmonics)
+        st = self.lib.cnpc_particle_sums(self.h, np_, _ptr(pos), _ptr(w), _ptr(wfkp), _ptr(nz), harr,
+                                         len(harmonics), _ptr(out), self.stream())
+        self._check(st, "cnpc_particle_sums")
+        _count("particle_sums")
+
+    def catalog_weights(self, np_, w, wfkp, power, out):
+        st = self.lib.cnpc_catalog_weights(self.h, np_, _ptr(w), _ptr(wfkp), power, _ptr(out), self.stream())
+        self._check(st, "cnpc_catalog_weights")
+        _count("catalog_weights")
+
+    def interlace_split(self, dtype, n, boxsize, spec, spec2, scale, accumulate, herm, anti):
+        e0 = _tstart()
+        st = self.lib.cnpc_interlace_split(self.h, dtype, n, boxsize, _ptr(spec), _ptr(spec2), float(scale),
+                                           int(bool(accumulate)), _ptr(herm), _ptr(anti), self.stream())
+        self._check(st, "cnpc_interlace_split")
+        _count("interlace_split")
+        _tstop("interlace_split", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * 4)
+
+    def xspace_harmonic(self, dtype, n, boxsize, boxcenter, re, im, harmonic, conj, scale, out_re, out_im):
+        b, bp = _darr(boxcenter)
+        e0 = _tstart()
+        st = self.lib.cnpc_xspace_harmonic(self.h, dtype, n, boxsize, bp, _ptr(re), _ptr(im),
+                                           ctypes.byref(harmonic), int(bool(conj)), float(scale), _ptr(out_re),
+                                           _ptr(out_im), self.stream())
+        self._check(st, "cnpc_xspace_harmonic")
+        _count("xspace_harmonic")
+        nio = 1 + (im is not None) + 1 + (out_im is not None)
+        _tstop("xspace_harmonic", e0, n ** 3 * _esz(dtype) * nio)
+
+    @staticmethod
+    def operand(p, q=None, scale=1.0, comp=COMP_NONE):
+        return Operand(_ptr(p), _ptr(q), float(scale), int(comp))
+
+    def survey_bins(self, dtype, n, boxsize, window, u, v, sbar, harmonic, conj_z, weight, edges, sums):
+        e, ep = _darr(edges)
+        hp = ctypes.byref(harmonic) if harmonic is not None else None
+        e0 = _tstart()
+        st = self.lib.cnpc_survey_bins(self.h, dtype, n, boxsize, window, ctypes.byref(u), ctypes.byref(v),
+                                       float(np.real(sbar)), float(np.imag(sbar)), hp, int(bool(conj_z)),
+                                       float(weight), ep, len(e), _ptr(sums), self.stream())
+        self._check(st, "cnpc_survey_bins")
+        _count("survey_bins")
+        nsp = 2 + (u.q is not None) + (v.q is not None)
+        _tstop("survey_bins", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * nsp)
+
+    def survey_source(self, dtype, n, boxsize, window, u, v, sbar, band, herm, anti):
+        e0 = _tstart()
+        st = self.lib.cnpc_survey_source(self.h, dtype, n, boxsize, window, ctypes.byref(u), ctypes.byref(v),
+                                         float(np.real(sbar)), float(np.imag(sbar)), float(band), _ptr(herm),
+                                         _ptr(anti), self.stream())
+        self._check(st, "cnpc_survey_source")
+        _count("survey_source")
+        _tstop("survey_source", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * 5)
+
+    def hermitian_accumulate(self, dtype, n, boxsize, window, x, harmonic, weight, out):
+        e0 = _tstart()
+        st = self.lib.cnpc_survey_hermitian_accumulate(self.h, dtype, n, boxsize, window, ctypes.byref(x),
+                                                       ctypes.byref(harmonic), float(weight), _ptr(out),
+                                                       self.stream())
+        self._check(st, "cnpc_survey_hermitian_accumulate")
+        _count("hermitian_accumulate")
+        _tstop("hermitian_accumulate", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * 4)
+
+    def field_product_sum(self, dtype, ncell, res, ims, out):
+        nf = len(res)
+        ra = (_vp * nf)(*[_ptr(t) for t in res])
+        ia = (_vp * nf)(*[_ptr(t) for t in ims])
+        st = self.lib.cnpc_field_product_sum(self.h, dtype, ncell, nf, ra, ia, _ptr(out), self.stream())
+        self._check(st, "cnpc_field_product_sum")
+        _count("field_product_sum")
+
+    def field_axpby(self, dtype, ncell, a, x, b, y, out):
+        st = self.lib.cnpc_field_axpby(self.h, dtype, ncell, float(a), _ptr(x), float(b), _ptr(y), _ptr(out),
+                                       self.stream())
+        self._check(st, "cnpc_field_axpby")
+        _count("field_axpby")

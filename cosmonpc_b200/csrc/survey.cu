@@ -537,6 +537,37 @@ __global__ void survey_source_kernel(OperandDev u, OperandDev v, int n, double L
     }
 }
 
+
+// out(k) += weight * (Z(k) X(k) + conj(Z(-k) X(-k))) / 2 with Z = Y(khat)
+// (Y(-khat) = (-1)^l Y(khat)): the Hermitian part of Y X, accumulated.
+template <typename T>
+__global__ void hermitian_accumulate_kernel(OperandDev x, int n, double L, int p, unsigned kinds,
+                                            cnpc_harmonic zh, double weight, cpx_t<T> *out, int64_t nh) {
+    extern __shared__ double sm[];
+    CompTables ct;
+    fill_comp_tables(ct, sm, n, L, p, kinds);
+    __syncthreads();
+    const int parity = (zh.l & 1) ? -1 : 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
+        const Mode m = mode_of(t, n);
+        const double kx = ct.k[m.nx + ct.half], ky = ct.k[m.ny + ct.half], kz = ct.k[m.nz + ct.half];
+        const double kn = knorm_from(kx, ky, kz);
+        const bool origin = kn == 0.0;
+        const double2 y = harmonic_eval<double>(zh, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
+                                                origin ? 0.0 : kz / kn, origin);
+        double2 xk, xm;
+        load_operand<T>(x, t, ct.factor(x.comp, m.nx, m.ny, m.nz), &xk, &xm);
+        // Z(k) X(k)
+        const double ar = y.x * xk.x - y.y * xk.y, ai = y.x * xk.y + y.y * xk.x;
+        // conj(Z(-k) X(-k)) = parity * conj(Y) conj(X(-k))
+        const double br = parity * (y.x * xm.x - y.y * xm.y);
+        const double bi = -parity * (y.x * xm.y + y.y * xm.x);
+        const double hr = 0.5 * weight * (ar + br), hi = 0.5 * weight * (ai + bi);
+        out[t] = mk<T>((T)((double)out[t].x + hr), (T)((double)out[t].y + hi));
+    }
+}
+
 // --------------------------------------------------- x-space reductions
 template <typename T>
 __global__ void product_sum_kernel(int64_t ncell, int nf, const T *r0, const T *i0, const T *r1, const T *i1,
@@ -822,6 +853,31 @@ int cnpc_survey_source(cnpc_ctx *ctx, int dtype, int n, double boxsize, int wind
         survey_source_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, band_kmax, (double2 *)d_herm, (double2 *)d_anti, nh);
     return check_launch(ctx, "survey_source_kernel");
+}
+
+int cnpc_survey_hermitian_accumulate(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window,
+                                     const cnpc_operand *x, const cnpc_harmonic *h_y, double weight,
+                                     void *d_out, cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
+    CNPC_REQUIRE(ctx, h_y && d_out, "null argument");
+    CNPC_REQUIRE(ctx, h_y->l >= 0 && h_y->l <= 8 && std::abs(h_y->m) <= h_y->l, "harmonic out of range");
+    OperandDev dx;
+    if ((st = check_operand(ctx, x, &dx))) return st;
+    const unsigned kinds = (1u << dx.comp) & 0xeu;
+    const int ntab = 1 + __builtin_popcount(kinds);
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    const size_t smem = sizeof(double) * ntab * (n + 1);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == CNPC_F32)
+        hermitian_accumulate_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            dx, n, boxsize, window, kinds, *h_y, weight, (float2 *)d_out, nh);
+    else
+        hermitian_accumulate_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
+            dx, n, boxsize, window, kinds, *h_y, weight, (double2 *)d_out, nh);
+    return check_launch(ctx, "hermitian_accumulate_kernel");
 }
 
 int cnpc_field_product_sum(cnpc_ctx *ctx, int dtype, int64_t ncell, int nf, const void *const *h_re,

@@ -33,6 +33,16 @@ def _save(output_dir, name, res):
 
 def run_task(statistic, correlation_mode, geometry, catalogs, **kwargs):
     """task_executor.py:11-328."""
+    from . import survey
+
+    survey.clear_cache()
+    try:
+        return _run_task(statistic, correlation_mode, geometry, catalogs, **kwargs)
+    finally:
+        survey.clear_cache()
+
+
+def _run_task(statistic, correlation_mode, geometry, catalogs, **kwargs):
     k_max, nmesh, boxsize = kwargs["k_max"], kwargs["nmesh"], kwargs["boxsize"]
     nyquist_freq = np.pi * nmesh[0] / boxsize[0]
     precision = kwargs.get("precision", "f64")

@@ -295,6 +295,15 @@ int cnpc_survey_source(cnpc_ctx *ctx, int dtype, int n, double boxsize, int wind
                        const cnpc_operand *u, const cnpc_operand *v, double sbar_re, double sbar_im,
                        double band_kmax, void *d_herm, void *d_anti, cnpc_stream_t stream);
 
+/* d_out(k) += weight * (Y(khat) X(k) + conj(Y(-khat) X(-k))) / 2: the
+ * Hermitian part of Y X for the operand x (a half spectrum, accumulated).
+ * Summed over m with the weights of get_G_ell it gives the fast-mode fields
+ * F_l = (G_l + conj G_l(-k)) / 2 of ce:402-417 without the space-inversion
+ * exchange of math_evaluator.py:806-977. */
+int cnpc_survey_hermitian_accumulate(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window,
+                                     const cnpc_operand *x, const cnpc_harmonic *h_y, double weight,
+                                     void *d_out, cnpc_stream_t stream);
+
 /* d_out[0] + i d_out[1] = sum_x prod_{j < nf} (re_j(x) + i im_j(x)), nf 1..3,
  * h_re / h_im: host arrays of nf device pointers (h_im or its entries may be
  * NULL).  Replaces the normalisation sums np.sum(D * R) and friends

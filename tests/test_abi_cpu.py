@@ -68,3 +68,26 @@ def test_device_path_fails_loudly_without_gpu():
 
     with pytest.raises(RuntimeError):
         _lib.Context.get()
+
+
+def test_survey_struct_layouts_match_c_compiler(tmp_path):
+    """sizeof / offsetof of the survey structs as gcc lays them out from the header."""
+    import subprocess
+
+    from cosmonpc_b200 import _lib
+
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "cosmonpc_b200.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(cnpc_column), sizeof(cnpc_catalog_spec),'
+        ' sizeof(cnpc_operand), offsetof(cnpc_catalog_spec, weight_rule), offsetof(cnpc_catalog_spec, h),'
+        ' offsetof(cnpc_operand, comp), sizeof(cnpc_harmonic)); return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    from cosmonpc_b200.angular import Harmonic
+
+    want = [ctypes.sizeof(_lib.Column), ctypes.sizeof(_lib.CatalogSpec), ctypes.sizeof(_lib.Operand),
+            _lib.CatalogSpec.weight_rule.offset, _lib.CatalogSpec.h.offset, _lib.Operand.comp.offset,
+            ctypes.sizeof(Harmonic)]
+    assert got == want
