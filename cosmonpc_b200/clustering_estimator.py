@@ -184,6 +184,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
     other = spec["a"] if correlation_mode == "auto" else spec.get("b")
     sn_sums = {}
     src_fields = {}
+    src_origin = {}
     cfg_info = []
     for (l1, l2, L_) in angu_configs:
         sn0 = N_gal["a"] if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
@@ -206,6 +207,14 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
             fld = torch.empty(n * n * n, dtype=rdt, device=dev)
             ctx.c2r(code, n, 1, src_spec, fld)
             del src_spec
+            if precision == "f32":
+                # x = 0 cell added in FP64 (engine.origin_correction)
+                d0 = torch.empty(2, dtype=torch.float64, device=dev)
+                ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                            float(sn0) if correlation_mode == "auto" else 0.0, window, None,
+                            [0.0, 2.0 * k_max], d0)
+                src_origin[sn0] = engine.HostCopy(d0)
+                fld[0] = 0.0
             src_fields[sn0] = fld
 
     # ---- signal: G_00 = Re c2r(delta) band-limited to |k| < 2 k_max (the only
@@ -244,6 +253,9 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         outs = engine.pair_sums(s3_groups, sfu, k_bins, diagonal, bsf)
         s3fft = {ci: outs[gi] for ci, gi in s3_index.items()}
         del sfu
+        if src_origin:
+            legs = [ps.leg1 for ps in all_sp] + [ps.leg2 for ps in all_sp if ps.mode == "leg"]
+            shell_origin = engine.unit_shell_origin(n, L, k_edge, precision, legs)
 
     # ---- host algebra while the GPU drains the queue
     ck = counts_k.get()
@@ -303,8 +315,13 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
                     return np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
                 ss_list = s3fft[ci].result()
                 s3 = np.zeros((k_bins, k_bins) if not diagonal else k_bins, dtype="complex128")
+                specs_ci = s3_groups[s3_index[ci]][1]
                 for ss, (m1, m2, _) in enumerate(cfgs):
                     S = ss_list[ss]
+                    if src_origin:
+                        v0 = src_origin[cfg_info[ci]].get()
+                        S = S + engine.origin_correction(specs_ci[ss], shell_origin, complex(v0[0], v0[1]),
+                                                         k_bins, diagonal)
                     if diagonal:
                         sub = np.zeros(k_bins, dtype="complex128")
                         ok = k_num > 0

@@ -390,8 +390,13 @@ struct OperandDev {
 
 template <typename T>
 __device__ inline void load_operand(const OperandDev &o, int64_t t, double f, double2 *vk, double2 *vm) {
-    const cpx_t<T> P = static_cast<const cpx_t<T> *>(o.p)[t];
     const double s = o.scale * f;
+    if (!o.p) {  // the unit spectrum
+        *vk = make_double2(s, 0.0);
+        *vm = *vk;
+        return;
+    }
+    const cpx_t<T> P = static_cast<const cpx_t<T> *>(o.p)[t];
     if (!o.q) {
         *vk = make_double2(s * (double)P.x, s * (double)P.y);
         *vm = make_double2(vk->x, -vk->y);
@@ -618,7 +623,8 @@ __global__ void axpby_kernel(int64_t ncell, double a, const T *x, double b, cons
 }
 
 static int check_operand(cnpc_ctx *ctx, const cnpc_operand *o, OperandDev *d) {
-    CNPC_REQUIRE(ctx, o != nullptr && o->p != nullptr, "null operand");
+    CNPC_REQUIRE(ctx, o != nullptr, "null operand");
+    CNPC_REQUIRE(ctx, o->p != nullptr || o->q == nullptr, "operand with q but no p");
     CNPC_REQUIRE(ctx, o->comp >= CNPC_COMP_NONE && o->comp <= CNPC_COMP_BKNOISE, "bad compensation kind");
     d->p = o->p;
     d->q = o->q;

@@ -234,7 +234,7 @@ def contract(G, sf, rows, cols):
         return False
 
     if sf.precision == "f32":
-        # tensor-core launches cover at most 48 rows x 24 columns
+        # one FP32 contraction launch covers at most 48 rows x 24 columns
         rb, cb = 48, 24
         if len(ridx) <= rb and len(cidx) <= cb:
             blocks = [(0, len(ridx), 0, len(cidx))]
@@ -371,6 +371,50 @@ def pair_sums(groups, sf, k_bins, diagonal, block_size):
                 outs[gi].add(contract(G, sf, rows_g[gi], cols_g[gi]), rows_g[gi], cols_g[gi], bi, bj)
         sf.release_all()
     return outs
+
+
+# ------------------------------------------------ x = 0 cell of FFT S3 sums
+# The FFT S3 source has a spike at x = 0 (the shot-noise constant S W(k) is
+# nearly flat in k), where the shell fields also peak.  In FP32 that one
+# product dominates the rounding of sum_x src F1 F2, so the FP32 contraction
+# runs with the source's x = 0 cell zeroed and the cell's product is added in
+# FP64: src(0) = sum_k src(k) and F(0) = sum_{k in bin} conj?(Y(khat)) are mode
+# sums evaluated in FP64 from the spectra.
+
+def unit_shell_origin(n, boxsize, edges, precision, legs):
+    """{leg: HostCopy of complex F(0) per bin} for unit-spectrum shell legs
+    (l, m, 2, conj): F(0) = sum over the bin's full-space modes of Y or conj Y."""
+    ctx = _lib.Context.get()
+    code = PRECISION[precision][0]
+    unit = ctx.operand(None)
+    out = {}
+    for leg in dict.fromkeys(legs):
+        l, m, src, conj = leg
+        if src != 2:
+            raise ValueError("origin values are defined for unit-spectrum legs only")
+        d = torch.empty(2 * (len(edges) - 1), dtype=torch.float64, device=_device())
+        ctx.survey_bins(code, n, float(boxsize), 1, unit, unit, 0.0, angular.harmonic(l, m, True), conj, 1.0,
+                        edges, d)
+        out[leg] = HostCopy(d)
+    return out
+
+
+def origin_correction(ps, origin, src0, k_bins, diagonal):
+    """src(0) F1_i(0) F2_j(0) for one pair spec (k_bins x k_bins, or the diagonal)."""
+    def vals(leg):
+        v = origin[leg].get()
+        return v[0::2] + 1j * v[1::2]
+
+    f1 = vals(ps.leg1)
+    if ps.mode == "eq":
+        f2 = f1
+    elif ps.mode == "conj":
+        f2 = ps.sign * np.conj(f1)
+    else:
+        f2 = vals(ps.leg2)
+    if diagonal:
+        return src0 * f1 * f2
+    return src0 * np.outer(f1, f2)
 
 
 def fields_capacity(n, precision, want, reserve_bytes=0):

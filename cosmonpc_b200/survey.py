@@ -138,7 +138,7 @@ def _decode_file(path, column_names, z_range, comp_weight_plan, catalog_type, co
     spec.omega_m = float(cosmology["Omega0"])
     dev = _device()
     nr = t.nrows
-    rows = torch.from_numpy(np.ascontiguousarray(t.rows()).reshape(-1)).pin_memory().to(dev)
+    rows = torch.from_numpy(np.array(t.rows(), copy=True).reshape(-1)).pin_memory().to(dev)
     cap = max(nr, 1)
     pos = torch.empty((cap, 3), dtype=torch.float64, device=dev)
     w = torch.empty(cap, dtype=torch.float64, device=dev)
@@ -253,6 +253,19 @@ def paint_field(items, n, boxsize, sampler, interlaced, boxcenter, precision):
     return SurveyField(mesh[0], mesh[1], n, boxsize, sampler, interlaced, precision, boxcenter)
 
 
+def to_precision(field, precision):
+    """The field rounded to ``precision`` once it is formed: the FKP and N fields
+    are painted, combined and interlace-split in FP64 (D - alpha R cancels to a
+    few per cent of D, which FP32 accumulation would not resolve) and only the
+    finished field is held in FP32 for the estimator stages."""
+    if precision == field.precision:
+        return field
+    rdt = engine.PRECISION[precision][1]
+    im = None if field.im is None else field.im.to(rdt)
+    return SurveyField(field.re.to(rdt), im, field.n, field.boxsize, field.sampler, field.interlaced, precision,
+                       field.boxcenter)
+
+
 def combine(a, X, b, Y):
     """a X + b Y (the x-space field arithmetic of mg:449-454, :666-668)."""
     ctx = _lib.Context.get()
@@ -337,11 +350,11 @@ def get_mesh_pk_survey(catalogs, correlation_mode, nmesh, geometry, column_names
     def fields(d, r, alpha):
         wd, wr = d.paint_weights(), r.paint_weights()
         if not separate:
-            F = paint_field([(d, wd, 1.0 / dV), (r, wr, -alpha / dV)], n, L, sampler, interlaced, bc, precision)
-            return F, None, None
-        D = paint_field([(d, wd, 1.0 / dV)], n, L, sampler, interlaced, bc, precision)
-        R = paint_field([(r, wr, 1.0 / dV)], n, L, sampler, interlaced, bc, precision)
-        return combine(1.0, D, -alpha, R), D, R
+            F = paint_field([(d, wd, 1.0 / dV), (r, wr, -alpha / dV)], n, L, sampler, interlaced, bc, "f64")
+            return to_precision(F, precision), None, None
+        D = paint_field([(d, wd, 1.0 / dV)], n, L, sampler, interlaced, bc, "f64")
+        R = paint_field([(r, wr, 1.0 / dV)], n, L, sampler, interlaced, bc, "f64")
+        return to_precision(combine(1.0, D, -alpha, R), precision), D, R
 
     fa, Da, Ra = fields(da, ra, alpha_a)
     fb = fa
@@ -544,13 +557,13 @@ def get_mesh_bk_survey(catalogs, correlation_mode, tracer_type, angu_config, nme
         attrs[f"S_LM_{label}"] = (sd.S_LM - alpha ** 3 * sr.S_LM) if auto else 0.0
         wd, wr = d.paint_weights(), r.paint_weights()
         if not (keep[label]["D"] or keep[label]["R"]):
-            F = paint_field([(d, wd, 1.0 / dV), (r, wr, -alpha / dV)], n, L, sampler, interlaced, bc, precision)
+            F = paint_field([(d, wd, 1.0 / dV), (r, wr, -alpha / dV)], n, L, sampler, interlaced, bc, "f64")
         else:
-            D = paint_field([(d, wd, 1.0 / dV)], n, L, sampler, interlaced, bc, precision)
-            R = paint_field([(r, wr, alpha / dV)], n, L, sampler, interlaced, bc, precision)
+            D = paint_field([(d, wd, 1.0 / dV)], n, L, sampler, interlaced, bc, "f64")
+            R = paint_field([(r, wr, alpha / dV)], n, L, sampler, interlaced, bc, "f64")
             F = combine(1.0, D, -1.0, R)
             cache[label] = (D if keep[label]["D"] else None, R if keep[label]["R"] else None)
-        fields[label] = F
+        fields[label] = to_precision(F, precision)
 
     prep("a")
     if correlation_mode == "cross":
@@ -573,8 +586,8 @@ def get_mesh_bk_survey(catalogs, correlation_mode, tracer_type, angu_config, nme
             raise ValueError("alpha_scheme must be either 'pypower' or 'nbodykit'.")
         sd, so, se = ParticleSums(d), ParticleSums(ro), ParticleSums(re_)
         a_odd, a_even = _alpha(sd, so, alpha_scheme), _alpha(sd, se, alpha_scheme)
-        Ro = paint_field([(ro, ro.paint_weights(), a_odd / dV)], n, L, sampler, interlaced, bc, precision)
-        Re = paint_field([(re_, re_.paint_weights(), a_even / dV)], n, L, sampler, interlaced, bc, precision)
+        Ro = paint_field([(ro, ro.paint_weights(), a_odd / dV)], n, L, sampler, interlaced, bc, "f64")
+        Re = paint_field([(re_, re_.paint_weights(), a_even / dV)], n, L, sampler, interlaced, bc, "f64")
         attrs["I_norm"] = dV * product_sum([D, Ro, Re])
     else:
         if tracer_type == "abc":
@@ -601,8 +614,9 @@ def get_N_field(catalogs, tracer_flag, alpha, nmesh, geometry, column_names, box
                      para_cosmo, normalization_scheme)
     d = read_catalog(catalogs[f"data_{tracer_flag}"], column_names, z_range, comp_weight_plan, "data",
                      para_cosmo, normalization_scheme)
-    return paint_field([(d, d.paint_weights(2), 1.0 / dV), (r, r.paint_weights(2), alpha ** 2 / dV)],
-                       n, L, sampler, interlaced, boxcenter, precision)
+    N = paint_field([(d, d.paint_weights(2), 1.0 / dV), (r, r.paint_weights(2), alpha ** 2 / dV)],
+                    n, L, sampler, interlaced, boxcenter, "f64")
+    return to_precision(N, precision)
 
 
 # ====================================================================== bk
@@ -904,26 +918,41 @@ def _s3_fft_sums(rshot, opn, cfgs, l1, l2, L_, S_arr, k_edge, k_bins, diagonal, 
             return 0.0 + 0.0j
         return S_arr[Mi] if Mi >= 0 else ((-1) ** Mi) * np.conj(S_arr[-Mi])
 
-    sums = {}
+    sums, origin = {}, {}
     for M in dict.fromkeys(M for (_, _, _, M, _) in plan):
         P, Q = harmonic_spectra(rshot, angular.harmonic(L_, M, True), True)
         x = ctx.operand(P, Q, scale_nv, _lib.COMP_SINC)
         src = torch.empty((2, n, n, n // 2 + 1), dtype=cdt, device=P.device)
         ctx.survey_source(rshot.code, n, rshot.boxsize, rshot.window, x, opn, s_val(M), band, src[0], src[1])
-        del P, Q
+        if rshot.precision == "f32":
+            # x = 0 cell added in FP64 (engine.origin_correction)
+            d0 = torch.empty(2, dtype=torch.float64, device=src.device)
+            ctx.survey_bins(rshot.code, n, rshot.boxsize, rshot.window, x, opn, s_val(M), None, False, 1.0,
+                            [0.0, band], d0)
+            origin[M] = engine.HostCopy(d0)
+        del P, Q, x
         fld = torch.empty((2, n * n * n), dtype=rdt, device=src.device)
         ctx.c2r(rshot.code, n, 2, src, fld)
         del src
+        if rshot.precision == "f32":
+            fld[:, 0] = 0.0
         group = {ss: (fld[0], fld[1], specs[ss]) for (ss, _, _, MM, _) in plan if MM == M}
         sums.update(_complex_pairs(group, sf, k_bins, diagonal, bs))
-    return plan, specs, sums
+    shell_origin = None
+    if origin:
+        legs = [ps.leg1 for ps in specs.values()] + [ps.leg2 for ps in specs.values() if ps.mode == "leg"]
+        shell_origin = engine.unit_shell_origin(n, rshot.boxsize, k_edge, rshot.precision, legs)
+    return plan, specs, sums, origin, shell_origin
 
 
 def _s3_fft_assemble(s3fft, cfgs, tj, l1, l2, k_num, k_bins, diagonal):
-    plan, specs, sums = s3fft
+    plan, specs, sums, origin, shell_origin = s3fft
     out = np.zeros((k_bins,) if diagonal else (k_bins, k_bins), dtype="complex128")
     for (ss, m1, m2, M, add_swap) in plan:
         S = _resolve(sums[ss])
+        if origin:
+            v0 = origin[M].get()
+            S = S + engine.origin_correction(specs[ss], shell_origin, complex(v0[0], v0[1]), k_bins, diagonal)
         if diagonal:
             sub = np.zeros(k_bins, dtype="complex128")
             ok = k_num > 0

@@ -269,7 +269,8 @@ int cnpc_xspace_harmonic(cnpc_ctx *ctx, int dtype, int n, double boxsize, const 
 /* A spectral operand of the survey sums: Hermitian half spectrum p (q NULL),
  * or X = P + i Q for the non-Hermitian FFT of a complex field whose real and
  * imaginary parts have half spectra P and Q (X(-k) = conj P + i conj Q).
- * The operand's value is scale * comp(k) * (p or X). */
+ * p NULL (and q NULL) is the unit spectrum.  The operand's value is
+ * scale * comp(k) * (p, X or 1). */
 typedef struct cnpc_operand {
     const void *p;
     const void *q;
@@ -336,7 +337,7 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
  * library routine: the per-block partial sums live in one fixed 8 MiB array in
  * the library's device memory, which every GPU that loads the library holds
  * until the process exits.  The caller still owns G, the fields and d_out.
- *  - Limits per call: CNPC_F32 at most 48 rows x 24 columns (one tensor-core
+ *  - Limits per call: CNPC_F32 at most 48 rows x 24 columns (one contraction
  *    launch); CNPC_F64 at most 128 x 128 with 1 + pad8(na) [+ pad4(nb) when
  *    b is not a contiguous run of a] <= 110 staged rows.  Larger calls, or
  *    misaligned fields (16-byte base, field_stride and ncell), return
