@@ -28,7 +28,7 @@ EXPORTED = (
     "cnpc_contract_gram", "cnpc_contract_gram_noalloc", "cnpc_paint_ex", "cnpc_catalog_decode",
     "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
-    "cnpc_survey_hermitian_accumulate",
+    "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -113,6 +113,8 @@ _SIGS = {
     "cnpc_field_axpby": [_vp, _i, _i64, _d, _vp, _d, _vp, _vp, _vp],
     "cnpc_survey_hermitian_accumulate": [_vp, _i, _i, _d, _i, ctypes.POINTER(Operand),
                                          ctypes.POINTER(Harmonic), _d, _vp, _vp],
+    "cnpc_shell_fields": [_vp, _i, _d, _vp, _vp, _dp, _i, ctypes.POINTER(Harmonic), _i,
+                          ctypes.POINTER(ShellItem), _i, ctypes.POINTER(_vp), _vp],
 }
 
 _lib = None
@@ -155,7 +157,7 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "shell_spectra": 1, "gram": 2, "catalog_decode": 3, "particle_sums": 2,
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
-                    "hermitian_accumulate": 1}
+                    "hermitian_accumulate": 1, "shell_fields": 2}
 launch_count = 0
 
 
@@ -331,6 +333,22 @@ class Context:
         _count("shell_spectra")
         nsrc = len({it.source for it in items if it.source < 2})
         _tstop("shell_spectra", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * (len(items) + nsrc))
+
+    def shell_fields(self, n, boxsize, a, b, edges, harmonics, items, outs):
+        """Fused synthesis + band-limited inverse FFT of FP32 shell fields."""
+        e, ep = _darr(edges)
+        harr = (Harmonic * len(harmonics))(*harmonics)
+        iarr = (ShellItem * len(items))(*items)
+        optr = (_vp * len(outs))(*[_ptr(t) for t in outs])
+        e0 = _tstart()
+        st = self.lib.cnpc_shell_fields(self.h, n, boxsize, _ptr(a), _ptr(b), ep, len(e), harr, len(harmonics),
+                                        iarr, len(items), optr, self.stream())
+        self._check(st, "cnpc_shell_fields")
+        _count("shell_fields")
+        nsrc = len({it.source for it in items if it.source < 2})
+        # algorithmic: band of each source read once, each field written once
+        band = n * (n // 2) * (n // 4) * 8
+        _tstop("shell_fields", e0, len(items) * n ** 3 * 4 + nsrc * band // 2)
 
     def gram(self, dtype, ncell, g, fields, stride, a_idx, b_idx, out):
         a, ap = _iarr(a_idx)

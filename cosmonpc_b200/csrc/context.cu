@@ -124,6 +124,7 @@ int cnpc_ctx_destroy(cnpc_ctx *ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->paint_ws) cudaFree(ctx->paint_ws);
     if (ctx->aux) cudaFree(ctx->aux);
+    if (ctx->shell_ws) cudaFree(ctx->shell_ws);
     delete ctx;
     return CNPC_OK;
 }

@@ -24,6 +24,9 @@ struct cnpc_ctx {
     // workspace of the catalog and survey reductions (block counts, partials)
     void *aux = nullptr;
     size_t aux_bytes = 0;
+    // workspace of the fused shell-field transform (output table + pass-1 columns)
+    void *shell_ws = nullptr;
+    size_t shell_ws_bytes = 0;
     int num_sms = 148;
 };
 

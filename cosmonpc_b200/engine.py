@@ -101,6 +101,18 @@ def kbin_counts(n, boxsize, edges):
 # Extra elements between consecutive shell fields (0: contiguous batches,
 # which cuFFT writes fastest).
 FIELD_PAD = 0
+# FP32 shell fields of n = 64/128/256 whose bins lie below k_Nyquist / 2 are
+# synthesised and inverse-transformed by the fused band-limited kernels
+# (cnpc_shell_fields) instead of shell spectra + cuFFT C2R.
+FUSED_SHELLS = True
+
+
+def fused_shells_apply(n, boxsize, edges, bins, precision):
+    if not FUSED_SHELLS or precision != "f32" or n not in (64, 128, 256):
+        return False
+    kf = 2.0 * np.pi / float(boxsize)
+    top = max(float(edges[b + 1]) for b in bins)
+    return top / kf < n / 4.0
 
 
 def leg_components(l, m):
@@ -133,9 +145,17 @@ class ShellFields:
         self.stride = n * n * n + FIELD_PAD
         self.fields = torch.empty((self.capacity, self.stride), dtype=self.rdt, device=dev)
         self.fft_batch = max(1, min(int(fft_batch), self.capacity))
-        self.scratch = torch.empty((self.fft_batch, n, n, n // 2 + 1), dtype=self.cdt, device=dev)
+        self._scratch = None
         self.slot = {}
         self.free = list(range(self.capacity))[::-1]
+
+    @property
+    def scratch(self):
+        """Half spectra of one FFT batch (only the cuFFT route needs them)."""
+        if self._scratch is None:
+            n = self.n
+            self._scratch = torch.empty((self.fft_batch, n, n, n // 2 + 1), dtype=self.cdt, device=_device())
+        return self._scratch
 
     def key(self, leg, b, comp):
         return (tuple(leg), int(b), int(comp))
@@ -168,6 +188,13 @@ class ShellFields:
                     harm_index[hk] = len(harmonics)
                     harmonics.append(angular.harmonic(l, m, self.racah))
                 items.append(_lib.ShellItem(b, harm_index[hk], comp, src, 1 if conj else 0))
+            if fused_shells_apply(self.n, self.boxsize, self.edges, [k[1] for k in batch], self.precision):
+                slots = [self.free.pop() for _ in batch]
+                ctx.shell_fields(self.n, self.boxsize, self.spec_a, self.spec_b, self.edges, harmonics, items,
+                                 [self.fields[s] for s in slots])
+                for k, s in zip(batch, slots):
+                    self.slot[k] = s
+                continue
             ctx.shell_spectra(self.code, self.n, self.boxsize, self.spec_a, self.spec_b, self.edges,
                               harmonics, items, self.scratch)
             slots = [self.free.pop() for _ in batch]
@@ -187,7 +214,7 @@ def band_limited_field(n, boxsize, spec, kmax_band, precision, racah=True):
     sf = ShellFields(n, boxsize, [0.0, float(kmax_band)], precision, spec, None, capacity=1, fft_batch=1)
     sf.ensure([sf.key((0, 0, 0, False), 0, 0)])
     out = sf.fields[0]
-    del sf.scratch
+    sf._scratch = None
     return out
 
 

@@ -317,6 +317,22 @@ int cnpc_field_product_sum(cnpc_ctx *ctx, int dtype, int64_t ncell, int nf, cons
 int cnpc_field_axpby(cnpc_ctx *ctx, int dtype, int64_t ncell, double a, const void *d_x, double b,
                      const void *d_y, void *d_out, cnpc_stream_t stream);
 
+/* Shell fields in one call, FP32: the real fields
+ *   h_out_fields[j] = c2r(src * Y * mask_bin * phi)   (item j, as in
+ * cnpc_shell_spectra followed by cnpc_fft_c2r) for n = 64, 128 or 256, when
+ * every item's bin lies below k = (n/4) 2 pi / L -- always the case for the
+ * bispectrum shells, whose top edge k_max is below k_Nyquist / 2 by the
+ * reference's own check (task_executor.py:192-196).  The inverse FFT runs on
+ * the band only (x pass on the in-band columns, then y and z per x-slab in
+ * shared memory) and each field is written once.  Output fields are n^3
+ * floats, 16-byte aligned; h_out_fields is a host array of nitems device
+ * pointers. */
+int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const void *d_spec_a,
+                      const void *d_spec_b, const double *h_edges, int nedges,
+                      const cnpc_harmonic *h_harmonics, int nharmonics,
+                      const cnpc_shell_item *h_items, int nitems, void *const *h_out_fields,
+                      cnpc_stream_t stream);
+
 /* ------------------------------------------------------ x-space reductions
  * Replaces np.sum(G * F1 * F2) of clustering_estimator.py:972, :1051, :1257,
  * :1341 for real component fields.

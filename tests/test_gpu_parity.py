@@ -117,3 +117,46 @@ def test_bk_full_64_against_oracle(precision, tmp_path):
             np.testing.assert_array_equal(got[k], ref[k])
         else:
             assert rel_err(got[k], ref[k]) < TOL[precision], (k, rel_err(got[k], ref[k]))
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_fused_shell_fields_match_cufft_route(n):
+    """cnpc_shell_fields (band-limited fused transform) against shell spectra
+    followed by cuFFT C2R, for every harmonic kind, component, source and conj."""
+    import torch
+    from cosmonpc_b200 import _lib, angular
+
+    L = 1000.0 * n / 64
+    kf = 2 * np.pi / L
+    edges = np.linspace(0.0, (n / 4 - 0.5) * kf, 6)
+    ctx = _lib.Context.get()
+    rng = np.random.default_rng(n)
+    specs = []
+    for _ in range(2):
+        real = torch.from_numpy(rng.standard_normal((n, n, n)).astype(np.float32)).cuda()
+        sp = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+        ctx.r2c(_lib.F32, n, 1, real, sp)
+        specs.append(sp)
+    harms = [angular.harmonic(0, 0), angular.harmonic(2, 1), angular.harmonic(1, 1), angular.harmonic(3, -2),
+             angular.harmonic(4, 0)]
+    # (harmonic, component) pairs whose field is not identically zero
+    comps = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (3, 0), (3, 1), (4, 0)]
+    items = []
+    for j in range(10):
+        hi, c = comps[j % len(comps)]
+        items.append(_lib.ShellItem(j % 5, hi, c, j % 3, (j // 3) % 2))
+    half = torch.empty((len(items), n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    ctx.shell_spectra(_lib.F32, n, L, specs[0], specs[1], edges, harms, items, half)
+    assert half.abs().amax(dim=(1, 2, 3)).min().item() > 0
+    ref = torch.empty((len(items), n, n, n), dtype=torch.float32, device="cuda")
+    ctx.c2r(_lib.F32, n, len(items), half, ref)
+    torch.cuda.synchronize()
+    del half
+    out = torch.empty_like(ref)
+    ctx.shell_fields(n, L, specs[0], specs[1], edges, harms, items, [out[j] for j in range(len(items))])
+    torch.cuda.synchronize()
+    for j in range(len(items)):
+        a, b = out[j].double(), ref[j].double()
+        scale = b.abs().max().item()
+        assert scale > 0
+        assert (a - b).abs().max().item() < 2e-6 * scale, (j, (a - b).abs().max().item() / scale)
