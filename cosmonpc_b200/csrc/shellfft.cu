@@ -118,17 +118,26 @@ __device__ __forceinline__ void idft16(float2 *v) {
     for (int i = 0; i < 16; ++i) v[i] = o[i];
 }
 
+// Exchange slots of one team: 16 rows of T + 1 (the pad makes the transposed
+// reads conflict-free), and a team stride of 9 (mod 16) float2 so that the
+// four teams of a warp fall on disjoint bank pairs two by two.
+template <int T> struct Exch {
+    static constexpr int kRow = T + 1;
+    static constexpr int kStride = 16 * (T + 1) + 9;
+};
+
 // Team FFT of size M = 16 T (inverse).  On entry thread t of the team holds
 // u[j] = x[T j + t]; on exit it holds X[k1 + 16 k2] for k1 = t (16/T) + q
-// (q < 16/T), k2 < T, stored as u[q * T + k2].  ex: the team's 16 T exchange
-// slots; tw: W_n table (n = 2M entries; W_M^j = tw[2 j]).
+// (q < 16/T), k2 < T, stored as u[q * T + k2].  ex: the team's exchange slots
+// (Exch<T>); tw: W_n table (n = 2M entries; W_M^j = tw[2 j]).
 template <int T>
 __device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const float2 *tw, unsigned mask) {
+    constexpr int R = Exch<T>::kRow;
     idft16(u);
 #pragma unroll
     for (int k1 = 1; k1 < 16; ++k1) u[k1] = cmul(u[k1], tw[2 * ((t * k1) % (16 * T))]);
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) ex[k1 * T + t] = u[k1];
+    for (int k1 = 0; k1 < 16; ++k1) ex[k1 * R + t] = u[k1];
     __syncwarp(mask);
     constexpr int Q = 16 / T;
 #pragma unroll
@@ -136,7 +145,7 @@ __device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const flo
         const int k1 = t * Q + q;
         float2 w[T];
 #pragma unroll
-        for (int i = 0; i < T; ++i) w[i] = ex[k1 * T + i];
+        for (int i = 0; i < T; ++i) w[i] = ex[k1 * R + i];
         if (T == 2) idft2(w[0], w[1]);
         if (T == 4) idft4(w[0], w[1], w[2], w[3]);
         if (T == 8) idft8(w);
@@ -166,147 +175,107 @@ struct ShellItemsDev {
 
 }  // namespace
 
-// ---------------------------------------------------------------- pass 1
-// One block per (row slot s = n_y + n/4 in [1, n/2), item).  Synthesises the
-// item's columns (all n_x, n_z in band) from the source spectrum, transforms
-// them along x and writes A_item[x][s][n_z].
-template <int T>
-__global__ void __launch_bounds__(128) shell_xpass_kernel(const float2 *__restrict__ A, const float2 *__restrict__ B,
-                                                          int n, double L, EdgeSet edges, HarmTable harm,
-                                                          ShellItemsDev items, float2 *__restrict__ work) {
-    constexpr int M = 16 * T;   // n / 2
-    constexpr int N = 2 * M;    // n
-    constexpr int H = M / 2;    // n / 4: band half-width (slots) and n_z count
-    constexpr int LD = H + 1;   // padded row of n_z values
-    extern __shared__ float4 smem4[];
-    float2 *in = reinterpret_cast<float2 *>(smem4);  // [M slots][LD]
-    float2 *out = in + M * LD;                       // [N x][LD]
-    float2 *tw = out + N * LD;                       // [N] twiddles W_n^j
-    float2 *ex = tw + N;                             // [teams][16 T]
-    double *kt = reinterpret_cast<double *>(ex + (blockDim.x / T) * 16 * T);  // [n + 1] k table
-    const int s = 1 + blockIdx.x / items.n;
-    const int item = blockIdx.x % items.n;
-    const cnpc_shell_item it = items.it[item];
-    const cnpc_harmonic &hm = harm.h[it.harmonic];
+// ------------------------------------------------------------ passes
+// Work layout per item: A[x][s][n_z] (pass 1 output, s = n_y + n/4) and
+// B[x][y][n_z] (pass 2 output); n_z < n/4 throughout.
+constexpr int kColThreads = 128;   // 16 teams of 8 (n = 256)
+constexpr int kKC = 16;            // n_z columns per block in passes 1 and 2
+
+__device__ __forceinline__ void fill_twiddles(float2 *tw, int N) {
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
         double sn, cs;
         sincospi(2.0 * j / N, &sn, &cs);
         tw[j] = make_float2((float)cs, (float)sn);
-    }
-    for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
-    __syncthreads();
-    const int ny = s - H;
-    const int iy = ny < 0 ? ny + n : ny;
-    const int nh2 = n / 2 + 1;
-    // synthesise the (n_x slot, n_z) tile of this row
-    for (int e = threadIdx.x; e < M * H; e += blockDim.x) {
-        const int xs = e / H, nz = e % H;
-        float2 v = make_float2(0.f, 0.f);
-        if (xs > 0) {
-            const int nx = xs - H;
-            const int ix = nx < 0 ? nx + n : nx;
-            const double kx = kt[nx + n / 2], ky = kt[ny + n / 2], kz = kt[nz + n / 2];
-            const double kn = knorm_from(kx, ky, kz);
-            if (find_bin(kn, edges.e, edges.n) == it.bin) {
-                const bool origin = kn == 0.0;
-                const double ik = origin ? 0.0 : 1.0 / kn;
-                float2 Y = harmonic_eval<float>(hm, (float)(kx * ik), (float)(ky * ik), (float)(kz * ik), origin);
-                if (it.conj) Y.y = -Y.y;
-                float2 phi;
-                if ((hm.l & 1) == 0)
-                    phi = it.component == 0 ? make_float2(Y.x, 0.f) : make_float2(Y.y, 0.f);
-                else
-                    phi = it.component == 0 ? make_float2(0.f, Y.y) : make_float2(0.f, -Y.x);
-                float2 src;
-                const int64_t t = ((int64_t)ix * n + iy) * nh2 + nz;
-                if (it.source == 0)
-                    src = A[t];
-                else if (it.source == 1)
-                    src = B[t];
-                else
-                    src = make_float2(1.f, 0.f);
-                v = cmul(src, phi);
-            }
-        }
-        in[xs * LD + nz] = v;
-    }
-    __syncthreads();
-    // inverse DFT along x of each n_z column, both output parities
-    const int team = threadIdx.x / T, t = threadIdx.x % T, nteams = blockDim.x / T;
-    const unsigned mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1)));
-    float2 *tex = ex + team * 16 * T;
-    for (int job = team; job < 2 * H; job += nteams) {
-        const int nz = job >> 1, r = job & 1;
-        float2 u[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int slot = T * j + t;
-            float2 v = in[slot * LD + nz];
-            if (r) v = cmul(v, tw[slot]);
-            u[j] = v;
-        }
-        team_fft<T>(u, t, tex, tw, mask);
-#pragma unroll
-        for (int q = 0; q < 16 / T; ++q)
-#pragma unroll
-            for (int k2 = 0; k2 < T; ++k2) {
-                const int m = team_out_index<T>(t, q, k2);
-                out[(2 * m + r) * LD + nz] = shift_phase(u[q * T + k2], m, r);
-            }
-    }
-    __syncthreads();
-    // A_item[x][s][n_z]
-    float2 *dst = work + (size_t)item * N * M * H;
-    for (int e = threadIdx.x; e < N * H; e += blockDim.x) {
-        const int x = e / H, nz = e % H;
-        dst[((size_t)x * M + s) * H + nz] = out[x * LD + nz];
     }
 }
 
-// ---------------------------------------------------------------- pass 2
-constexpr int kShellThreads = 128;
-// two staged output rows of N = 32 T floats per team of T threads: 64 kShellThreads floats
-constexpr int kStagedFloat2 = 32 * kShellThreads;
-// One block per (x, item): y-transform of the n/4 columns, then the real
-// z-output two rows at a time; writes field[x][y][z].
-template <int T>
-__global__ void __launch_bounds__(kShellThreads) shell_yzpass_kernel(const float2 *__restrict__ work, int nitems,
-                                                           float *const *__restrict__ outs) {
-    constexpr int M = 16 * T;
-    constexpr int N = 2 * M;
-    constexpr int H = M / 2;
-    constexpr int LD = H + 1;
-    // A region: the [M slots][LD] input, later the teams' staged output rows
-    constexpr int ASZ = (M * LD > kStagedFloat2) ? M * LD : kStagedFloat2;
+__device__ __forceinline__ unsigned team_mask(int T) {
+    return (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1)));
+}
+
+// Passes 1 and 2: transform kKC in-band columns along one axis.
+//  SYNTH (pass 1): block (s, chunk, item) synthesises its columns over n_x
+//    from the source spectrum, transforms along x, writes A[x][s][chunk].
+//  !SYNTH (pass 2): block (x, chunk, item) loads A[x][s][chunk] over s,
+//    transforms along y, writes B[x][y][chunk].
+template <int T, bool SYNTH>
+__global__ void __launch_bounds__(kColThreads) shell_column_kernel(
+    const float2 *__restrict__ Aspec, const float2 *__restrict__ Bspec, int n, double L, EdgeSet edges,
+    HarmTable harm, ShellItemsDev items, const float2 *__restrict__ src, float2 *__restrict__ dst) {
+    constexpr int M = 16 * T, N = 2 * M, H = M / 2;
+    constexpr int KC = (kKC < H) ? kKC : H;
+    constexpr int LDC = KC + 1;
+    constexpr int NCH = H / KC;
     extern __shared__ float4 smem4[];
-    float2 *A = reinterpret_cast<float2 *>(smem4);
-    float2 *B = A + ASZ;                            // [N y][LD]
-    float2 *tw = B + N * LD;                        // [N]
-    float2 *ex = tw + N;                            // [teams][16 T]
-    const int x = blockIdx.x / nitems;
+    float2 *in = reinterpret_cast<float2 *>(smem4);  // [M][LDC]
+    float2 *out = in + M * LDC;                      // [N][LDC]
+    float2 *tw = out + N * LDC;                      // [N]
+    float2 *ex = tw + N;                             // [teams][Exch<T>::kStride]
+    double *kt = reinterpret_cast<double *>(ex + (kColThreads / T) * Exch<T>::kStride);  // [n + 1]
+    const int nitems = items.n;
     const int item = blockIdx.x % nitems;
-    for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        double sn, cs;
-        sincospi(2.0 * j / N, &sn, &cs);
-        tw[j] = make_float2((float)cs, (float)sn);
-    }
-    const float2 *src = work + ((size_t)item * N + x) * M * H;
-    for (int e = threadIdx.x; e < M * H; e += blockDim.x) {
-        const int s = e / H, nz = e % H;
-        A[s * LD + nz] = s == 0 ? make_float2(0.f, 0.f) : src[e];
+    const int chunk = (blockIdx.x / nitems) % NCH;
+    const int row = blockIdx.x / (nitems * NCH);  // s - 1 (pass 1) or x (pass 2)
+    const int kz0 = chunk * KC;
+    fill_twiddles(tw, N);
+    if (SYNTH) {
+        for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
+        __syncthreads();
+        const cnpc_shell_item it = items.it[item];
+        const cnpc_harmonic &hm = harm.h[it.harmonic];
+        const int s = row + 1;
+        const int ny = s - H;
+        const int iy = ny < 0 ? ny + n : ny;
+        const int nh2 = n / 2 + 1;
+        for (int e = threadIdx.x; e < M * KC; e += blockDim.x) {
+            const int xs = e / KC, nz = kz0 + e % KC;
+            float2 v = make_float2(0.f, 0.f);
+            if (xs > 0) {
+                const int nx = xs - H;
+                const int ix = nx < 0 ? nx + n : nx;
+                const double kx = kt[nx + n / 2], ky = kt[ny + n / 2], kz = kt[nz + n / 2];
+                const double kn = knorm_from(kx, ky, kz);
+                if (find_bin(kn, edges.e, edges.n) == it.bin) {
+                    const bool origin = kn == 0.0;
+                    const double ik = origin ? 0.0 : 1.0 / kn;
+                    float2 Y = harmonic_eval<float>(hm, (float)(kx * ik), (float)(ky * ik), (float)(kz * ik), origin);
+                    if (it.conj) Y.y = -Y.y;
+                    float2 phi;
+                    if ((hm.l & 1) == 0)
+                        phi = it.component == 0 ? make_float2(Y.x, 0.f) : make_float2(Y.y, 0.f);
+                    else
+                        phi = it.component == 0 ? make_float2(0.f, Y.y) : make_float2(0.f, -Y.x);
+                    const int64_t t = ((int64_t)ix * n + iy) * nh2 + nz;
+                    float2 sv;
+                    if (it.source == 0)
+                        sv = Aspec[t];
+                    else if (it.source == 1)
+                        sv = Bspec[t];
+                    else
+                        sv = make_float2(1.f, 0.f);
+                    v = cmul(sv, phi);
+                }
+            }
+            in[xs * LDC + (nz - kz0)] = v;
+        }
+    } else {
+        const float2 *a = src + ((size_t)item * N + row) * M * H;  // A[x = row]
+        for (int e = threadIdx.x; e < M * KC; e += blockDim.x) {
+            const int sl = e / KC, c = e % KC;
+            in[sl * LDC + c] = sl == 0 ? make_float2(0.f, 0.f) : a[(size_t)sl * H + kz0 + c];
+        }
     }
     __syncthreads();
-    const int team = threadIdx.x / T, t = threadIdx.x % T, nteams = blockDim.x / T;
-    const unsigned mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1)));
-    float2 *tex = ex + team * 16 * T;
-    // y: B[y][n_z]
-    for (int job = team; job < 2 * H; job += nteams) {
-        const int nz = job >> 1, r = job & 1;
+    const int team = threadIdx.x / T, t = threadIdx.x % T, nteams = kColThreads / T;
+    const unsigned mask = team_mask(T);
+    float2 *tex = ex + team * Exch<T>::kStride;
+    for (int job = team; job < 2 * KC; job += nteams) {
+        const int c = job >> 1, r = job & 1;
         float2 u[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int slot = T * j + t;
-            float2 v = A[slot * LD + nz];
+            float2 v = in[slot * LDC + c];
             if (r) v = cmul(v, tw[slot]);
             u[j] = v;
         }
@@ -316,18 +285,87 @@ __global__ void __launch_bounds__(kShellThreads) shell_yzpass_kernel(const float
 #pragma unroll
             for (int k2 = 0; k2 < T; ++k2) {
                 const int m = team_out_index<T>(t, q, k2);
-                B[(2 * m + r) * LD + nz] = shift_phase(u[q * T + k2], m, r);
+                out[(2 * m + r) * LDC + c] = shift_phase(u[q * T + k2], m, r);
             }
     }
     __syncthreads();
-    // z: rows y1 = 2p, y2 = 2p + 1 through one complex transform of
-    // v(k_z) = B1~(k_z) + i B2~(k_z), B~(-k_z) = conj B(k_z), B~(0) = Re B(0)
-    float *rows = reinterpret_cast<float *>(A) + team * 2 * N;  // two staged rows per team
-    float *dst = outs[item] + (size_t)x * N * N;
-    for (int p = team; p < N / 2; p += nteams) {
-        const float2 *b1 = B + (2 * p) * LD, *b2 = B + (2 * p + 1) * LD;
+    float2 *d;
+    size_t stride;
+    if (SYNTH) {  // A[x][s][kz]
+        d = dst + (size_t)item * N * M * H + (size_t)(row + 1) * H + kz0;
+        stride = (size_t)M * H;
+    } else {      // B[x][y][kz]
+        d = dst + ((size_t)item * N + row) * N * H + kz0;
+        stride = H;
+    }
+    for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+        const int p = e / KC, c = e % KC;
+        d[p * stride + c] = out[p * LDC + c];
+    }
+}
+
+// Passes 2+3 fused: block (x, y parity ry, item).  The y transform of the n/4
+// columns of A[x] (read from global memory) yields the rows y = 2m + ry,
+// m < n/2, of B[x] into shared memory; the z pass then turns row pairs
+// (m1, m2) into two real rows of the field through one complex transform of
+// v(k_z) = B1~(k_z) + i B2~(k_z), B~(-k_z) = conj B(k_z), B~(0) = Re B(0).
+// Thread t of a team ends the z pass holding z = 2Q t + c + 32 k2 (c < 2Q)
+// of both rows, written as float4 runs without staging.
+constexpr int kYZThreads = 256;
+
+template <int T> struct YZLayout {
+    static constexpr int M = 16 * T, N = 2 * M, H = M / 2, LD = H + 1;
+    static constexpr int TEAMS = kYZThreads / T;
+    static constexpr int kEx = N;                                    // after the twiddles
+    static constexpr int kB = ((kEx + TEAMS * Exch<T>::kStride + 1) / 2) * 2;
+    static constexpr int kTotal = kB + M * LD;                       // float2
+};
+
+template <int T>
+__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work, int nitems,
+                                                                  float *const *__restrict__ outs) {
+    using YL = YZLayout<T>;
+    constexpr int M = YL::M, N = YL::N, H = YL::H, LD = YL::LD, TEAMS = YL::TEAMS;
+    constexpr int Q = 16 / T;
+    extern __shared__ float4 smem4[];
+    float2 *tw = reinterpret_cast<float2 *>(smem4);
+    float2 *Bh = tw + YL::kB;  // [M][LD]: rows y = 2m + ry
+    const int item = blockIdx.x % nitems;
+    const int ry = (blockIdx.x / nitems) & 1;
+    const int x = blockIdx.x / (2 * nitems);
+    fill_twiddles(tw, N);
+    __syncthreads();
+    const int team = threadIdx.x / T, t = threadIdx.x % T;
+    const unsigned mask = team_mask(T);
+    float2 *tex = tw + YL::kEx + team * Exch<T>::kStride;
+    const float2 *a = work + ((size_t)item * N + x) * M * H;  // A[x][slot][kz]
+    // y: one team per k_z column
+    for (int kz = team; kz < H; kz += TEAMS) {
+        float2 u[16];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int j = 0; j < 16; ++j) {
+            const int slot = T * j + t;
+            float2 v = slot == 0 ? make_float2(0.f, 0.f) : __ldg(a + (size_t)slot * H + kz);
+            if (ry) v = cmul(v, tw[slot]);
+            u[j] = v;
+        }
+        team_fft<T>(u, t, tex, tw, mask);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+#pragma unroll
+            for (int k2 = 0; k2 < T; ++k2) {
+                const int m = team_out_index<T>(t, q, k2);
+                Bh[m * LD + kz] = shift_phase(u[q * T + k2], m, ry);
+            }
+    }
+    __syncthreads();
+    float *fout = outs[item] + (size_t)x * N * N;
+    // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity
+    for (int p = team; p < M / 2; p += TEAMS) {
+        const float2 *b1 = Bh + (2 * p) * LD, *b2 = b1 + LD;
+        float2 res[2][16];
+#pragma unroll
+        for (int rz = 0; rz < 2; ++rz) {
             float2 u[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -340,59 +378,64 @@ __global__ void __launch_bounds__(kShellThreads) shell_yzpass_kernel(const float
                     v = make_float2(b1[-kz].x + b2[-kz].y, b2[-kz].x - b1[-kz].y);
                 else if (kz == 0)
                     v = make_float2(b1[0].x, b2[0].x);
-                if (r) v = cmul(v, tw[slot]);
+                if (rz) v = cmul(v, tw[slot]);
                 u[j] = v;
             }
             team_fft<T>(u, t, tex, tw, mask);
 #pragma unroll
-            for (int q = 0; q < 16 / T; ++q)
-#pragma unroll
-                for (int k2 = 0; k2 < T; ++k2) {
-                    const int m = team_out_index<T>(t, q, k2);
-                    const float2 g = shift_phase(u[q * T + k2], m, r);
-                    rows[2 * m + r] = g.x;
-                    rows[N + 2 * m + r] = g.y;
-                }
+            for (int i = 0; i < 16; ++i) res[rz][i] = u[i];
         }
-        __syncwarp(mask);
-        float4 *d1 = reinterpret_cast<float4 *>(dst + (size_t)(2 * p) * N);
-        const float4 *s4 = reinterpret_cast<const float4 *>(rows);
-        for (int i = t; i < N / 2; i += T) d1[i] = s4[i];  // both rows are contiguous in the field
-        __syncwarp(mask);
+        float *row1 = fout + (size_t)(2 * (2 * p) + ry) * N;      // y = 2 m1 + ry
+        float *row2 = fout + (size_t)(2 * (2 * p + 1) + ry) * N;  // y = 2 m2 + ry
+#pragma unroll
+        for (int k2 = 0; k2 < T; ++k2) {
+            float re[2 * Q], im[2 * Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int rz = 0; rz < 2; ++rz) {
+                    const int m = team_out_index<T>(t, q, k2);
+                    const float2 g = shift_phase(res[rz][q * T + k2], m, rz);
+                    re[2 * q + rz] = g.x;
+                    im[2 * q + rz] = g.y;
+                }
+            const int z0 = 2 * Q * t + 32 * k2;
+#pragma unroll
+            for (int c = 0; c < 2 * Q; c += 4) {
+                *reinterpret_cast<float4 *>(row1 + z0 + c) = make_float4(re[c], re[c + 1], re[c + 2], re[c + 3]);
+                *reinterpret_cast<float4 *>(row2 + z0 + c) = make_float4(im[c], im[c + 1], im[c + 2], im[c + 3]);
+            }
+        }
     }
 }
 
 // ------------------------------------------------------------ dispatch
-static size_t xpass_smem(int T, int threads) {
-    const int M = 16 * T, N = 2 * M, LD = M / 2 + 1;
-    return sizeof(float2) * ((size_t)M * LD + (size_t)N * LD + N + (threads / T) * 16 * T) +
+template <int T> static size_t column_smem() {
+    const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
+    return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride) +
            sizeof(double) * (N + 1);
 }
-static size_t yzpass_smem(int T, int threads) {
-    const int M = 16 * T, N = 2 * M, LD = M / 2 + 1;
-    size_t a = (size_t)M * LD;
-    if ((size_t)kStagedFloat2 > a) a = kStagedFloat2;  // same A region as the kernel
-    return sizeof(float2) * (a + (size_t)N * LD + N + (threads / T) * 16 * T);
-}
+template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLayout<T>::kTotal; }
 
 template <int T>
 static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, const float2 *B, const EdgeSet &es,
-                            const HarmTable &ht, const ShellItemsDev &items, float2 *work, float *const *d_outs,
-                            cudaStream_t s) {
-    const int threads = kShellThreads;
-    const size_t s1 = xpass_smem(T, threads), s2 = yzpass_smem(T, threads);
-    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_xpass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)s1), "shell xpass smem");
+                            const HarmTable &ht, const ShellItemsDev &items, float2 *workA,
+                            float *const *d_outs, cudaStream_t s) {
+    constexpr int M = 16 * T, N = 2 * M, H = M / 2;
+    constexpr int KC = kKC < H ? kKC : H;
+    constexpr int NCH = H / KC;
+    const size_t sc = column_smem<T>(), sr = yz_smem<T>();
+    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T, true>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc), "shell smem");
     if (st) return st;
-    st = check_cuda(ctx, cudaFuncSetAttribute(shell_yzpass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)s2), "shell yzpass smem");
+    st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)sr), "shell smem");
     if (st) return st;
-    const int M = 16 * T;
-    shell_xpass_kernel<T><<<(M - 1) * items.n, threads, s1, s>>>(A, B, n, L, es, ht, items, work);
-    st = check_launch(ctx, "shell_xpass_kernel");
-    if (st) return st;
-    shell_yzpass_kernel<T><<<n * items.n, threads, s2, s>>>(work, items.n, d_outs);
-    return check_launch(ctx, "shell_yzpass_kernel");
+    const int ni = items.n;
+    shell_column_kernel<T, true><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, nullptr,
+                                                                             workA);
+    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, d_outs);
+    return check_launch(ctx, "shell_fields kernels");
 }
 
 }  // namespace cnpc
@@ -437,14 +480,14 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
         items.it[j] = it;
     }
     const int T = n / 32;
-    const size_t per_item = sizeof(float2) * (size_t)n * (n / 2) * (n / 4);
+    const size_t per_item_a = sizeof(float2) * (size_t)n * (n / 2) * (n / 4);  // A[x][s][n_z]
     cudaStream_t s = (cudaStream_t)stream;
     // output pointer table and the pass-1 work array in one workspace
     const size_t ptr_bytes = (sizeof(float *) * nitems + 255) / 256 * 256;
-    st = ensure_buffer(ctx, &ctx->shell_ws, &ctx->shell_ws_bytes, ptr_bytes + per_item * nitems, s);
+    st = ensure_buffer(ctx, &ctx->shell_ws, &ctx->shell_ws_bytes, ptr_bytes + per_item_a * nitems, s);
     if (st) return st;
     float **d_ptrs = static_cast<float **>(ctx->shell_ws);
-    float2 *work = reinterpret_cast<float2 *>(static_cast<char *>(ctx->shell_ws) + ptr_bytes);
+    float2 *workA = reinterpret_cast<float2 *>(static_cast<char *>(ctx->shell_ws) + ptr_bytes);
     std::vector<float *> hp(nitems);
     for (int j = 0; j < nitems; ++j) hp[j] = static_cast<float *>(h_out_fields[j]);
     // pageable source: the copy completes before the call returns
@@ -453,7 +496,7 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
     if (st) return st;
     const float2 *A = static_cast<const float2 *>(d_spec_a);
     const float2 *B = static_cast<const float2 *>(d_spec_b);
-    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, work, d_ptrs, s);
-    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, work, d_ptrs, s);
-    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, work, d_ptrs, s);
+    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
+    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
+    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
 }
