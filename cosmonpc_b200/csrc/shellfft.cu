@@ -19,6 +19,7 @@
 // each: a 16-point DFT in registers, twiddles, one shared-memory exchange and
 // T-point DFTs.  Twiddles come from an FP64-computed table rounded to FP32.
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "bins.cuh"
@@ -171,7 +172,16 @@ __device__ __forceinline__ float2 shift_phase(float2 v, int m, int r) {
 struct ShellItemsDev {
     int n;
     cnpc_shell_item it[CNPC_MAX_ITEMS];
+    // band of the item (with a relative slack of 1e-9 so that FP64 rounding of
+    // |k| never puts a mode outside it): no mode has |n_d| > rmax or
+    // n_y^2 + n_z^2 > r2max
+    int rmax[CNPC_MAX_ITEMS];
+    int r2max[CNPC_MAX_ITEMS];
 };
+
+// Pass 1 writes the (s, chunk) tile of an item only when it can hold a mode of
+// the shell; pass 2 reads exactly those tiles (others are zero).
+__device__ __forceinline__ bool tile_live(int ny, int kz0, int r2max) { return ny * ny + kz0 * kz0 <= r2max; }
 
 }  // namespace
 
@@ -217,6 +227,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     const int chunk = (blockIdx.x / nitems) % NCH;
     const int row = blockIdx.x / (nitems * NCH);  // s - 1 (pass 1) or x (pass 2)
     const int kz0 = chunk * KC;
+    if (SYNTH && !tile_live(row + 1 - H, kz0, items.r2max[item])) return;
     fill_twiddles(tw, N);
     if (SYNTH) {
         for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
@@ -322,7 +333,8 @@ template <int T> struct YZLayout {
 };
 
 template <int T>
-__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work, int nitems,
+__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work,
+                                                                  const int *__restrict__ rmax_of, int nitems,
                                                                   float *const *__restrict__ outs) {
     using YL = YZLayout<T>;
     constexpr int M = YL::M, N = YL::N, H = YL::H, LD = YL::LD, TEAMS = YL::TEAMS;
@@ -339,13 +351,18 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     const unsigned mask = team_mask(T);
     float2 *tex = tw + YL::kEx + team * Exch<T>::kStride;
     const float2 *a = work + ((size_t)item * N + x) * M * H;  // A[x][slot][kz]
+    const int rmax = rmax_of[2 * item], r2max = rmax_of[2 * item + 1];
+    const int K = rmax + 1 < H ? rmax + 1 : H;  // columns k_z >= K are zero
+    constexpr int KC = (kKC < H) ? kKC : H;
     // y: one team per k_z column
-    for (int kz = team; kz < H; kz += TEAMS) {
+    for (int kz = team; kz < K; kz += TEAMS) {
+        const int kz0 = (kz / KC) * KC;
         float2 u[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int slot = T * j + t;
-            float2 v = slot == 0 ? make_float2(0.f, 0.f) : __ldg(a + (size_t)slot * H + kz);
+            float2 v = make_float2(0.f, 0.f);
+            if (slot > 0 && tile_live(slot - H, kz0, r2max)) v = __ldg(a + (size_t)slot * H + kz);
             if (ry) v = cmul(v, tw[slot]);
             u[j] = v;
         }
@@ -360,27 +377,38 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     }
     __syncthreads();
     float *fout = outs[item] + (size_t)x * N * N;
-    // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity
-    for (int p = team; p < M / 2; p += TEAMS) {
+    // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity.  Teams of one warp
+    // take pairs 4 apart, so their rows sit 8 * LD float2 (16 banks) apart.
+    for (int p0 = 0; p0 < M / 2; p0 += TEAMS) {
+        const int p = p0 + ((TEAMS >= 16 && (TEAMS & 15) == 0)
+                                ? ((team & 3) * 4 + ((team >> 2) & 3) + 16 * (team >> 4))
+                                : team);
+        if (p >= M / 2) continue;
         const float2 *b1 = Bh + (2 * p) * LD, *b2 = b1 + LD;
+        float2 v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int slot = T * j + t;
+            const int kz = slot - H;
+            const int ak = kz < 0 ? -kz : kz;
+            float2 w = make_float2(0.f, 0.f);  // slot 0 (k_z = -n/4) and |k_z| >= K are zero
+            if (slot > 0 && ak < K) {
+                const float2 c1 = b1[ak], c2 = b2[ak];
+                if (kz > 0)
+                    w = make_float2(c1.x - c2.y, c1.y + c2.x);
+                else if (kz < 0)
+                    w = make_float2(c1.x + c2.y, c2.x - c1.y);
+                else
+                    w = make_float2(c1.x, c2.x);
+            }
+            v[j] = w;
+        }
         float2 res[2][16];
 #pragma unroll
         for (int rz = 0; rz < 2; ++rz) {
             float2 u[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int slot = T * j + t;
-                const int kz = slot - H;
-                float2 v = make_float2(0.f, 0.f);  // slot 0 is k_z = -n/4, outside the band
-                if (kz > 0)
-                    v = make_float2(b1[kz].x - b2[kz].y, b1[kz].y + b2[kz].x);
-                else if (kz < 0 && slot > 0)
-                    v = make_float2(b1[-kz].x + b2[-kz].y, b2[-kz].x - b1[-kz].y);
-                else if (kz == 0)
-                    v = make_float2(b1[0].x, b2[0].x);
-                if (rz) v = cmul(v, tw[slot]);
-                u[j] = v;
-            }
+            for (int j = 0; j < 16; ++j) u[j] = rz ? cmul(v[j], tw[T * j + t]) : v[j];
             team_fft<T>(u, t, tex, tw, mask);
 #pragma unroll
             for (int i = 0; i < 16; ++i) res[rz][i] = u[i];
@@ -420,7 +448,7 @@ template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLay
 template <int T>
 static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, const float2 *B, const EdgeSet &es,
                             const HarmTable &ht, const ShellItemsDev &items, float2 *workA,
-                            float *const *d_outs, cudaStream_t s) {
+                            float *const *d_outs, const int *d_rmax, cudaStream_t s) {
     constexpr int M = 16 * T, N = 2 * M, H = M / 2;
     constexpr int KC = kKC < H ? kKC : H;
     constexpr int NCH = H / KC;
@@ -434,7 +462,7 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     const int ni = items.n;
     shell_column_kernel<T, true><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, nullptr,
                                                                              workA);
-    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, d_outs);
+    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, d_rmax, ni, d_outs);
     return check_launch(ctx, "shell_fields kernels");
 }
 
@@ -478,25 +506,34 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
         // every mode of the shell must lie in |n_d| < n/4
         CNPC_REQUIRE(ctx, h_edges[it.bin + 1] / kf < n / 4.0, "shell band reaches n/4 (needs k < k_Nyquist / 2)");
         items.it[j] = it;
+        const double rt = h_edges[it.bin + 1] / kf * (1.0 + 1e-9);
+        items.rmax[j] = (int)std::floor(rt);
+        items.r2max[j] = (int)std::floor(rt * rt) + 1;
     }
     const int T = n / 32;
     const size_t per_item_a = sizeof(float2) * (size_t)n * (n / 2) * (n / 4);  // A[x][s][n_z]
     cudaStream_t s = (cudaStream_t)stream;
     // output pointer table and the pass-1 work array in one workspace
-    const size_t ptr_bytes = (sizeof(float *) * nitems + 255) / 256 * 256;
+    const size_t ptr_bytes = (sizeof(float *) * nitems + 2 * sizeof(int) * nitems + 255) / 256 * 256;
     st = ensure_buffer(ctx, &ctx->shell_ws, &ctx->shell_ws_bytes, ptr_bytes + per_item_a * nitems, s);
     if (st) return st;
     float **d_ptrs = static_cast<float **>(ctx->shell_ws);
     float2 *workA = reinterpret_cast<float2 *>(static_cast<char *>(ctx->shell_ws) + ptr_bytes);
-    std::vector<float *> hp(nitems);
-    for (int j = 0; j < nitems; ++j) hp[j] = static_cast<float *>(h_out_fields[j]);
-    // pageable source: the copy completes before the call returns
-    st = check_cuda(ctx, cudaMemcpyAsync(d_ptrs, hp.data(), sizeof(float *) * nitems, cudaMemcpyHostToDevice, s),
+    // output pointers, then the items' rmax (pageable source: copied before the call returns)
+    std::vector<char> table(sizeof(float *) * nitems + 2 * sizeof(int) * nitems);
+    for (int j = 0; j < nitems; ++j) {
+        float *pj = static_cast<float *>(h_out_fields[j]);
+        const int band[2] = {items.rmax[j], items.r2max[j]};
+        std::memcpy(table.data() + sizeof(float *) * j, &pj, sizeof(float *));
+        std::memcpy(table.data() + sizeof(float *) * nitems + 2 * sizeof(int) * j, band, sizeof(band));
+    }
+    st = check_cuda(ctx, cudaMemcpyAsync(d_ptrs, table.data(), table.size(), cudaMemcpyHostToDevice, s),
                     "shell output table");
     if (st) return st;
+    const int *d_rmax = reinterpret_cast<const int *>(reinterpret_cast<char *>(d_ptrs) + sizeof(float *) * nitems);
     const float2 *A = static_cast<const float2 *>(d_spec_a);
     const float2 *B = static_cast<const float2 *>(d_spec_b);
-    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
-    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
-    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, s);
+    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
+    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
+    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
 }
