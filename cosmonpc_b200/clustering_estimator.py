@@ -97,7 +97,7 @@ def _legs_for_s3fft(l1, l2, m1, m2):
     return engine.PairSpec(leg1, "leg", (l2, m2, 2, True))
 
 
-def _plan_blocks(specs, k_bins, n, precision, requested, diagonal):
+def _plan_blocks(specs, k_bins, n, precision, requested, diagonal, free_bytes=None):
     """Bin block size and shell-field capacity for one pair_sums call.
 
     ``requested`` is the reference's block_size (ce:867-879): "full"/None means all
@@ -118,7 +118,7 @@ def _plan_blocks(specs, k_bins, n, precision, requested, diagonal):
     def need(b):
         return union_pb * b if b == k_bins else split_pb * b
 
-    cap = engine.fields_capacity(n, precision, need(bs))
+    cap = engine.fields_capacity(n, precision, need(bs), free_bytes=free_bytes)
     while bs > 1 and need(bs) > cap:
         bs = (bs + 1) // 2
     if need(bs) > cap:
@@ -192,29 +192,27 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         if tracer_type == "abc":
             continue
         key = (L_, sn0)
-        if key not in sn_sums:
-            d = torch.empty(2 * k3_bins, dtype=torch.float64, device=dev)
-            yl0 = angular.harmonic(L_, 0, True) if L_ != 0 else None
-            ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                        float(sn0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d)
+        need_sum = key not in sn_sums
+        need_src = shotnoise_mode in ("fft", "both") and tracer_type != "abb" and sn0 not in src_fields
+        if not (need_sum or need_src):
+            continue
+        # one pass gives the k3-bin sums, the source spectrum and its x = 0 value
+        d = torch.empty(2 * (k3_bins + 1), dtype=torch.float64, device=dev)
+        yl0 = angular.harmonic(L_, 0, True) if (L_ != 0 and need_sum) else None
+        src_spec = torch.empty(spec["a"].shape, dtype=cdt, device=dev) if need_src else None
+        ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
+                    float(sn0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d,
+                    source=src_spec, band=2.0 * k_max if need_src else 0.0)
+        if need_sum:
             sn_sums[key] = engine.HostCopy(d)
-        if shotnoise_mode in ("fft", "both") and tracer_type != "abb" and sn0 not in src_fields:
-            src_spec = torch.empty(spec["a"].shape, dtype=cdt, device=dev)
-            d = torch.empty(2 * k3_bins, dtype=torch.float64, device=dev)
-            ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                        float(sn0) if correlation_mode == "auto" else 0.0, window, None, k3_edge, d,
-                        source=src_spec, band=2.0 * k_max)
+        if need_src:
             fld = torch.empty(n * n * n, dtype=rdt, device=dev)
             ctx.c2r(code, n, 1, src_spec, fld)
             del src_spec
             if precision == "f32":
                 # x = 0 cell added in FP64 (engine.origin_correction)
-                d0 = torch.empty(2, dtype=torch.float64, device=dev)
-                ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                            float(sn0) if correlation_mode == "auto" else 0.0, window, None,
-                            [0.0, 2.0 * k_max], d0)
-                src_origin[sn0] = engine.HostCopy(d0)
-                fld[0] = 0.0
+                src_origin[sn0] = engine.HostCopy(d[2 * k3_bins:])
+                fld.narrow(0, 0, 1).zero_()
             src_fields[sn0] = fld
 
     # ---- signal: G_00 = Re c2r(delta) band-limited to |k| < 2 k_max (the only
@@ -229,7 +227,8 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
             entries.append((len(specs), (m1, m2), tj[ss]))
             specs.append(_legs_for_signal(l1, l2, m1, m2, correlation_mode, tracer_type))
         per_cfg.append(entries)
-    bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal)
+    free_bytes = engine.free_device_bytes()
+    bs, capacity = _plan_blocks(specs, k_bins, n, precision, block_size, diagonal, free_bytes)
     sf = engine.ShellFields(n, L, k_edge, precision, spec["a"], spec.get("b"), capacity=capacity)
     signal = engine.pair_sums([(G, specs)], sf, k_bins, diagonal, bs)[0]
     del sf, G
@@ -248,7 +247,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
     s3fft = {}
     if s3_groups:
         all_sp = [ps for (_, sp) in s3_groups for ps in sp]
-        bsf, capf = _plan_blocks(all_sp, k_bins, n, precision, block_size, diagonal)
+        bsf, capf = _plan_blocks(all_sp, k_bins, n, precision, block_size, diagonal, free_bytes)
         sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
         outs = engine.pair_sums(s3_groups, sfu, k_bins, diagonal, bsf)
         s3fft = {ci: outs[gi] for ci, gi in s3_index.items()}
@@ -274,7 +273,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
             SN0, SN1, SN2, SN3 = 0.0, 0.0, 0.0, 0.0
         else:
             SN0 = cfg_info[ci]
-            dd = sn_sums[(L_, SN0)].get()
+            dd = sn_sums[(L_, SN0)].get()[:2 * k3_bins]
             total_sum = dd[0::2] + 1j * dd[1::2]
             SN1, SN2 = 0.0, 0.0
             if l1 == L_ and l2 == 0:
@@ -320,7 +319,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
                     S = ss_list[ss]
                     if src_origin:
                         v0 = src_origin[cfg_info[ci]].get()
-                        S = S + engine.origin_correction(specs_ci[ss], shell_origin, complex(v0[0], v0[1]),
+                        S = S + engine.origin_correction(specs_ci[ss], shell_origin, complex(v0[0], 0.0),
                                                          k_bins, diagonal)
                     if diagonal:
                         sub = np.zeros(k_bins, dtype="complex128")

@@ -1,6 +1,7 @@
 // Shared pieces of the k-space kernels: edge / harmonic tables passed by
 // value, launch sizing, the warp-aggregated bin accumulator and argument checks.
 #pragma once
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -44,6 +45,43 @@ __device__ inline void warp_bin_add(double *s, int bin, double v) {
         if (lane == leader) atomicAdd(&s[b], x);
         active &= ~same;
     }
+}
+
+// Modes of the half spectrum with every |n_d| <= R (R < n/2): a compact index
+// u over n_x, n_y in [-R, R], n_z in [0, R].  Shell sums only see modes below
+// their last edge, so they iterate over that cube (R = -1: every mode).
+struct BandIter {
+    int n, R;
+    int64_t count;
+    __device__ __forceinline__ Mode mode(int64_t u, int64_t *t) const {
+        if (R < 0) {
+            *t = u;
+            return mode_of(u, n);
+        }
+        const int w = 2 * R + 1, nzc = R + 1;
+        const int iz = (int)(u % nzc);
+        const int64_t r = u / nzc;
+        const int jy = (int)(r % w), jx = (int)(r / w);
+        Mode m;
+        m.nx = jx - R;
+        m.ny = jy - R;
+        m.nz = iz;
+        const int ix = m.nx < 0 ? m.nx + n : m.nx, iy = m.ny < 0 ? m.ny + n : m.ny;
+        *t = ((int64_t)ix * n + iy) * (n / 2 + 1) + iz;
+        m.mult = (iz == 0 || 2 * iz == n) ? 1 : 2;
+        return m;
+    }
+};
+
+inline BandIter band_iter(int n, double boxsize, double e_last) {
+    BandIter b;
+    b.n = n;
+    const double kf = 2.0 * kPi / boxsize;
+    const double r = e_last / kf * (1.0 + 1e-9);
+    b.R = (r < 0.5 * n - 1.0) ? (int)std::floor(r) + 1 : -1;
+    if (b.R >= 0 && 2 * b.R + 1 >= n) b.R = -1;
+    b.count = b.R < 0 ? (int64_t)n * n * (n / 2 + 1) : (int64_t)(2 * b.R + 1) * (2 * b.R + 1) * (b.R + 1);
+    return b;
 }
 
 inline int load_edges(cnpc_ctx *ctx, const double *h_edges, int nedges, EdgeSet *es) {

@@ -46,7 +46,8 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
 
 // ------------------------------------------------------------ mode counts
 __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *counts, double *ksum,
-                                   int64_t nh) {
+                                   BandIter bi) {
+    const int64_t nh = bi.count;
     extern __shared__ double sm[];
     AxisTable ax;
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
@@ -62,7 +63,8 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
         int bin = -1;
         double kn = 0.0, mult = 0.0;
         if (t < nh) {
-            const Mode m = mode_of(t, n);
+            int64_t tt;
+            const Mode m = bi.mode(t, &tt);
             kn = knorm_from(ax.kx(m.nx), ax.kx(m.ny), ax.kx(m.nz));
             bin = find_bin(kn, edges.e, edges.n);
             mult = m.mult;
@@ -86,7 +88,8 @@ struct PoleSet {
 
 template <typename T>
 __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, EdgeSet edges,
-                               PoleSet poles, double *sums, int64_t nh) {
+                               PoleSet poles, double *sums, BandIter bi) {
+    const int64_t nh = bi.count;
     extern __shared__ double sm[];
     AxisTable ax;
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
@@ -102,12 +105,13 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
         int bin = -1;
         double pv = 0.0, mu = 0.0;
         if (t < nh) {
-            const Mode m = mode_of(t, n);
+            int64_t tt;
+            const Mode m = bi.mode(t, &tt);
             const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
             const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, edges.e, edges.n);
             if (bin >= 0) {
-                const cpx_t<T> va = a[t], vb = b[t];
+                const cpx_t<T> va = a[tt], vb = b[tt];
                 pv = m.mult * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
                 if (kn > 0.0)
                     mu = (kx / kn) * poles.los[0] + (ky / kn) * poles.los[1] + (kz / kn) * poles.los[2];
@@ -141,7 +145,9 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
     fill_axis_table(ax, sm, n, L, sn0 != 0.0 ? CNPC_COMP_BKNOISE : CNPC_COMP_NONE, p);
     double *bins = sm + 2 * (n + 1);
     const int nb = edges.n - 1;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) bins[i] = 0.0;
+    // with a source, bins[nb] collects the full-space sum of the source (its x = 0 value)
+    const int nbt = source ? nb + 1 : nb;
+    for (int i = threadIdx.x; i < nbt; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
@@ -149,7 +155,8 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
          base += wstride) {
         const int64_t t = base + lane;
         int bin = -1;
-        double val = 0.0;
+        double val = 0.0, tot = 0.0;
+        bool in_band = false;
         if (t < nh) {
             const Mode m = mode_of(t, n);
             const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
@@ -161,7 +168,12 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                 double pr = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
                 const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
                 if (sn0 != 0.0) pr -= sn0 * (ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz));
-                if (source) source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+                if (source) {
+                    source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+                    // the stored source is Hermitian on |k| < band: mult * Re sums the full space
+                    in_band = keep;
+                    tot = m.mult * (double)(T)pr;
+                }
                 if (bin >= 0) {
                     double y = 1.0;
                     if (use_y) {
@@ -176,9 +188,10 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
             }
         }
         warp_bin_add(bins, bin, val);
+        if (source) warp_bin_add(bins, in_band ? nb : -1, tot);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    for (int i = threadIdx.x; i < nbt; i += blockDim.x)
         if (bins[i] != 0.0) atomicAdd(&sums[2 * i], bins[i]);
 }
 
@@ -277,10 +290,11 @@ int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges
     if (st) return st;
     st = check_cuda(ctx, cudaMemsetAsync(d_ksum, 0, sizeof(double) * nb, s), "memset");
     if (st) return st;
-    const int64_t nh = half_modes(n);
+    const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
+    const int64_t nh = bi.count;
     const int threads = 256;
     kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, (n + 1 + 2 * nb) * sizeof(double), s>>>(
-        n, boxsize, es, d_counts, d_ksum, nh);
+        n, boxsize, es, d_counts, d_ksum, bi);
     return check_launch(ctx, "kbin_counts_kernel");
 }
 
@@ -305,15 +319,16 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     cudaStream_t s = (cudaStream_t)stream;
     st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * nb * npoles, s), "memset");
     if (st) return st;
-    const int64_t nh = half_modes(n);
+    const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
+    const int64_t nh = bi.count;
     const int threads = 256;
     const size_t smem = sizeof(double) * (n + 1 + nb * npoles);
     if (dtype == CNPC_F32)
         pk_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ps, d_sums, nh);
+            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ps, d_sums, bi);
     else
         pk_bins_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ps, d_sums, nh);
+            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ps, d_sums, bi);
     return check_launch(ctx, "pk_bins_kernel");
 }
 
@@ -335,12 +350,13 @@ int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
         CNPC_REQUIRE(ctx, y.l >= 0 && y.l <= 8 && y.m == 0, "Y_L0 harmonic expected");
     }
     const int nb = nedges - 1;
+    const int nbt = d_source ? nb + 1 : nb;
     cudaStream_t s = (cudaStream_t)stream;
-    st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nb, s), "memset");
+    st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nbt, s), "memset");
     if (st) return st;
     const int64_t nh = half_modes(n);
     const int threads = 256;
-    const size_t smem = sizeof(double) * (2 * (n + 1) + nb);
+    const size_t smem = sizeof(double) * (2 * (n + 1) + nbt);
     if (dtype == CNPC_F32)
         sn_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, volume_sq, sn0, window,

@@ -445,7 +445,8 @@ __device__ inline void fill_comp_tables(CompTables &ct, double *smem, int n, dou
 template <typename T>
 __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, int p, unsigned kinds,
                                    double sbr, double sbi, int has_z, cnpc_harmonic zh, int conj_z,
-                                   double weight, EdgeSet edges, double *sums, int64_t nh) {
+                                   double weight, EdgeSet edges, double *sums, BandIter bi) {
+    const int64_t nh = bi.count;
     extern __shared__ double sm[];
     CompTables ct;
     fill_comp_tables(ct, sm, n, L, p, kinds);
@@ -462,14 +463,15 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
         int bin = -1;
         double accr = 0.0, acci = 0.0;
         if (t < nh) {
-            const Mode m = mode_of(t, n);
+            int64_t tt;
+            const Mode m = bi.mode(t, &tt);
             const double kx = ct.k[m.nx + ct.half], ky = ct.k[m.ny + ct.half], kz = ct.k[m.nz + ct.half];
             const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, edges.e, edges.n);
             if (bin >= 0) {
                 double2 uk, um, vk, vm;
-                load_operand<T>(u, t, ct.factor(u.comp, m.nx, m.ny, m.nz), &uk, &um);
-                load_operand<T>(v, t, ct.factor(v.comp, m.nx, m.ny, m.nz), &vk, &vm);
+                load_operand<T>(u, tt, ct.factor(u.comp, m.nx, m.ny, m.nz), &uk, &um);
+                load_operand<T>(v, tt, ct.factor(v.comp, m.nx, m.ny, m.nz), &vk, &vm);
                 const double wsn = sbar ? ct.factor(CNPC_COMP_BKNOISE, m.nx, m.ny, m.nz) : 0.0;
                 double zr = 1.0, zi = 0.0;
                 int parity = 1;
@@ -822,15 +824,16 @@ int cnpc_survey_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window
     cudaStream_t s = (cudaStream_t)stream;
     st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nb, s), "memset");
     if (st) return st;
-    const int64_t nh = half_modes(n);
+    const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
+    const int64_t nh = bi.count;
     const int threads = 256;
     const size_t smem = sizeof(double) * (ntab * (n + 1) + 2 * nb);
     if (dtype == CNPC_F32)
         survey_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, h_z ? 1 : 0, zh, conj_z, weight, es, d_sums, nh);
+            du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, h_z ? 1 : 0, zh, conj_z, weight, es, d_sums, bi);
     else
         survey_bins_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, h_z ? 1 : 0, zh, conj_z, weight, es, d_sums, nh);
+            du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, h_z ? 1 : 0, zh, conj_z, weight, es, d_sums, bi);
     return check_launch(ctx, "survey_bins_kernel");
 }
 

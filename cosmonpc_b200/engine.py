@@ -444,9 +444,29 @@ def origin_correction(ps, origin, src0, k_bins, diagonal):
     return src0 * np.outer(f1, f2)
 
 
-def fields_capacity(n, precision, want, reserve_bytes=0):
-    """How many real n^3 fields fit in the free HBM (leaving headroom)."""
+_DEVICE_BASE = {}
+
+
+def free_device_bytes():
+    """Device memory available to new tensors, without a driver query on the
+    hot path (cudaMemGetInfo can stall behind queued work): the driver's free
+    memory plus torch's reserved pool, measured once per device, minus what
+    torch has allocated since."""
+    dev = torch.cuda.current_device()
+    base = _DEVICE_BASE.get(dev)
+    if base is None:
+        free, _ = torch.cuda.mem_get_info()
+        base = int(free + torch.cuda.memory_reserved()) - int(torch.cuda.memory_allocated())
+        base = (base, int(torch.cuda.memory_allocated()))
+        _DEVICE_BASE[dev] = base
+    avail, alloc0 = base
+    return avail - (int(torch.cuda.memory_allocated()) - alloc0)
+
+
+def fields_capacity(n, precision, want, reserve_bytes=0, free_bytes=None):
+    """How many real n^3 fields fit in the available HBM (leaving headroom).
+    ``free_bytes`` (from :func:`free_device_bytes`) spares the driver query."""
     esz = 4 if precision == "f32" else 8
-    free, _ = torch.cuda.mem_get_info()
+    free = free_device_bytes() if free_bytes is None else int(free_bytes)
     avail = int(free * 0.8) - reserve_bytes
     return max(1, min(int(want), avail // (esz * n ** 3)))

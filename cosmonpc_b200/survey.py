@@ -935,7 +935,7 @@ def _s3_fft_sums(rshot, opn, cfgs, l1, l2, L_, S_arr, k_edge, k_bins, diagonal, 
         ctx.c2r(rshot.code, n, 2, src, fld)
         del src
         if rshot.precision == "f32":
-            fld[:, 0] = 0.0
+            fld[:, 0:1].zero_()
         group = {ss: (fld[0], fld[1], specs[ss]) for (ss, _, _, MM, _) in plan if MM == M}
         sums.update(_complex_pairs(group, sf, k_bins, diagonal, bs))
     shell_origin = None

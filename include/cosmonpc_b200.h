@@ -162,7 +162,9 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
  *   P(k) = V^2 a(k) conj(b(k)) - sn0 * W_bknoise(k)
  *   d_sums[2*bin + {0,1}] = sum_{bin} P(k) * Y_L0(khat)   (complex, FP64)
  * with harmonic h_yl0 (NULL: 1).  If d_source is non-NULL, P(k) (without Y)
- * is also written there, zeroed at |k| >= band_kmax when band_kmax > 0. */
+ * is also written there, zeroed at |k| >= band_kmax when band_kmax > 0, and
+ * d_sums[2*(nedges-1)] receives the full-space sum of that source (its value
+ * at x = 0 after the c2r), so d_sums then holds nedges pairs. */
 int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
                  const void *d_spec_b, double volume_sq, double sn0, int window,
                  const cnpc_harmonic *h_yl0, const double *h_edges, int nedges,
