@@ -33,6 +33,10 @@ WORKLOAD = dict(n_particles=4_000_000, boxsize=2000.0, nmesh=256, sampler="pcs",
                 k_min=0.01, k_max=0.20, k_bins=20, angu_configs=[(0, 0, 0), (2, 0, 2)],
                 data_vector_mode="full", shotnoise_mode="both")
 SMALL = dict(WORKLOAD, n_particles=500_000, nmesh=128, boxsize=1000.0, k_max=0.19, k_bins=12)
+# batched mocks: 3 shape classes, CIC interlaced, pk [0,2,4] + bk (0,0,0) diagonal, 15 bins 0.01-0.16
+MOCK_CLASSES = [(128, 1000.0), (192, 1500.0), (256, 2000.0)]
+MOCKS = dict(n_particles=1_500_000, sampler="cic", interlaced=True, k_min=0.01, k_max=0.16, k_bins=15,
+             poles=(0, 2, 4), angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana")
 METRIC = "bk_sugi 256^3 full-mode s/data-vector"
 UNIT = "s/data-vector"
 
@@ -163,6 +167,58 @@ def cpu_baseline_estimate(workload, seed):
 
 
 # ----------------------------------------------------------------- main
+def _mocks_throughput(per_class, seed, barrier, max_over_ranks):
+    """mocks/s of the fast form (FP32 fields, one paint per mock, the next mock
+    queued before the previous one's results are read) with every mock resident
+    in HBM, and of the plain FP64 per-call path (separate pk and bk calls) on one
+    mock per class."""
+    import torch
+
+    from cosmonpc_b200 import api
+    from cosmonpc_b200.mocks import lognormal_box
+
+    M = MOCKS
+    fast_s, plain_s, total = 0.0, 0.0, 0
+    classes = {}
+    for ci, (n, L) in enumerate(MOCK_CLASSES):
+        cats = [torch.from_numpy(lognormal_box(M["n_particles"], L, seed + 1000 * ci + i)).cuda()
+                for i in range(per_class)]
+        kw = dict(nmesh=n, boxsize=L, sampler=M["sampler"], interlaced=M["interlaced"], k_min=M["k_min"],
+                  k_max=M["k_max"], k_bins=M["k_bins"], poles=M["poles"], angu_configs=M["angu_configs"],
+                  data_vector_mode=M["data_vector_mode"], shotnoise_mode=M["shotnoise_mode"])
+        api.mock_pk_bk(cats[0], None, precision="f32", **kw)  # warm-up: plans and buffers of this class
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pending = None
+        for c in cats:
+            # queue this mock's device work, then read the previous mock's results
+            fin = api.mock_pk_bk(c, None, precision="f32", deferred=True, **kw)
+            if pending is not None:
+                pending()
+            pending = fin
+        pending()
+        e1.record()
+        barrier()
+        tf = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+        api.mock_pk_bk_plain(cats[0], None, **kw)
+        barrier()
+        e0.record()
+        api.mock_pk_bk_plain(cats[0], None, **kw)
+        e1.record()
+        barrier()
+        tp = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+        classes["%d^3/L%d" % (n, L)] = {"fast_s_per_mock": tf / len(cats), "plain_s_per_mock": tp}
+        fast_s += tf
+        plain_s += tp * len(cats)
+        total += len(cats)
+        del cats
+    return {"value": total / fast_s, "unit": "mocks/s", "plain_value": total / plain_s,
+            "speedup": plain_s / fast_s, "mocks": total, "per_class": classes,
+            "workload": "pk [0,2,4] + bk_sugi (0,0,0) diagonal, 15 bins 0.01-0.16, CIC interlaced, "
+                        "lognormal mocks of 1.5e6 particles; classes 128^3/L1000, 192^3/L1500, 256^3/L2000"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +229,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mocks", type=int, default=4, help="mocks per shape class for the mocks/s line (0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -316,6 +373,11 @@ def main():
                     rel_by_key[tag + ":" + key] = e
                     max_rel = max(max_rel, e)
 
+    # ---- batched mocks (pk + bk diagonal per mock, three shape classes)
+    mocks = None
+    if args.mocks > 0:
+        mocks = _mocks_throughput(args.mocks, seed + 100 * rank, barrier, max_over_ranks)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -350,6 +412,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None},
         "kernels": kernels,
+        "mocks": mocks,
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,

@@ -81,3 +81,43 @@ def pk_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max
                       k_min=k_min, k_max=k_max, k_bins=k_bins, sampler=sampler, interlaced=interlaced,
                       poles=list(poles), rsd=list(rsd))
     return ce.calculate_power_spectrum_box(pm, None, "auto", attrs)
+
+
+def mock_pk_bk(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles=(0, 2, 4),
+               angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana", precision="f32",
+               rsd=(0, 0, 1), deferred=False):
+    """Power-spectrum multipoles and bispectrum configurations of one mock from a
+    single paint: the interlaced R2C spectra are finished twice (the power
+    spectrum and the bispectrum overdensity use different scalings and k = 0
+    values).  Returns (pk result dict, [bk result dict per configuration]), or
+    with ``deferred`` a function returning them, after the device work of this
+    mock is queued, so that the next mock can be queued before the results are
+    read."""
+    wsum = _weight_sum(pos, weight)
+    dpos, dw = _to_device(pos, weight)
+    pm = engine.paint(dpos, dw, nmesh, boxsize, sampler, interlaced, precision, sum_w=wsum)
+    pm_bk = engine.PaintedMesh(pm.raw.clone(), pm.n, pm.boxsize, pm.sampler, pm.interlaced, pm.N_gal, pm.sum_w,
+                               pm.precision)
+    common = dict(boxsize=[boxsize] * 3, nmesh=[nmesh] * 3, k_min=k_min, k_max=k_max, k_bins=k_bins,
+                  sampler=sampler, interlaced=interlaced)
+    pk = ce.calculate_power_spectrum_box(pm, None, "auto", box_attrs(dpos.shape[0], wsum, boxsize,
+                                                                      poles=list(poles), rsd=list(rsd), **common),
+                                         deferred=True)
+    attrs = box_attrs(dpos.shape[0], wsum, boxsize, data_vector_mode=data_vector_mode,
+                      shotnoise_mode=shotnoise_mode, **common)
+    bk = ce.bk_sugi_box_submit({"a": pm_bk}, "auto", "aaa", [tuple(c) for c in angu_configs], attrs,
+                               precision=precision, block_size=None)
+    finalize = lambda: (pk(), bk())
+    return finalize if deferred else finalize()
+
+
+def mock_pk_bk_plain(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles=(0, 2, 4),
+                     angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana", rsd=(0, 0, 1)):
+    """The plain FP64 per-call form of :func:`mock_pk_bk`: one power-spectrum and
+    one bispectrum call per mock, each painting its catalog (as separate
+    ``run_stats`` calls do)."""
+    pk = pk_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles, rsd,
+                       precision="f64")
+    bk = bk_sugi_box_plain(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, angu_configs,
+                           data_vector_mode, shotnoise_mode, block_size=None)
+    return pk, bk

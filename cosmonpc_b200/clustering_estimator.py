@@ -46,16 +46,24 @@ def calculate_power_spectrum_box(rfield_a, rfield_b, correlation_mode, stat_attr
     prec = rfield_a.precision
     code = engine.PRECISION[prec][0]
 
-    counts, ksum = engine.kbin_counts(n, L, k_edge)
+    counts = engine.HostCopy(torch.stack(engine.kbin_counts(n, L, k_edge)))
     even = [p for p in poles if not p & 1]
-    sums = None
+    dsum = None
     if even:
         ctx = _lib.Context.get()
         dsum = torch.empty((len(even), k_bins), dtype=torch.float64, device=ca.device)
         ctx.pk_bins(code, n, L, ca, cb, k_edge, even, rsd, dsum)
-        sums = dsum.cpu().numpy()
-    k_num = counts.cpu().numpy()
-    k_eff = ksum.cpu().numpy() / k_num
+        dsum = engine.HostCopy(dsum)
+    finalize = lambda: _pk_box_results(counts, dsum, poles, even, k_bins, correlation_mode, boxsize, nmesh,
+                                       NZ_a, NZ_b, P_shot)
+    return finalize if kwargs.get("deferred") else finalize()
+
+
+def _pk_box_results(counts, dsum, poles, even, k_bins, correlation_mode, boxsize, nmesh, NZ_a, NZ_b, P_shot):
+    c = counts.get()
+    sums = dsum.get() if dsum is not None else None
+    k_num = c[0].copy()
+    k_eff = c[1] / c[0]
     results = {"k_eff": k_eff, "k_num": k_num}
     for pole in poles:
         if pole & 1:
@@ -128,6 +136,13 @@ def _plan_blocks(specs, k_bins, n, precision, requested, diagonal, free_bytes=No
 
 def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_attrs,
                       precision="f64", block_size=None, shotnoise_ana_all_eff=True):
+    """See :func:`bk_sugi_box_submit`; returns the result dicts."""
+    return bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat_attrs, precision,
+                              block_size, shotnoise_ana_all_eff)()
+
+
+def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat_attrs,
+                       precision="f64", block_size=None, shotnoise_ana_all_eff=True):
     """Sugiyama bispectrum multipoles for several angular configurations of one
     set of painted meshes, sharing the forward transforms, G, the shell fields and
     the FFT shot-noise shells among configurations.
@@ -136,7 +151,9 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
     shot-noise shell sums as soon as they are ready (the analytical S3 algebra
     overlaps the remaining GPU work) and the pair sums last.  Returns one
     reference-format result dict per configuration; with a single configuration
-    this is ``calculate_bk_sugi_box``.
+    this is ``calculate_bk_sugi_box``.  Returns a function that waits for the
+    device results and assembles the dicts, so callers can queue the next
+    catalog's work first.
     """
     data_vector_mode = stat_attrs.get("data_vector_mode", "diagonal")
     shotnoise_mode = stat_attrs.get("shotnoise_mode", "ana")
@@ -245,6 +262,7 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
         s3_index[ci] = len(s3_groups)
         s3_groups.append((src_fields[sn0], [_legs_for_s3fft(l1, l2, m1, m2) for (m1, m2, _) in cfgs]))
     s3fft = {}
+    shell_origin = None
     if s3_groups:
         all_sp = [ps for (_, sp) in s3_groups for ps in sp]
         bsf, capf = _plan_blocks(all_sp, k_bins, n, precision, block_size, diagonal, free_bytes)
@@ -256,7 +274,18 @@ def bk_sugi_box_multi(meshes, correlation_mode, tracer_type, angu_configs, stat_
             legs = [ps.leg1 for ps in all_sp] + [ps.leg2 for ps in all_sp if ps.mode == "leg"]
             shell_origin = engine.unit_shell_origin(n, L, k_edge, precision, legs)
 
-    # ---- host algebra while the GPU drains the queue
+    return lambda: _bk_box_results(
+        angu_configs, tracer_type, correlation_mode, diagonal, shotnoise_mode, shotnoise_ana_all_eff, k_bins,
+        k_edge, k3_center, nmesh, V, vol_per_cell, N_gal, counts_k, counts_k3, sn_sums, cfg_info, s3fft,
+        s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg)
+
+
+def _bk_box_results(angu_configs, tracer_type, correlation_mode, diagonal, shotnoise_mode, shotnoise_ana_all_eff,
+                    k_bins, k_edge, k3_center, nmesh, V, vol_per_cell, N_gal, counts_k, counts_k3, sn_sums,
+                    cfg_info, s3fft, s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg):
+    """Host algebra of bk_sugi_box_multi, run once the device work is queued."""
+    k_center = 0.5 * (k_edge[1:] + k_edge[:-1])
+    k3_bins = len(k3_center)
     ck = counts_k.get()
     k_num, k_eff = ck[0].copy(), ck[1] / ck[0]
     c3 = counts_k3.get()

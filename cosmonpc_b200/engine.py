@@ -107,6 +107,11 @@ FIELD_PAD = 0
 FUSED_SHELLS = True
 
 
+# diagonal data vectors contract only their same-bin component pairs
+# (cnpc_contract_pairs) instead of whole Gram blocks
+PAIR_LIST = True
+
+
 def fused_shells_apply(n, boxsize, edges, bins, precision):
     if not FUSED_SHELLS or precision != "f32" or n not in (64, 128, 256):
         return False
@@ -306,11 +311,32 @@ class PairSpec:
         return [sf.key(leg, b, c) for b in bins for c in leg_components(leg[0], leg[1])]
 
 
+def _assemble_entry(ps, t, bi, bj):
+    """Complex S(bi, bj) of one pair spec from real component sums t(k1, k2)."""
+    leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
+    R1, I1 = (ps.leg1, bi, 0), (ps.leg1, bi, 1)
+    R2, I2 = (leg2, bj, 0), (leg2, bj, 1)
+    if ps.mode == "conj":
+        re = t(R1, R2) + t(I1, I2)
+        im = t(I1, R2) - t(R1, I2)
+        return ps.sign * complex(re, im)
+    re = t(R1, R2) - t(I1, I2)
+    im = t(R1, I2) + t(I1, R2)
+    return complex(re, im)
+
+
+def _entry_keys(ps, sf, bi, bj):
+    """The (row key, column key) component pairs _assemble_entry reads."""
+    leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
+    c1 = leg_components(ps.leg1[0], ps.leg1[1])
+    c2 = leg_components(leg2[0], leg2[1])
+    return [(sf.key(ps.leg1, bi, a), sf.key(leg2, bj, b)) for a in c1 for b in c2]
+
+
 def assemble(ps, T, rows, cols, rbins, cbins):
     """Complex S[i, j] over the (rbins x cbins) block from the real Gram T."""
     ri = {k: i for i, k in enumerate(rows)}
     ci = {k: j for j, k in enumerate(cols)}
-    leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
 
     def t(k1, k2):
         i = ri.get(k1)
@@ -321,18 +347,20 @@ def assemble(ps, T, rows, cols, rbins, cbins):
 
     S = np.zeros((len(rbins), len(cbins)), dtype=np.complex128)
     for a, bi in enumerate(rbins):
-        R1, I1 = (ps.leg1, bi, 0), (ps.leg1, bi, 1)
         for c, bj in enumerate(cbins):
-            R2, I2 = (leg2, bj, 0), (leg2, bj, 1)
-            if ps.mode == "conj":
-                re = t(R1, R2) + t(I1, I2)
-                im = t(I1, R2) - t(R1, I2)
-                S[a, c] = ps.sign * complex(re, im)
-            else:
-                re = t(R1, R2) - t(I1, I2)
-                im = t(R1, I2) + t(I1, R2)
-                S[a, c] = complex(re, im)
+            S[a, c] = _assemble_entry(ps, t, bi, bj)
     return S
+
+
+def contract_pairs(G, sf, pairs):
+    """Device tensor v[p] = sum_x G F_a F_b for the (key_a, key_b) pairs (FP64)."""
+    ctx = _lib.Context.get()
+    out = torch.empty(len(pairs), dtype=torch.float64, device=_device())
+    for p0 in range(0, len(pairs), 256):
+        chunk = pairs[p0:p0 + 256]
+        ctx.contract_pairs(sf.code, sf.n ** 3, G, sf.fields, sf.stride, [sf.slot[a] for a, _ in chunk],
+                           [sf.slot[b] for _, b in chunk], out[p0:p0 + len(chunk)])
+    return out
 
 
 class DeferredPairSums:
@@ -348,11 +376,21 @@ class DeferredPairSums:
     def add(self, T, rows, cols, bi, bj):
         self.blocks.append((HostCopy(T), rows, cols, bi, bj))
 
+    def add_pairs(self, vals, pairs, bins):
+        self.blocks.append((HostCopy(vals), pairs, None, bins, None))
+
     def result(self):
         k_bins = self.k_bins
         results = [np.zeros((k_bins, k_bins) if not self.diagonal else k_bins, dtype=np.complex128)
                    for _ in self.pair_specs]
         for hc, rows, cols, bi, bj in self.blocks:
+            if cols is None:  # pair-list sums of the diagonal
+                lookup = dict(zip(rows, hc.get()))
+                t = lambda k1, k2: lookup.get((k1, k2), 0.0)
+                for r, ps in enumerate(self.pair_specs):
+                    for b in bi:
+                        results[r][b] = _assemble_entry(ps, t, b, b)
+                continue
             T = hc.get()
             for r, ps in enumerate(self.pair_specs):
                 S = assemble(ps, T, rows, cols, bi, bj)
@@ -376,6 +414,20 @@ def pair_sums(groups, sf, k_bins, diagonal, block_size):
     outs = [DeferredPairSums(specs, k_bins, diagonal) for (_, specs) in groups]
     bs = k_bins if block_size is None else int(block_size)
     blocks = [list(range(b0, min(k_bins, b0 + bs))) for b0 in range(0, k_bins, bs)]
+    if diagonal and PAIR_LIST:
+        # only the same-bin component pairs are needed: pair-list contraction
+        for bi in blocks:
+            need = []
+            for (_, specs) in groups:
+                for ps in specs:
+                    need += ps.row_keys(sf, bi) + ps.col_keys(sf, bi)
+            sf.release([k for k in list(sf.slot) if k not in set(need)])
+            sf.ensure(need)
+            for gi, (G, specs) in enumerate(groups):
+                pairs = list(dict.fromkeys(kp for ps in specs for b in bi for kp in _entry_keys(ps, sf, b, b)))
+                outs[gi].add_pairs(contract_pairs(G, sf, pairs), pairs, bi)
+            sf.release_all()
+        return outs
     for bi in blocks:
         rows_g = []
         for (_, specs) in groups:

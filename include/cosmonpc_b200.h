@@ -347,6 +347,14 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
                        const int *h_a, int na, const int *h_b, int nb, double *d_out,
                        cnpc_stream_t stream);
 
+/* Pair-list form: d_out[p] = sum_x G(x) F_{h_a[p]}(x) F_{h_b[p]}(x), p < npairs
+ * (<= 256), FP64 result; the diagonal data vector's same-bin pairs
+ * (clustering_estimator.py:998-1061, :1983-2035) without the whole Gram block.
+ * ncell and field_stride multiples of 4; G and fields aligned to 4 elements. */
+int cnpc_contract_pairs(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
+                        const void *d_fields, int64_t field_stride, const int *h_a,
+                        const int *h_b, int npairs, double *d_out, cnpc_stream_t stream);
+
 /* Allocation-free form of cnpc_contract_gram.  It has no counterpart in the
  * reference; it exists for callers that must not have a library allocate
  * device memory, such as an application whose own pool owns the whole device,

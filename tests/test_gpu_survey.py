@@ -2,7 +2,8 @@
 reference's own golden vectors.
 
 Tolerances as for the box: FP64 to 1e-8 of each multipole's max |value|, FP32
-to 1e-5, mode counts bit for bit; stage checks against the oracle at FP64
+to 1e-5 (or 4x the single-precision FFT conditioning of a case, conftest.tol),
+mode counts bit for bit; stage checks against the oracle at FP64
 rounding level.
 """
 import copy
@@ -12,7 +13,7 @@ import numpy as np
 import pytest
 
 from cases import SURVEY_CASES, build_case, flatten_result
-from conftest import GOLDEN, rel_err
+from conftest import GOLDEN, rel_err, tol
 
 pytestmark = pytest.mark.gpu
 
@@ -165,6 +166,6 @@ def test_survey_golden_case(name, precision, tmp_path):
     for k in ("k_num", "nmodes"):
         if k in keys:
             np.testing.assert_array_equal(got[k], gold[k])
-    bad = {k: e for k, e in errs.items() if not e < TOL[precision]}
+    bad = {k: e for k, e in errs.items() if not e < tol(precision, name, k)}
     assert not bad, (bad, errs)
     assert res["nmesh"] == cfg["nmesh"] and "nyquist_freq" in res
