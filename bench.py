@@ -7,7 +7,10 @@ over 0.01-0.20 h/Mpc, angular configurations (0,0,0) and (2,0,2) full 20x20
 ((0,2,2) is their transpose), shot noise "both" (analytical and FFT S3).
 
 value  = seconds per data vector of the fast form (FP32 fields, FP64
-         accumulation, shared transforms) with the catalog resident in HBM.
+         accumulation, shared transforms) with the catalog resident in HBM,
+         over K data vectors computed back to back (each one's device work is
+         enqueued before the previous one's host algebra runs); "serial" is
+         the same with one data vector at a time.
 e2e    = the same through the public in-memory API with the catalog in pinned
          host memory: H2D of positions and D2H of the results every step.
 plain  = the FP64 per-configuration drop-in on the same catalog (reported,
@@ -288,6 +291,17 @@ def main():
     def step_resident():
         return api.bk_sugi_box_vector(pos_dev, None, precision="f32", **common)
 
+    def run_vectors(k, pos):
+        """k data vectors back to back: each one's device work is enqueued
+        before the previous one's host algebra runs (the deferred API)."""
+        prev = None
+        for _ in range(k):
+            f = api.bk_sugi_box_vector(pos, None, precision="f32", deferred=True, **common)
+            if prev is not None:
+                prev()
+            prev = f
+        return prev()
+
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -310,13 +324,22 @@ def main():
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record()
-        for _ in range(args.steps):
-            res_fast = step_resident()
+        res_fast = run_vectors(args.steps, pos_dev)
         ev1.record()
         barrier()
     t_fast = ev0.elapsed_time(ev1) / 1000.0
     launches = (_lib.launch_count - launches0) // args.steps
     t_fast = max_over_ranks(t_fast)
+    # the same data vectors one at a time (host algebra not overlapped)
+    barrier()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        step_resident()
+    s1.record()
+    barrier()
+    t_serial = max_over_ranks(s0.elapsed_time(s1) / 1000.0) / args.steps
     # ---- per-kernel breakdown: a separate pass with every library call
     #      bracketed by CUDA events on the launching stream
     kpass = max(1, min(args.steps, 5))
@@ -335,8 +358,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
-            r = api.bk_sugi_box_vector(pos_pinned.numpy(), None, precision="f32", **common)
+        r = run_vectors(args.steps, pos_pinned.numpy())
         e1.record()
         barrier()
         t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
@@ -407,6 +429,8 @@ def main():
                        (3 * W["k_bins"]) * W["nmesh"] ** 3 * 4 / 1e9),
                    "parallelism": "replicas x%d" % world},
         "e2e": e2e,
+        "serial": {"value": t_serial, "unit": UNIT,
+                   "note": "one data vector at a time, host algebra not overlapped with the next vector"},
         "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),
                       "max_rel_err_fast_vs_plain": max_rel, "rel_err_by_key": rel_by_key},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,

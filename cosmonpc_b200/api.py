@@ -46,17 +46,21 @@ def box_attrs(n_gal, weight_sum, box_length, **settings):
 
 def bk_sugi_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins,
                        angu_configs, data_vector_mode="full", shotnoise_mode="both",
-                       precision="f32", block_size="full"):
+                       precision="f32", block_size="full", deferred=False):
     """Auto bispectrum multipoles of one box catalog for every configuration in
-    ``angu_configs`` (list of (l1, l2, L)); returns a list of result dicts."""
+    ``angu_configs`` (list of (l1, l2, L)); returns a list of result dicts, or
+    with ``deferred`` a function returning them once the device work of this
+    catalog is enqueued (the next catalog's work can then be enqueued before
+    this one's host algebra runs)."""
     wsum = _weight_sum(pos, weight)
     dpos, dw = _to_device(pos, weight)
     pm = engine.paint(dpos, dw, nmesh, boxsize, sampler, interlaced, precision, sum_w=wsum)
     attrs = box_attrs(dpos.shape[0], wsum, boxsize, boxsize=[boxsize] * 3, nmesh=[nmesh] * 3,
                       k_min=k_min, k_max=k_max, k_bins=k_bins, sampler=sampler, interlaced=interlaced,
                       data_vector_mode=data_vector_mode, shotnoise_mode=shotnoise_mode)
-    return ce.bk_sugi_box_multi({"a": pm}, "auto", "aaa", [tuple(c) for c in angu_configs], attrs,
-                                precision=precision, block_size=block_size)
+    finalize = ce.bk_sugi_box_submit({"a": pm}, "auto", "aaa", [tuple(c) for c in angu_configs], attrs,
+                                     precision=precision, block_size=block_size)
+    return finalize if deferred else finalize()
 
 
 def bk_sugi_box_plain(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins,

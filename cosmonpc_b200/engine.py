@@ -334,22 +334,26 @@ def _entry_keys(ps, sf, bi, bj):
 
 
 def assemble(ps, T, rows, cols, rbins, cbins):
-    """Complex S[i, j] over the (rbins x cbins) block from the real Gram T."""
+    """Complex S[i, j] over the (rbins x cbins) block from the real Gram T
+    (_assemble_entry for every entry, by index arrays; a component that is not
+    a row or column of T reads as zero)."""
+    nr, nc = len(rows), len(cols)
     ri = {k: i for i, k in enumerate(rows)}
     ci = {k: j for j, k in enumerate(cols)}
-
-    def t(k1, k2):
-        i = ri.get(k1)
-        j = ci.get(k2)
-        if i is None or j is None:
-            return 0.0
-        return T[i, j]
-
-    S = np.zeros((len(rbins), len(cbins)), dtype=np.complex128)
-    for a, bi in enumerate(rbins):
-        for c, bj in enumerate(cbins):
-            S[a, c] = _assemble_entry(ps, t, bi, bj)
-    return S
+    Tx = np.zeros((nr + 1, nc + 1))
+    Tx[:nr, :nc] = T
+    leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
+    r_re = [ri.get((ps.leg1, b, 0), nr) for b in rbins]
+    r_im = [ri.get((ps.leg1, b, 1), nr) for b in rbins]
+    c_re = [ci.get((leg2, b, 0), nc) for b in cbins]
+    c_im = [ci.get((leg2, b, 1), nc) for b in cbins]
+    rr = Tx[np.ix_(r_re, c_re)]
+    ii = Tx[np.ix_(r_im, c_im)]
+    ir = Tx[np.ix_(r_im, c_re)]
+    ri_ = Tx[np.ix_(r_re, c_im)]
+    if ps.mode == "conj":
+        return ps.sign * ((rr + ii) + 1j * (ir - ri_))
+    return (rr - ii) + 1j * (ri_ + ir)
 
 
 def contract_pairs(G, sf, pairs):

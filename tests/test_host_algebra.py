@@ -94,3 +94,31 @@ def test_vectorised_q_matches_oracle():
             for j in range(4):
                 np.testing.assert_allclose(Q[i, j], O.q_ells_eff(i, j, k_eff, *cfg, k3), atol=1e-13)
         assert np.all(Q[4] == 0) and np.all(Q[:, 4] == 0)
+
+
+@pytest.mark.parametrize("mode,leg1,leg2,sign", [("leg", (2, 1, 0, False), (0, 0, 1, False), 1.0),
+                                                 ("eq", (2, -2, 0, False), None, 1.0),
+                                                 ("conj", (1, 1, 0, True), None, -1.0),
+                                                 ("conj", (2, 0, 0, False), None, 1.0)])
+def test_gram_block_assembly_matches_entrywise(mode, leg1, leg2, sign):
+    """The index-array assembly of a Gram block equals the per-entry rule,
+    with components missing from the block reading as zero."""
+    from cosmonpc_b200 import engine
+
+    class SF:
+        def key(self, leg, b, comp):
+            return (tuple(leg), int(b), int(comp))
+
+    sf = SF()
+    ps = engine.PairSpec(leg1, mode, leg2, sign)
+    rbins, cbins = [1, 2, 4], [0, 2, 3, 5]
+    rows = list(dict.fromkeys(ps.row_keys(sf, rbins)))[:-1]  # one row component absent
+    cols = list(dict.fromkeys(ps.col_keys(sf, cbins)))
+    rng = np.random.default_rng(5)
+    T = rng.standard_normal((len(rows), len(cols)))
+    S = engine.assemble(ps, T, rows, cols, rbins, cbins)
+    ri = {k: i for i, k in enumerate(rows)}
+    ci = {k: j for j, k in enumerate(cols)}
+    t = lambda k1, k2: T[ri[k1], ci[k2]] if k1 in ri and k2 in ci else 0.0
+    ref = np.array([[engine._assemble_entry(ps, t, a, c) for c in cbins] for a in rbins])
+    np.testing.assert_array_equal(S, ref)
