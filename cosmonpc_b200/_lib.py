@@ -29,6 +29,7 @@ EXPORTED = (
     "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
+    "cnpc_contract_gram_tc",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -116,6 +117,7 @@ _SIGS = {
     "cnpc_shell_fields": [_vp, _i, _d, _vp, _vp, _dp, _i, ctypes.POINTER(Harmonic), _i,
                           ctypes.POINTER(ShellItem), _i, ctypes.POINTER(_vp), _vp],
     "cnpc_contract_pairs": [_vp, _i, _i64, _vp, _vp, _i64, _ip, _ip, _i, _vp, _vp],
+    "cnpc_contract_gram_tc": [_vp, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
 }
 
 _lib = None
@@ -158,7 +160,8 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "shell_spectra": 1, "gram": 2, "catalog_decode": 3, "particle_sums": 2,
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
-                    "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3}
+                    "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
+                    "gram_tc": 2}
 launch_count = 0
 
 
@@ -360,6 +363,16 @@ class Context:
         self._check(st, "cnpc_contract_gram")
         _count("gram")
         _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * _esz(dtype))
+
+    def gram_tc(self, ncell, g, fields, stride, a_idx, b_idx, out):
+        a, ap = _iarr(a_idx)
+        b, bp = _iarr(b_idx)
+        e0 = _tstart()
+        st = self.lib.cnpc_contract_gram_tc(self.h, ncell, _ptr(g), _ptr(fields), stride, ap, len(a), bp, len(b),
+                                            _ptr(out), self.stream())
+        self._check(st, "cnpc_contract_gram_tc")
+        _count("gram_tc")
+        _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * 4)
 
     def contract_pairs(self, dtype, ncell, g, fields, stride, a_idx, b_idx, out):
         a, ap = _iarr(a_idx)

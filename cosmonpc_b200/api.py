@@ -16,16 +16,34 @@ from . import clustering_estimator as ce
 from . import engine
 
 
+_COPY_STREAMS = {}
+
+
+def _h2d(host, dev):
+    """Device copy of a host array on a side stream, so that it overlaps the
+    work already queued on the current stream; the current stream waits for
+    the copy before its next launch."""
+    t = torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64))
+    if not t.is_pinned():
+        t = t.pin_memory()
+    cs = _COPY_STREAMS.get(dev.index)
+    if cs is None:
+        cs = _COPY_STREAMS[dev.index] = torch.cuda.Stream(dev)
+    cur = torch.cuda.current_stream(dev)
+    with torch.cuda.stream(cs):
+        d = torch.empty(t.shape, dtype=t.dtype, device=dev)
+        d.copy_(t, non_blocking=True)
+    cur.wait_stream(cs)
+    d.record_stream(cur)
+    return d
+
+
 def _to_device(pos, weight):
     dev = torch.device("cuda", torch.cuda.current_device())
     if isinstance(pos, np.ndarray):
-        tp = torch.from_numpy(np.ascontiguousarray(pos, dtype=np.float64))
-        if not tp.is_pinned():
-            tp = tp.pin_memory()
-        pos = tp.to(dev, non_blocking=True)
+        pos = _h2d(pos, dev)
     if isinstance(weight, np.ndarray):
-        tw = torch.from_numpy(np.ascontiguousarray(weight, dtype=np.float64)).pin_memory()
-        weight = tw.to(dev, non_blocking=True)
+        weight = _h2d(weight, dev)
     return pos, weight
 
 

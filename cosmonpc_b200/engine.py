@@ -107,6 +107,13 @@ FIELD_PAD = 0
 FUSED_SHELLS = True
 
 
+# FP32 Gram blocks on the tensor cores (cnpc_contract_gram_tc, TF32 pairs)
+# instead of the CUDA-core FFMA kernel.  Off by default: at 256^3 with 40 x 20
+# outputs the tcgen05 kernel takes 3.4 ms against 1.0 ms for the FFMA kernel
+# (its MMA stream alone takes 0.75 ms; per-chunk CTA synchronisation and the
+# accumulator folds dominate the rest).
+GRAM_TC = False
+
 # diagonal data vectors contract only their same-bin component pairs
 # (cnpc_contract_pairs) instead of whole Gram blocks
 PAIR_LIST = True
@@ -265,9 +272,11 @@ def contract(G, sf, rows, cols):
                 return True
         return False
 
+    tc = sf.precision == "f32" and GRAM_TC
     if sf.precision == "f32":
-        # one FP32 contraction launch covers at most 48 rows x 24 columns
-        rb, cb = 48, 24
+        # one FP32 contraction launch covers at most 64 rows x 32 columns on the
+        # tensor cores, 48 x 24 on the CUDA cores
+        rb, cb = (64, 32) if tc else (48, 24)
         if len(ridx) <= rb and len(cidx) <= cb:
             blocks = [(0, len(ridx), 0, len(cidx))]
         else:
@@ -280,11 +289,13 @@ def contract(G, sf, rows, cols):
                   for r0 in range(0, len(ridx), 48) for c0 in range(0, len(cidx), 48)]
     for (r0, r1, c0, c1) in blocks:
         rr, cc = ridx[r0:r1], cidx[c0:c1]
+        run = (lambda o: ctx.gram_tc(ncell, G, sf.fields, sf.stride, rr, cc, o)) if tc else \
+            (lambda o: ctx.gram(sf.code, ncell, G, sf.fields, sf.stride, rr, cc, o))
         if (r1 - r0, c1 - c0) == (len(ridx), len(cidx)):
-            ctx.gram(sf.code, ncell, G, sf.fields, sf.stride, rr, cc, T)
+            run(T)
         else:
             out = torch.empty((len(rr), len(cc)), dtype=torch.float64, device=dev)
-            ctx.gram(sf.code, ncell, G, sf.fields, sf.stride, rr, cc, out)
+            run(out)
             T[r0:r1, c0:c1] = out
     return T
 

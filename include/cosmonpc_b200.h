@@ -355,6 +355,16 @@ int cnpc_contract_pairs(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g
                         const void *d_fields, int64_t field_stride, const int *h_a,
                         const int *h_b, int npairs, double *d_out, cnpc_stream_t stream);
 
+/* FP32 Gram contraction on the tensor cores (tcgen05.mma kind::tf32, each FP32
+ * operand split into a TF32 hi/lo pair, hi*hi + hi*lo + lo*hi in FP32 TMEM
+ * accumulators folded into FP64 every 256 cells): d_out[i*nb + j] = sum_x G F_{h_a[i]}
+ * F_{h_b[j]} for na <= 64 rows and nb <= 32 columns.  ncell and field_stride are
+ * multiples of 4; G and fields 16-byte aligned.  Same sums as cnpc_contract_gram
+ * (clustering_estimator.py:911-981, :1983-2035), product error ~2^-22 relative. */
+int cnpc_contract_gram_tc(cnpc_ctx *ctx, int64_t ncell, const float *d_g, const float *d_fields,
+                          int64_t field_stride, const int *h_a, int na, const int *h_b, int nb,
+                          double *d_out, cnpc_stream_t stream);
+
 /* Allocation-free form of cnpc_contract_gram.  It has no counterpart in the
  * reference; it exists for callers that must not have a library allocate
  * device memory, such as an application whose own pool owns the whole device,

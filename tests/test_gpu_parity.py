@@ -186,3 +186,35 @@ def test_pair_contraction_matches_fp64_sums(dtype, n):
     scale = torch.stack([(gl.abs() * fl[i, :ncell].abs() * fl[j, :ncell].abs()).sum() for i, j in zip(a, b)])
     err = ((out - ref).abs() / scale).max().item()
     assert err < (1e-14 if dtype == "f64" else 1e-6), err
+
+
+@pytest.mark.parametrize("ncell,na,nb,shared", [(4096 + 36, 1, 1, False), (32 ** 3, 8, 8, True),
+                                                (64 ** 3, 40, 20, True), (64 ** 3, 64, 32, False),
+                                                (48 ** 3, 24, 20, False), (64 ** 3 + 100, 17, 9, False)])
+def test_tensor_core_gram_matches_fp64(ncell, na, nb, shared):
+    """cnpc_contract_gram_tc (3xTF32 on tcgen05) against FP64 sums of the same
+    FP32 inputs and against the CUDA-core FFMA Gram, with ragged last chunks,
+    padded rows/columns, shared row/column fields and a padded field stride."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    rng = np.random.default_rng(ncell + na + nb)
+    nf = na if shared else na + nb
+    stride = (ncell + 7) // 4 * 4 + 4
+    f = torch.from_numpy(rng.standard_normal((nf, stride)).astype(np.float32)).cuda()
+    g = torch.from_numpy(rng.standard_normal(ncell).astype(np.float32)).cuda()
+    a = list(rng.permutation(nf)[:na])
+    b = [a[(3 * j) % na] for j in range(nb)] if shared else list(range(na, na + nb))
+    ctx = _lib.Context.get()
+    out = torch.empty((na, nb), dtype=torch.float64, device="cuda")
+    ctx.gram_tc(ncell, g, f, stride, a, b, out)
+    fd, gd = f[:, :ncell].double(), g.double()
+    ref = (gd * fd[a]) @ fd[b].T
+    scale = (gd.abs() * fd[a].abs()) @ fd[b].abs().T
+    err = ((out - ref).abs() / scale).max().item()
+    assert err < 2e-6, err
+    if na + nb <= 40:  # the FFMA kernel's staging limit
+        ff = torch.empty_like(out)
+        ctx.gram(_lib.F32, ncell, g, f, stride, a, b, ff)
+        err_ff = ((ff - ref).abs() / scale).max().item()
+        assert err < 4 * err_ff + 1e-7, (err, err_ff)
