@@ -170,14 +170,15 @@ def cpu_baseline_estimate(workload, seed):
 
 
 # ----------------------------------------------------------------- main
-def _mocks_throughput(per_class, seed, barrier, max_over_ranks):
+def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
     """mocks/s of the fast form (FP32 fields, one paint per mock, the next mock
     queued before the previous one's results are read) with every mock resident
     in HBM, and of the plain FP64 per-call path (separate pk and bk calls) on one
-    mock per class."""
+    mock per class.  With N ranks each rank runs its own per_class mocks per
+    class and the rate is the whole job's (N x mocks over the slowest rank)."""
     import torch
 
-    from cosmonpc_b200 import api
+    from cosmonpc_b200 import api, replicas
     from cosmonpc_b200.mocks import lognormal_box
 
     M = MOCKS
@@ -216,7 +217,8 @@ def _mocks_throughput(per_class, seed, barrier, max_over_ranks):
         plain_s += tp * len(cats)
         total += len(cats)
         del cats
-    return {"value": total / fast_s, "unit": "mocks/s", "plain_value": total / plain_s,
+    return {"value": replicas.job_rate(total, fast_s, world), "unit": "mocks/s",
+            "plain_value": replicas.job_rate(total, plain_s, world),
             "speedup": plain_s / fast_s, "mocks": total, "per_class": classes,
             "workload": "pk [0,2,4] + bk_sugi (0,0,0) diagonal, 15 bins 0.01-0.16, CIC interlaced, "
                         "lognormal mocks of 1.5e6 particles; classes 128^3/L1000, 192^3/L1500, 256^3/L2000"}
@@ -276,7 +278,7 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    from cosmonpc_b200 import _lib, api, build
+    from cosmonpc_b200 import _lib, api, build, replicas
     from cosmonpc_b200.mocks import lognormal_box
 
     build.build()
@@ -308,11 +310,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x)
 
     for _ in range(args.warmup):
         step_resident()
@@ -398,7 +396,7 @@ def main():
     # ---- batched mocks (pk + bk diagonal per mock, three shape classes)
     mocks = None
     if args.mocks > 0:
-        mocks = _mocks_throughput(args.mocks, seed + 100 * rank, barrier, max_over_ranks)
+        mocks = _mocks_throughput(args.mocks, seed + 100 * rank, barrier, max_over_ranks, world)
 
     if rank != 0:
         if dist is not None:
