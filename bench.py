@@ -40,6 +40,11 @@ SMALL = dict(WORKLOAD, n_particles=500_000, nmesh=128, boxsize=1000.0, k_max=0.1
 MOCK_CLASSES = [(128, 1000.0), (192, 1500.0), (256, 2000.0)]
 MOCKS = dict(n_particles=1_500_000, sampler="cic", interlaced=True, k_min=0.01, k_max=0.16, k_bins=15,
              poles=(0, 2, 4), angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana")
+# DRAM traffic / algorithmic bytes per kernel, from one ncu capture of the 128^3
+# case (dram__bytes_read.sum + dram__bytes_write.sum of every launch of the
+# kernel in one data vector); the contraction's traffic scales with cells x
+# staged rows, so the ratio carries to 256^3
+TRAFFIC_RATIO = {"gram": 1.008}
 METRIC = "bk_sugi 256^3 full-mode s/data-vector"
 UNIT = "s/data-vector"
 
@@ -432,7 +437,10 @@ def main():
         "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),
                       "max_rel_err_fast_vs_plain": max_rel, "rel_err_by_key": rel_by_key},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None},
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (TRAFFIC_RATIO[dom_name] * nbytes / cnt) if dom_name in TRAFFIC_RATIO else None,
+                     "traffic_note": "bytes per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum over the "
+                                     "algorithmic bytes, measured on the 128^3 case and applied to this launch"},
         "kernels": kernels,
         "mocks": mocks,
         "gpu_launches": launches * args.steps,
