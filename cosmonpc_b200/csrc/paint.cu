@@ -108,9 +108,19 @@ static int launch_paint(cnpc_ctx *ctx, const double *pos, const double *w, int64
 // Particles are counting-sorted by the 16^3-cell tile of their base node
 // floor(g); a block then deposits one tile's particles into a (16+4)^3
 // shared-memory region per mesh (every node a particle of the tile can reach,
-// for both the plain and the +1/2-shifted grid and every window order) with
-// shared atomics, and adds the region to the mesh with one global atomic per
-// node.  Node selection and weights are those of the per-particle kernel.
+// for both the plain and the +1/2-shifted grid and every window order) and
+// adds the region to the mesh with one global atomic per node.  Node
+// selection and weights are those of the per-particle kernel.
+//
+// The region accumulates in 32-bit fixed point (integer shared atomics run
+// about twice as fast as FP32 ones and make the sum order-independent).  The
+// tile's scale 2^e is the finest one that cannot overflow: a node receives at
+// most one deposit from each particle whose first stencil node lies in the
+// (P+1) x (P+1) column window behind it (P+1 covers the shifted grid), so
+// |sum| <= (max window count) x max|mass| x wmax^3 with wmax the largest 1-D
+// weight of the window (e <= 100).  One particle's deposit is then resolved to
+// (max window count) x 2^-31 of itself; a tile whose window count exceeds
+// 4096 (coarser than 2^-19) accumulates in FP32 instead.
 constexpr int kTile = 16;
 constexpr int kRegion = kTile + 4;  // nodes [b - 1, b + 3] of a base node b in the tile
 constexpr int kRegionCells = kRegion * kRegion * kRegion;
@@ -185,11 +195,36 @@ __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double
 __device__ inline void red_shared_add(float *addr, float v) {
     asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "f"(v) : "memory");
 }
+__device__ inline void red_shared_add(int *addr, int v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "r"(v) : "memory");
+}
+
+// Region accumulator: fixed point (scale 2^e) or, for a tile too heavy for
+// 32 bits, FP32 in the same words.
+struct RegionAcc {
+    int *reg;
+    float scale;
+    bool fixed;
+    __device__ inline void add(int idx, float v) const {
+        if (fixed)
+            red_shared_add(reg + idx, __float2int_rn(v * scale));
+        else
+            red_shared_add(reinterpret_cast<float *>(reg) + idx, v);
+    }
+};
+
+// largest 1-D weight of the window: NGP/CIC 1, TSC 3/4, PCS 2/3
+template <int P> __device__ constexpr float window_wmax() { return P <= 2 ? 1.f : (P == 3 ? 0.75f : 0.6666667f); }
+
+// first (unwrapped) stencil node of one axis, as in axis_first
+template <int P> __device__ inline int axis_base(double g) {
+    return (P % 2 == 0) ? (int)floor(g) - (P / 2 - 1) : (int)floor(__dadd_rn(g, 0.5)) - (P - 1) / 2;
+}
 
 // 1-D window of one axis: first (unwrapped) node and the P weights, computed
 // exactly as axis_weights does.
 template <int P> __device__ inline int axis_first(double g, float *w) {
-    const int base = (P % 2 == 0) ? (int)floor(g) - (P / 2 - 1) : (int)floor(__dadd_rn(g, 0.5)) - (P - 1) / 2;
+    const int base = axis_base<P>(g);
 #pragma unroll
     for (int o = 0; o < P; ++o) w[o] = (float)bspline<P>(__dsub_rn((double)(base + o), g));
     return base;
@@ -197,19 +232,20 @@ template <int P> __device__ inline int axis_first(double g, float *w) {
 
 // Deposit into a shared region whose index 0 is the unwrapped node org.
 template <int P>
-__device__ inline void deposit_region(float *reg, const int *org, double gx, double gy, double gz, float mass) {
+__device__ inline void deposit_region(const RegionAcc &acc, const int *org, double gx, double gy, double gz,
+                                      float mass) {
     float wx[P], wy[P], wz[P];
     const int bx = axis_first<P>(gx, wx) - org[0];
     const int by = axis_first<P>(gy, wy) - org[1];
     const int bz = axis_first<P>(gz, wz) - org[2];
-    float *base = reg + (bx * kRegion + by) * kRegion + bz;
+    const int base = (bx * kRegion + by) * kRegion + bz;
 #pragma unroll
     for (int a = 0; a < P; ++a) {
 #pragma unroll
         for (int b = 0; b < P; ++b) {
             const float wab = mass * wx[a] * wy[b];
 #pragma unroll
-            for (int c = 0; c < P; ++c) red_shared_add(base + (a * kRegion + b) * kRegion + c, wab * wz[c]);
+            for (int c = 0; c < P; ++c) acc.add(base + (a * kRegion + b) * kRegion + c, wab * wz[c]);
         }
     }
 }
@@ -225,29 +261,73 @@ __device__ inline int region_origin(double g, int n) {
 template <typename T, int P>
 __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int *__restrict__ offset, int ntiles,
                                   int tpa, int n, T *mesh, T *mesh_shifted) {
-    extern __shared__ float reg[];  // [2][kRegionCells]
+    extern __shared__ int reg[];  // [2][kRegionCells]
+    __shared__ int colc[kRegion * kRegion];
+    __shared__ unsigned s_mbits;
+    __shared__ int s_cmax;
     const int nreg = mesh_shifted ? 2 : 1;
+    const int lane = threadIdx.x & 31;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int p0 = offset[tile], p1 = offset[tile + 1];
         if (p0 == p1) continue;
         __syncthreads();
-        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0.f;
+        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0;
+        for (int i = threadIdx.x; i < kRegion * kRegion; i += blockDim.x) colc[i] = 0;
+        if (threadIdx.x == 0) s_mbits = 0u, s_cmax = 0;
         __syncthreads();
+        // bound of any node's sum: particles per first-node column, max |mass|
+        float mloc = 0.f;
+        for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+            const double4 q = sorted[i];
+            const int fx = axis_base<P>(q.x) - region_origin(q.x, n);
+            const int fy = axis_base<P>(q.y) - region_origin(q.y, n);
+            atomicAdd(&colc[fx * kRegion + fy], 1);
+            mloc = fmaxf(mloc, fabsf((float)q.w));
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) mloc = fmaxf(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
+        if (lane == 0) atomicMax(&s_mbits, __float_as_uint(mloc));  // non-negative floats order as integers
+        __syncthreads();
+        int cm = 0;
+        for (int c = threadIdx.x; c < kRegion * kRegion; c += blockDim.x) {
+            const int x = c / kRegion, y = c % kRegion;
+            int sum = 0;
+            for (int dx = 0; dx <= P && dx <= x; ++dx)
+                for (int dy = 0; dy <= P && dy <= y; ++dy) sum += colc[(x - dx) * kRegion + (y - dy)];
+            cm = max(cm, sum);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) cm = max(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+        if (lane == 0) atomicMax(&s_cmax, cm);
+        __syncthreads();
+        constexpr float wa = window_wmax<P>();
+        // (1 + 2^-20): FP32 products of rounded weights may exceed wmax^3 by a few ulps
+        const double bound =
+            (double)s_cmax * (double)__uint_as_float(s_mbits) * (double)(wa * wa * wa) * (1.0 + 0x1p-20);
+        // rounding adds at most 1/2 per deposit, one deposit per particle of the window
+        const double room = 2147483647.0 - (double)s_cmax;
+        int e = 100;
+        if (bound > 0.0) e = min(100, ilogb(room / bound));
+        RegionAcc acc{reg, ldexpf(1.f, e), s_cmax <= 4096};
         for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
             const double4 q = sorted[i];
             int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};
-            deposit_region<P>(reg, org, q.x, q.y, q.z, (float)q.w);
-            if (mesh_shifted)
-                deposit_region<P>(reg + kRegionCells, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5),
-                                  __dadd_rn(q.z, 0.5), (float)q.w);
+            deposit_region<P>(acc, org, q.x, q.y, q.z, (float)q.w);
+            if (mesh_shifted) {
+                const RegionAcc acc2{reg + kRegionCells, acc.scale, acc.fixed};
+                deposit_region<P>(acc2, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5), __dadd_rn(q.z, 0.5),
+                                  (float)q.w);
+            }
         }
         __syncthreads();
+        const double unscale = ldexp(1.0, -e);
         // wrapped origin of the region: tile origin - 1
         const int tz = tile % tpa, ty = (tile / tpa) % tpa, tx = tile / (tpa * tpa);
         const int ox = tx * kTile - 1, oy = ty * kTile - 1, oz = tz * kTile - 1;
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
-            const float v = reg[i];
-            if (v == 0.f) continue;
+            const int word = reg[i];
+            if (word == 0) continue;
+            const float v = acc.fixed ? (float)((double)word * unscale) : __int_as_float(word);
             const int r = i % kRegionCells;
             const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
             const size_t cell = ((size_t)wrapi(ox + rx, n) * n + wrapi(oy + ry, n)) * n + wrapi(oz + rz, n);
@@ -283,7 +363,7 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
     tile_scatter_kernel<<<pblocks, threads, 0, s>>>(pos, w, np, scale, tile_of, cursor, sorted);
     st = check_launch(ctx, "tile sort");
     if (st) return st;
-    const size_t smem = sizeof(float) * kRegionCells * (m2 ? 2 : 1);
+    const size_t smem = sizeof(int) * kRegionCells * (m2 ? 2 : 1);
     const int tblocks = (int)std::min<int64_t>(nt, (int64_t)ctx->num_sms * 8);
     switch (window) {
 #define CNPC_TP(P_)                                                                                        \

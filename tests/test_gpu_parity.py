@@ -218,3 +218,36 @@ def test_tensor_core_gram_matches_fp64(ncell, na, nb, shared):
         ctx.gram(_lib.F32, ncell, g, f, stride, a, b, ff)
         err_ff = ((ff - ref).abs() / scale).max().item()
         assert err < 4 * err_ff + 1e-7, (err, err_ff)
+
+
+@pytest.mark.parametrize("case", ["clustered", "heavy_one_tile", "light_weights"])
+def test_tiled_paint_fixed_point_scales(case):
+    """The tiled FP32 paint's per-tile fixed-point scale: a clustered catalog,
+    one tile holding every particle with weights 1e3 (window counts above 4096:
+    FP32 region), and weights of 1e-9 (scale 2^60 and more), against the FP64
+    oracle paint."""
+    import torch
+    from cosmonpc_b200 import _lib
+    from oracle.pmesh_lite import paint_mass
+
+    n, L, window = 64, 640.0, 4
+    rng = np.random.default_rng(len(case))
+    if case == "clustered":
+        centres = rng.random((40, 3)) * L
+        pos = (centres[rng.integers(0, 40, 120000)] + rng.normal(0, 6.0, (120000, 3))) % L
+        w = 0.5 + rng.random(len(pos))
+    elif case == "heavy_one_tile":
+        pos = 100.0 + rng.random((60000, 3)) * 150.0  # inside one 16^3-cell tile (cells 10..25)
+        w = 1e3 * (0.5 + rng.random(len(pos)))
+    else:
+        pos = rng.random((60000, 3)) * L
+        w = 1e-9 * (0.5 + rng.random(len(pos)))
+    ctx = _lib.Context.get()
+    mesh = torch.empty((2, n, n, n), dtype=torch.float32, device="cuda")
+    ctx.paint(_lib.F32, torch.from_numpy(pos).cuda(), torch.from_numpy(w).cuda(), n, L, window, mesh[0], mesh[1])
+    g = pos * (n / L)
+    for k, shift in enumerate((0.0, 0.5)):
+        ref = paint_mass(g + shift, w, [n] * 3, window)
+        got = mesh[k].double().cpu().numpy()
+        assert np.max(np.abs(got - ref)) < 2e-6 * np.max(ref), (case, k)
+        assert abs(got.sum() - w.sum()) < 1e-6 * w.sum()
