@@ -29,7 +29,7 @@ EXPORTED = (
     "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
-    "cnpc_contract_gram_tc",
+    "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -118,6 +118,8 @@ _SIGS = {
                           ctypes.POINTER(ShellItem), _i, ctypes.POINTER(_vp), _vp],
     "cnpc_contract_pairs": [_vp, _i, _i64, _vp, _vp, _i64, _ip, _ip, _i, _vp, _vp],
     "cnpc_contract_gram_tc": [_vp, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
+    "cnpc_contract_gram_multi_g": [_vp, _i64, ctypes.POINTER(_vp), _i, _vp, _i64, _ip, _ip, _i, _ip, _i, _vp,
+                                   _vp],
 }
 
 _lib = None
@@ -161,7 +163,7 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
                     "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
-                    "gram_tc": 2}
+                    "gram_tc": 2, "gram_multi_g": 2}
 launch_count = 0
 
 
@@ -373,6 +375,19 @@ class Context:
         self._check(st, "cnpc_contract_gram_tc")
         _count("gram_tc")
         _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * 4)
+
+    def gram_multi_g(self, ncell, gs, fields, stride, a_idx, a_g, b_idx, out):
+        """FP32 Gram whose row i is weighted by gs[a_g[i]] (one launch)."""
+        a, ap = _iarr(a_idx)
+        ag, agp = _iarr(a_g)
+        b, bp = _iarr(b_idx)
+        garr = (_vp * len(gs))(*[_ptr(t) for t in gs])
+        e0 = _tstart()
+        st = self.lib.cnpc_contract_gram_multi_g(self.h, ncell, garr, len(gs), _ptr(fields), stride, ap, agp, len(a),
+                                                 bp, len(b), _ptr(out), self.stream())
+        self._check(st, "cnpc_contract_gram_multi_g")
+        _count("gram_multi_g")
+        _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + len(gs)) * ncell * 4)
 
     def contract_pairs(self, dtype, ncell, g, fields, stride, a_idx, b_idx, out):
         a, ap = _iarr(a_idx)

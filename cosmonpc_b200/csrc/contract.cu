@@ -295,10 +295,17 @@ template <int N> __device__ inline void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int RB, int CB, int NBUF>
+// Several weight fields in one launch (MG): staged rows [G_0 .. G_{k-1}][A][B],
+// window row i multiplied by G_{grow[i]}; union_field -2 - j names G_j.
+struct FfMulti {
+    const float *g[4];
+    int grow[48];
+};
+
+template <int RB, int CB, int NBUF, bool MG>
 __global__ void __launch_bounds__(kFfWarps * 32, 2)
     gram_ffma_kernel(const float *__restrict__ g, const float *__restrict__ fields, const GramParams P,
-                     double *partial) {
+                     const FfMulti X, double *partial) {
     constexpr int WR = 8 * RB, WC = 4 * CB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -319,8 +326,9 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
             if (f == -1) continue;  // padding row: only feeds discarded outputs
             const int64_t cell = c0 + part * 4;
             float *d = dst + row * kFfRow + part * 4;
+            const float *src = f >= 0 ? fields + (int64_t)f * P.field_stride : (MG ? X.g[-2 - f] : g);
             if (cell < P.ncell)  // ncell is a multiple of 4, so the 16 bytes are all valid
-                cp_async16(d, (f == -2 ? g : fields + (int64_t)f * P.field_stride) + cell);
+                cp_async16(d, src + cell);
             else
                 *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -330,6 +338,9 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
     const int gl = lane >> 2, hl = lane & 3;
     const int a_row = P.a_slot[0] + gl;  // rows a_row + 8 r
     const int b_row = P.b_slot[0] + hl;  // rows b_row + 4 q
+    int gofs[RB];                        // staged G row of each window row (MG)
+#pragma unroll
+    for (int r = 0; r < RB; ++r) gofs[r] = (MG ? X.grow[gl + 8 * r] : P.g_row) * kFfRow;
     // FP32 partials are folded every kFfFold chunks into this warp's own FP64
     // partial in global memory (L2 resident), keeping registers for the tile
     double *dst = partial + ((int64_t)blockIdx.x * kFfWarps + warp) * (WR * WC);
@@ -372,7 +383,8 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
             float2 a2[RB], b2[CB];
 #pragma unroll
             for (int r = 0; r < RB; ++r)
-                a2[r] = __fmul2_rn(g2, *reinterpret_cast<const float2 *>(ra + 8 * r * kFfRow + c));
+                a2[r] = __fmul2_rn(MG ? *reinterpret_cast<const float2 *>(sb + gofs[r] + c) : g2,
+                                   *reinterpret_cast<const float2 *>(ra + 8 * r * kFfRow + c));
 #pragma unroll
             for (int q = 0; q < CB; ++q) b2[q] = *reinterpret_cast<const float2 *>(rb + 4 * q * kFfRow + c);
 #pragma unroll
@@ -408,7 +420,8 @@ struct FfPlan {
     size_t smem;
 };
 
-static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const int *b, int nb, FfPlan *pl) {
+static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const int *b, int nb, FfPlan *pl,
+                    int ngs = 1) {
     GramParams &P = pl->P;
     std::memset(&P, 0, sizeof(P));
     pl->RB = (na + 7) / 8;
@@ -427,16 +440,16 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
         if (same && off + pl->wc <= pl->wr) b_off = off;
     }
     std::vector<int> rows;
-    rows.push_back(-2);
+    for (int j = 0; j < ngs; ++j) rows.push_back(-2 - j);  // weight fields G_j
     for (int i = 0; i < pl->wr; ++i) rows.push_back(i < na ? a[i] : -1);
-    const int b_base = b_off >= 0 ? 1 + b_off : (int)rows.size();
+    const int b_base = b_off >= 0 ? ngs + b_off : (int)rows.size();
     if (b_off < 0)
         for (int j = 0; j < pl->wc; ++j) rows.push_back(j < nb ? b[j] : -1);
     if ((int)rows.size() > kMaxUnion) return false;
     P.nunion = (int)rows.size();
     for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
     P.g_row = 0;
-    P.a_slot[0] = 1;
+    P.a_slot[0] = ngs;
     P.b_slot[0] = b_base;
     P.ncell = ncell;
     P.field_stride = stride;
@@ -447,27 +460,28 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
     return pl->nbuf >= 2;
 }
 
-template <int R_, int C_>
-static cudaError_t ff_launch_rc(const FfPlan &pl, int nblocks, const float *g, const float *fields, double *part,
-                                cudaStream_t s) {
+template <int R_, int C_, bool MG>
+static cudaError_t ff_launch_rc(const FfPlan &pl, int nblocks, const float *g, const float *fields,
+                                const FfMulti &X, double *part, cudaStream_t s) {
     cudaError_t e;
-#define CNPC_FF_NB(NB_)                                                                                       \
-    if (pl.nbuf == NB_) {                                                                                     \
-        e = cudaFuncSetAttribute(gram_ffma_kernel<R_, C_, NB_>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                 (int)pl.smem);                                                               \
-        if (e != cudaSuccess) return e;                                                                       \
-        gram_ffma_kernel<R_, C_, NB_><<<nblocks, kFfWarps * 32, pl.smem, s>>>(g, fields, pl.P, part);         \
-        return cudaGetLastError();                                                                            \
+#define CNPC_FF_NB(NB_)                                                                                          \
+    if (pl.nbuf == NB_) {                                                                                        \
+        e = cudaFuncSetAttribute(gram_ffma_kernel<R_, C_, NB_, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)pl.smem);                                                                  \
+        if (e != cudaSuccess) return e;                                                                          \
+        gram_ffma_kernel<R_, C_, NB_, MG><<<nblocks, kFfWarps * 32, pl.smem, s>>>(g, fields, pl.P, X, part);     \
+        return cudaGetLastError();                                                                               \
     }
     CNPC_FF_NB(2) CNPC_FF_NB(3) CNPC_FF_NB(4)
 #undef CNPC_FF_NB
     return cudaErrorInvalidValue;
 }
 
-static cudaError_t ff_launch(const FfPlan &pl, int nblocks, const float *g, const float *fields, double *part,
-                             cudaStream_t s) {
+template <bool MG>
+static cudaError_t ff_launch(const FfPlan &pl, int nblocks, const float *g, const float *fields, const FfMulti &X,
+                             double *part, cudaStream_t s) {
 #define CNPC_FF_CASE(R_, C_) \
-    if (pl.RB == R_ && pl.CB == C_) return ff_launch_rc<R_, C_>(pl, nblocks, g, fields, part, s);
+    if (pl.RB == R_ && pl.CB == C_) return ff_launch_rc<R_, C_, MG>(pl, nblocks, g, fields, X, part, s);
 #define CNPC_FF_ROW(R_) \
     CNPC_FF_CASE(R_, 1) CNPC_FF_CASE(R_, 2) CNPC_FF_CASE(R_, 3) CNPC_FF_CASE(R_, 4) CNPC_FF_CASE(R_, 5) CNPC_FF_CASE(R_, 6)
     CNPC_FF_ROW(1) CNPC_FF_ROW(2) CNPC_FF_ROW(3) CNPC_FF_ROW(4) CNPC_FF_ROW(5) CNPC_FF_ROW(6)
@@ -490,7 +504,38 @@ static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const flo
     int st = ensure_scratch(ctx, (size_t)nparts * pl.wr * pl.wc * sizeof(double) + 256, s);
     if (st) return st;
     double *part = (double *)ctx->scratch;
-    st = check_cuda(ctx, ff_launch(pl, nblocks, g, fields, part, s), "gram_ffma_kernel");
+    FfMulti X;
+    std::memset(&X, 0, sizeof(X));
+    st = check_cuda(ctx, ff_launch<false>(pl, nblocks, g, fields, X, part, s), "gram_ffma_kernel");
+    if (st) return st;
+    const int nout = na * nb;
+    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
+    return check_launch(ctx, "gram_window_reduce_kernel");
+}
+
+// Several weight fields in one FP32 launch: out[i, j] = sum_x G_{ag[i]} F_{a_i} F_{b_j}.
+static int run_gram_ffma_mg(cnpc_ctx *ctx, int64_t ncell, const float *const *gs, int ngs, const float *fields,
+                            int64_t stride, const int *a, const int *ag, int na, const int *b, int nb, double *out,
+                            cudaStream_t s) {
+    CNPC_REQUIRE(ctx, ((stride * sizeof(float)) % 16 == 0) && (ncell % 4 == 0) && ((uintptr_t)fields % 16 == 0),
+                 "contraction needs 16-byte aligned fields, field_stride and ncell");
+    FfPlan pl;
+    CNPC_REQUIRE(ctx, ff_plan(ncell, stride, a, na, b, nb, &pl, ngs),
+                 "FP32 multi-weight Gram launch covers at most 48 x 24 outputs");
+    FfMulti X;
+    std::memset(&X, 0, sizeof(X));
+    for (int j = 0; j < ngs; ++j) {
+        CNPC_REQUIRE(ctx, gs[j] != nullptr && (uintptr_t)gs[j] % 16 == 0, "weight fields must be 16-byte aligned");
+        X.g[j] = gs[j];
+    }
+    for (int i = 0; i < na; ++i) X.grow[i] = ag[i];
+    const int64_t nchunks = (ncell + kFfChunk - 1) / kFfChunk;
+    const int nblocks = (int)std::min<int64_t>(2 * ctx->num_sms, nchunks);
+    const int nparts = nblocks * kFfWarps;
+    int st = ensure_scratch(ctx, (size_t)nparts * pl.wr * pl.wc * sizeof(double) + 256, s);
+    if (st) return st;
+    double *part = (double *)ctx->scratch;
+    st = check_cuda(ctx, ff_launch<true>(pl, nblocks, gs[0], fields, X, part, s), "gram_ffma_kernel");
     if (st) return st;
     const int nout = na * nb;
     gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
@@ -626,6 +671,23 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
                             h_a, na, h_b, nb, d_out, s);
 }
 
+int cnpc_contract_gram_multi_g(cnpc_ctx *ctx, int64_t ncell, const float *const *h_gs, int ngs,
+                               const float *d_fields, int64_t field_stride, const int *h_a, const int *h_ag,
+                               int na, const int *h_b, int nb, double *d_out, cnpc_stream_t stream) {
+    int st = check_contract(ctx, CNPC_F32, ncell, h_gs ? h_gs[0] : nullptr, d_fields, field_stride);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, h_a && h_ag && h_b && d_out, "null argument");
+    CNPC_REQUIRE(ctx, ngs >= 1 && ngs <= 4, "ngs must be 1..4");
+    CNPC_REQUIRE(ctx, na >= 1 && na <= 48 && nb >= 1 && nb <= 24, "multi-weight Gram covers 1..48 x 1..24 outputs");
+    for (int i = 0; i < na; ++i) {
+        CNPC_REQUIRE(ctx, h_a[i] >= 0, "negative field index");
+        CNPC_REQUIRE(ctx, h_ag[i] >= 0 && h_ag[i] < ngs, "row weight index out of range");
+    }
+    for (int j = 0; j < nb; ++j) CNPC_REQUIRE(ctx, h_b[j] >= 0, "negative field index");
+    return run_gram_ffma_mg(ctx, ncell, h_gs, ngs, d_fields, field_stride, h_a, h_ag, na, h_b, nb, d_out,
+                            (cudaStream_t)stream);
+}
+
 }  // extern "C"
 
 // ===========================================================================
@@ -701,7 +763,9 @@ static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, 
     const int nblocks =
         (int)std::min<int64_t>(std::min<int64_t>(2 * sms, nchunks), kNoAllocStatusSlot / per_block);
     if (nblocks < 1) return CNPC_EINVAL;
-    st = noalloc_cuda(ff_launch(pl, nblocks, g, fields, scratch, s));
+    FfMulti X;
+    std::memset(&X, 0, sizeof(X));
+    st = noalloc_cuda(ff_launch<false>(pl, nblocks, g, fields, X, scratch, s));
     if (st) return st;
     const int nout = na * nb;
     gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na, nb,

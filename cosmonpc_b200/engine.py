@@ -114,6 +114,10 @@ FUSED_SHELLS = True
 # accumulator folds dominate the rest).
 GRAM_TC = False
 
+# FP32 Gram blocks of several weight fields (the FFT S3 sums of several
+# configurations) with the same columns share one launch
+GRAM_MULTI = True
+
 # diagonal data vectors contract only their same-bin component pairs
 # (cnpc_contract_pairs) instead of whole Gram blocks
 PAIR_LIST = True
@@ -461,10 +465,67 @@ def pair_sums(groups, sf, k_bins, diagonal, block_size):
             keep = set().union(*rows_g, *cols_g)
             sf.release([k for k in list(sf.slot) if k not in keep])
             sf.ensure([k for r in rows_g for k in r] + [k for c in cols_g for k in c])
-            for gi, (G, _) in enumerate(groups):
-                outs[gi].add(contract(G, sf, rows_g[gi], cols_g[gi]), rows_g[gi], cols_g[gi], bi, bj)
+            for idxs in _launch_groups(sf, rows_g, cols_g):
+                if len(idxs) == 1:
+                    gi = idxs[0]
+                    outs[gi].add(contract(groups[gi][0], sf, rows_g[gi], cols_g[gi]), rows_g[gi], cols_g[gi], bi, bj)
+                    continue
+                Ts = contract_multi([groups[gi][0] for gi in idxs], sf, [rows_g[gi] for gi in idxs],
+                                    cols_g[idxs[0]])
+                for gi, T in zip(idxs, Ts):
+                    outs[gi].add(T, rows_g[gi], cols_g[gi], bi, bj)
         sf.release_all()
     return outs
+
+
+def _launch_groups(sf, rows_g, cols_g):
+    """Groups (weight fields) contracted together: FP32 groups with the same
+    columns share one multi-weight launch while rows <= 48, columns <= 24 and
+    at most 4 weights; the rest get a launch each."""
+    plan = []
+    if sf.precision != "f32" or not GRAM_MULTI or GRAM_TC:
+        return [[gi] for gi in range(len(rows_g))]
+
+    def fits(members):
+        # the FFMA launch stages G_0..G_k-1, the padded row window and, unless
+        # the columns are a run of the rows inside it, the padded column window;
+        # two slab buffers per warp must fit (<= 48 staged rows)
+        ridx = [sf.slot[k] for j in members for k in rows_g[j]]
+        cidx = [sf.slot[k] for k in cols_g[members[0]]]
+        wr, wc = -(-len(ridx) // 8) * 8, -(-len(cidx) // 4) * 4
+        shared = any(ridx[o:o + len(cidx)] == cidx and o + wc <= wr for o in range(len(ridx) - len(cidx) + 1))
+        return (len(ridx) <= 48 and len(cidx) <= 24 and len(members) <= 4
+                and len(members) + wr + (0 if shared else wc) <= 48)
+
+    open_by_cols = {}
+    for gi, (rows, cols) in enumerate(zip(rows_g, cols_g)):
+        key = tuple(cols)
+        cur = open_by_cols.get(key)
+        if cur is not None and rows and cols and fits(cur + [gi]):
+            cur.append(gi)
+            continue
+        cur = [gi]
+        plan.append(cur)
+        open_by_cols[key] = cur
+    return plan
+
+
+def contract_multi(Gs, sf, rows_list, cols):
+    """[T_g] with T_g[i, j] = sum_x G_g F_rows_g[i] F_cols[j] (FP64) for FP32
+    fields, in one launch (cnpc_contract_gram_multi_g)."""
+    ctx = _lib.Context.get()
+    ridx, ag = [], []
+    for g, rows in enumerate(rows_list):
+        ridx += [sf.slot[k] for k in rows]
+        ag += [g] * len(rows)
+    cidx = [sf.slot[k] for k in cols]
+    T = torch.empty((len(ridx), len(cidx)), dtype=torch.float64, device=_device())
+    ctx.gram_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
+    out, r0 = [], 0
+    for rows in rows_list:
+        out.append(T[r0:r0 + len(rows)])
+        r0 += len(rows)
+    return out
 
 
 # ------------------------------------------------ x = 0 cell of FFT S3 sums

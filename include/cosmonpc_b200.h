@@ -347,6 +347,17 @@ int cnpc_contract_gram(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g,
                        const int *h_a, int na, const int *h_b, int nb, double *d_out,
                        cnpc_stream_t stream);
 
+/* FP32 Gram with several weight fields in one launch: d_out[i*nb + j] =
+ * sum_x G_{h_ag[i]}(x) F_{h_a[i]}(x) F_{h_b[j]}(x), where h_gs[0..ngs) (ngs <= 4) are
+ * device pointers to the weight fields and h_ag gives each row's weight; na <= 48,
+ * nb <= 24, and ngs + na (padded to 8) + nb (padded to 4, omitted when the columns
+ * are a run of the rows) <= 48 staged rows.  The FFT S3 sums of several angular configurations share their unit
+ * shell fields (clustering_estimator.py:1257, :1341) and are contracted together. */
+int cnpc_contract_gram_multi_g(cnpc_ctx *ctx, int64_t ncell, const float *const *h_gs, int ngs,
+                               const float *d_fields, int64_t field_stride, const int *h_a,
+                               const int *h_ag, int na, const int *h_b, int nb, double *d_out,
+                               cnpc_stream_t stream);
+
 /* Pair-list form: d_out[p] = sum_x G(x) F_{h_a[p]}(x) F_{h_b[p]}(x), p < npairs
  * (<= 256), FP64 result; the diagonal data vector's same-bin pairs
  * (clustering_estimator.py:998-1061, :1983-2035) without the whole Gram block.

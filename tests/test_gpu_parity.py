@@ -251,3 +251,40 @@ def test_tiled_paint_fixed_point_scales(case):
         got = mesh[k].double().cpu().numpy()
         assert np.max(np.abs(got - ref)) < 2e-6 * np.max(ref), (case, k)
         assert abs(got.sum() - w.sum()) < 1e-6 * w.sum()
+
+
+@pytest.mark.parametrize("ngs,rows,nb,shared", [(2, (20, 20), 20, True), (3, (5, 9, 11), 8, False),
+                                                (1, (17,), 7, False), (4, (10, 10, 10, 10), 20, True)])
+def test_multi_weight_gram_matches_separate_launches(ngs, rows, nb, shared):
+    """cnpc_contract_gram_multi_g (several weight fields, rows weighted per
+    group, columns shared) against one cnpc_contract_gram per weight field and
+    against FP64 sums."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    n = 48
+    ncell = n ** 3
+    rng = np.random.default_rng(ngs * 100 + nb)
+    na = sum(rows)
+    nf = na + (0 if shared else nb)
+    stride = ncell + 4
+    f = torch.from_numpy(rng.standard_normal((nf, stride)).astype(np.float32)).cuda()
+    gs = [torch.from_numpy(rng.standard_normal(ncell).astype(np.float32)).cuda() for _ in range(ngs)]
+    a = list(rng.permutation(na))
+    ag = [g for g, r in enumerate(rows) for _ in range(r)]
+    b = a[:nb] if shared else list(range(na, na + nb))
+    ctx = _lib.Context.get()
+    out = torch.empty((na, nb), dtype=torch.float64, device="cuda")
+    ctx.gram_multi_g(ncell, gs, f, stride, a, ag, b, out)
+    fd = f[:, :ncell].double()
+    r0 = 0
+    for g, r in enumerate(rows):
+        rr = a[r0:r0 + r]
+        sep = torch.empty((r, nb), dtype=torch.float64, device="cuda")
+        ctx.gram(_lib.F32, ncell, gs[g], f, stride, rr, b, sep)
+        ref = (gs[g].double() * fd[rr]) @ fd[b].T
+        scale = (gs[g].double().abs() * fd[rr].abs()) @ fd[b].abs().T
+        got = out[r0:r0 + r]
+        assert ((got - ref).abs() / scale).max().item() < 1e-6
+        assert ((got - sep).abs() / scale).max().item() < 1e-6
+        r0 += r
