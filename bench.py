@@ -40,11 +40,12 @@ SMALL = dict(WORKLOAD, n_particles=500_000, nmesh=128, boxsize=1000.0, k_max=0.1
 MOCK_CLASSES = [(128, 1000.0), (192, 1500.0), (256, 2000.0)]
 MOCKS = dict(n_particles=1_500_000, sampler="cic", interlaced=True, k_min=0.01, k_max=0.16, k_bins=15,
              poles=(0, 2, 4), angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana")
-# DRAM traffic / algorithmic bytes per kernel, from one ncu capture of the 128^3
-# case (dram__bytes_read.sum + dram__bytes_write.sum of every launch of the
-# kernel in one data vector); the contraction's traffic scales with cells x
-# staged rows, so the ratio carries to 256^3
-TRAFFIC_RATIO = {"gram": 1.008}
+# DRAM traffic / algorithmic bytes per kernel (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum): the contraction from every launch of one 128^3 data
+# vector (its traffic scales with cells x staged rows, so the ratio carries to
+# 256^3); the shell fields from one 8-field call at 256^3 (column + y/z
+# kernels; the last fields' writes still sit in L2 when the kernel ends)
+TRAFFIC_RATIO = {"gram": 1.008, "shell_fields": 0.90}
 METRIC = "bk_sugi 256^3 full-mode s/data-vector"
 UNIT = "s/data-vector"
 
@@ -174,6 +175,59 @@ def cpu_baseline_estimate(workload, seed):
     return total, sample, os.cpu_count()
 
 
+# ------------------------------------------------------- survey workload
+SURVEY = dict(n_data=2_000_000, n_randoms=40_000_000, ra=(100.0, 260.0), dec=(0.0, 60.0), z_mu=0.5,
+              z_sigma=0.1, z_clip=(0.2, 0.8), nmesh=512, boxsize=3500.0, sampler="tsc", interlaced=True)
+
+
+def _survey_runs(seed, reps, scale=1.0):
+    """Seconds per run_stats call of the survey cross workload (pk cross [0,2,4];
+    bk_sugi aab (0,0,0) and (2,0,2) diagonal), FITS catalogs on local disk,
+    FP32 form and the plain FP64 drop-in; each call reads and decodes its
+    catalogs like the reference's.  ``scale`` shrinks the catalogs."""
+    import tempfile
+
+    import cosmonpc_b200
+    from cosmonpc_b200 import mocks
+
+    S = SURVEY
+    tmp = tempfile.mkdtemp(prefix="cnpc_survey_")
+    geo = dict(ra=S["ra"], dec=S["dec"], z_mu=S["z_mu"], z_sigma=S["z_sigma"], z_clip=S["z_clip"])
+    nd, nr = int(S["n_data"] * scale), int(S["n_randoms"] * scale)
+    d_a, r_a = mocks.survey_catalogs(nd, nr, seed, **geo)
+    d_b, _ = mocks.survey_catalogs(nd // 2, 1000, seed + 1, **geo)  # independent overdensity
+    paths = {}
+    for key, cols in (("data_a", d_a), ("randoms_a", r_a), ("data_b", d_b)):
+        paths[key] = mocks.write_fits_catalog(os.path.join(tmp, key + ".fits"), cols)
+    paths["randoms_b"] = paths["randoms_a"]
+    base = dict(geometry="survey-like", catalogs=paths, column_names=["RA", "DEC", "Z", "WEIGHT_FKP", "NZ"],
+                cosmology={"h": 0.676, "Omega0": 0.31}, compensation=True, nmesh=[S["nmesh"]] * 3,
+                boxsize=[S["boxsize"]] * 3, z_range=list(S["z_clip"]), sampler=S["sampler"],
+                interlaced=S["interlaced"], comp_weight_plan={"scheme": None, "name_alias": None},
+                alpha_scheme="pypower", normalization_scheme="mixed-mesh", output_dir=os.path.join(tmp, "out"))
+    runs = {"pk_cross_024": dict(statistic="pk", correlation_mode="cross", k_min=0.005, k_max=0.305, k_bins=30,
+                                 poles=[0, 2, 4]),
+            "bk_aab_000_diag": dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="aab", k_min=0.01,
+                                    k_max=0.21, k_bins=20, angu_config=[0, 0, 0], data_vector_mode="diagonal",
+                                    shotnoise_mode="ana"),
+            "bk_aab_202_diag": dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="aab", k_min=0.01,
+                                    k_max=0.21, k_bins=20, angu_config=[2, 0, 2], data_vector_mode="diagonal",
+                                    shotnoise_mode="ana")}
+    out = {}
+    for name, over in runs.items():
+        for prec in ("f32", "f64"):
+            cfg = dict(base, **over, precision=prec)
+            cosmonpc_b200.run_stats(dict(cfg))  # warm-up: plans, buffers, page cache
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                cosmonpc_b200.run_stats(dict(cfg))
+            out["%s:%s" % (name, prec)] = (time.perf_counter() - t0) / reps
+    import shutil
+
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out, nd, nr
+
+
 # ----------------------------------------------------------------- main
 def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
     """mocks/s of the fast form (FP32 fields, one paint per mock, the next mock
@@ -240,6 +294,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mocks", type=int, default=4, help="mocks per shape class for the mocks/s line (0: skip)")
+    ap.add_argument("--survey", action="store_true",
+                    help="time the survey cross workload (512^3, 2e6 data, 4e7 randoms) instead; one JSON line")
+    ap.add_argument("--survey-scale", type=float, default=1.0, help="catalog size factor of --survey")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +306,21 @@ def main():
     from cosmonpc_b200.mocks import BASE_SEED
 
     seed = BASE_SEED + 3
+
+    if args.survey:
+        import torch
+
+        from cosmonpc_b200.mocks import BASE_SEED as _BS
+
+        t, nd, nr = _survey_runs(_BS + 4, max(1, args.steps), args.survey_scale)
+        f32 = sum(v for k, v in t.items() if k.endswith("f32"))
+        f64 = sum(v for k, v in t.items() if k.endswith("f64"))
+        print(json.dumps({"metric": "survey cross pk + bk aab 512^3 s/data-vector (run_stats, FITS read included)",
+                          "value": f32, "unit": "s/data-vector", "higher_is_better": False, "n_gpus": 1,
+                          "steps": max(1, args.steps), "plain_f64": f64, "speedup": f64 / f32,
+                          "per_call_s": t, "data": "synthetic", "catalogs": {"data": nd, "randoms": nr},
+                          "gpu": torch.cuda.get_device_name(0)}))
+        return 0
 
     if args.impl == "reference":
         if rank != 0:

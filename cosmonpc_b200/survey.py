@@ -138,7 +138,13 @@ def _decode_file(path, column_names, z_range, comp_weight_plan, catalog_type, co
     spec.omega_m = float(cosmology["Omega0"])
     dev = _device()
     nr = t.nrows
-    rows = torch.from_numpy(np.array(t.rows(), copy=True).reshape(-1)).pin_memory().to(dev)
+    # file rows -> one pinned buffer (a single host copy) -> device
+    raw = t.rows()
+    host = torch.empty(raw.size, dtype=torch.uint8, pin_memory=True)
+    if raw.size:
+        np.copyto(host.numpy().reshape(raw.shape), raw)
+    rows = host.to(dev, non_blocking=True)
+    del raw, host
     cap = max(nr, 1)
     pos = torch.empty((cap, 3), dtype=torch.float64, device=dev)
     w = torch.empty(cap, dtype=torch.float64, device=dev)
