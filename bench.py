@@ -512,8 +512,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (TRAFFIC_RATIO[dom_name] * nbytes / cnt) if dom_name in TRAFFIC_RATIO else None,
-                     "traffic_note": "bytes per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum over the "
-                                     "algorithmic bytes, measured on the 128^3 case and applied to this launch"},
+                     "traffic_note": "bytes per launch: the kernel's ncu (dram__bytes_read.sum + "
+                                     "dram__bytes_write.sum) / algorithmic-bytes ratio (gram: 128^3 capture, "
+                                     "shell_fields: 256^3 capture) times this launch's algorithmic bytes"},
         "kernels": kernels,
         "mocks": mocks,
         "gpu_launches": launches * args.steps,
