@@ -133,6 +133,55 @@ def mock_pk_bk(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k
     return finalize if deferred else finalize()
 
 
+class MockGraphs:
+    """:func:`mock_pk_bk` for a stream of same-shaped mocks, replayed from CUDA
+    graphs: the device work of one mock (paint, transforms, shell fields,
+    contractions, copies of the sums to pinned host memory) is captured once
+    per slot and replayed for every mock, so the host no longer issues ~100
+    launches per mock.  Catalogs must have ``npart`` particles (no weights)
+    inside the box.  ``submit(pos)`` copies ``pos`` into the slot's input,
+    replays, and returns a function that waits for that replay and returns
+    (pk result, [bk results]); call it before submitting ``slots`` more mocks.
+
+    Raises RuntimeError when the device work cannot be captured (then use
+    :func:`mock_pk_bk`)."""
+
+    def __init__(self, npart, nmesh, boxsize, slots=2, **kw):
+        self.kw = dict(kw, nmesh=nmesh, boxsize=boxsize)
+        self.slots = []
+        self.count = 0
+        dev = torch.device("cuda", torch.cuda.current_device())
+        for _ in range(slots):
+            pos = torch.empty((int(npart), 3), dtype=torch.float64, device=dev)
+            pos.uniform_(0.0, float(boxsize) * (1.0 - 1e-12))
+            for _ in range(2):  # plans, workspaces and pinned buffers at their final sizes
+                mock_pk_bk(pos, None, **self.kw)
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            try:
+                with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+                    fin = mock_pk_bk(pos, None, deferred=True, **self.kw)
+            except Exception as e:  # a host synchronisation or allocation inside the work
+                raise RuntimeError("mock pipeline could not be captured: %s" % e) from e
+            self.slots.append((pos, graph, fin))
+
+    def submit(self, pos):
+        inp, graph, fin = self.slots[self.count % len(self.slots)]
+        self.count += 1
+        if tuple(pos.shape) != tuple(inp.shape):
+            raise ValueError("catalog shape %s differs from the captured %s" % (tuple(pos.shape), tuple(inp.shape)))
+        inp.copy_(pos, non_blocking=True)
+        graph.replay()
+        done = torch.cuda.Event()
+        done.record()
+
+        def finalize():
+            done.synchronize()
+            return fin()
+
+        return finalize
+
+
 def mock_pk_bk_plain(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles=(0, 2, 4),
                      angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana", rsd=(0, 0, 1)):
     """The plain FP64 per-call form of :func:`mock_pk_bk`: one power-spectrum and

@@ -332,10 +332,17 @@ template <int T> struct YZLayout {
     static constexpr int kTotal = kB + M * LD;                       // float2
 };
 
+// Output fields and band limits of the items, passed by value (no host-to-device
+// table copy, so a call can be captured in a CUDA graph).
+struct YZOut {
+    float *out[CNPC_MAX_ITEMS];
+    int rmax[CNPC_MAX_ITEMS];
+    int r2max[CNPC_MAX_ITEMS];
+};
+
 template <int T>
-__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work,
-                                                                  const int *__restrict__ rmax_of, int nitems,
-                                                                  float *const *__restrict__ outs) {
+__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work, int nitems,
+                                                                  const YZOut O) {
     using YL = YZLayout<T>;
     constexpr int M = YL::M, N = YL::N, H = YL::H, LD = YL::LD, TEAMS = YL::TEAMS;
     constexpr int Q = 16 / T;
@@ -351,7 +358,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     const unsigned mask = team_mask(T);
     float2 *tex = tw + YL::kEx + team * Exch<T>::kStride;
     const float2 *a = work + ((size_t)item * N + x) * M * H;  // A[x][slot][kz]
-    const int rmax = rmax_of[2 * item], r2max = rmax_of[2 * item + 1];
+    const int rmax = O.rmax[item], r2max = O.r2max[item];
     const int K = rmax + 1 < H ? rmax + 1 : H;  // columns k_z >= K are zero
     constexpr int KC = (kKC < H) ? kKC : H;
     // y: one team per k_z column
@@ -376,7 +383,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             }
     }
     __syncthreads();
-    float *fout = outs[item] + (size_t)x * N * N;
+    float *fout = O.out[item] + (size_t)x * N * N;
     // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity.  Teams of one warp
     // take pairs 4 apart, so their rows sit 8 * LD float2 (16 banks) apart.
     for (int p0 = 0; p0 < M / 2; p0 += TEAMS) {
@@ -448,7 +455,7 @@ template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLay
 template <int T>
 static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, const float2 *B, const EdgeSet &es,
                             const HarmTable &ht, const ShellItemsDev &items, float2 *workA,
-                            float *const *d_outs, const int *d_rmax, cudaStream_t s) {
+                            const YZOut &O, cudaStream_t s) {
     constexpr int M = 16 * T, N = 2 * M, H = M / 2;
     constexpr int KC = kKC < H ? kKC : H;
     constexpr int NCH = H / KC;
@@ -462,7 +469,7 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     const int ni = items.n;
     shell_column_kernel<T, true><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, nullptr,
                                                                              workA);
-    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, d_rmax, ni, d_outs);
+    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, O);
     return check_launch(ctx, "shell_fields kernels");
 }
 
@@ -513,27 +520,20 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
     const int T = n / 32;
     const size_t per_item_a = sizeof(float2) * (size_t)n * (n / 2) * (n / 4);  // A[x][s][n_z]
     cudaStream_t s = (cudaStream_t)stream;
-    // output pointer table and the pass-1 work array in one workspace
-    const size_t ptr_bytes = (sizeof(float *) * nitems + 2 * sizeof(int) * nitems + 255) / 256 * 256;
-    st = ensure_buffer(ctx, &ctx->shell_ws, &ctx->shell_ws_bytes, ptr_bytes + per_item_a * nitems, s);
+    // the pass-1 work array
+    st = ensure_buffer(ctx, &ctx->shell_ws, &ctx->shell_ws_bytes, per_item_a * nitems, s);
     if (st) return st;
-    float **d_ptrs = static_cast<float **>(ctx->shell_ws);
-    float2 *workA = reinterpret_cast<float2 *>(static_cast<char *>(ctx->shell_ws) + ptr_bytes);
-    // output pointers, then the items' rmax (pageable source: copied before the call returns)
-    std::vector<char> table(sizeof(float *) * nitems + 2 * sizeof(int) * nitems);
+    float2 *workA = static_cast<float2 *>(ctx->shell_ws);
+    YZOut O;
+    std::memset(&O, 0, sizeof(O));
     for (int j = 0; j < nitems; ++j) {
-        float *pj = static_cast<float *>(h_out_fields[j]);
-        const int band[2] = {items.rmax[j], items.r2max[j]};
-        std::memcpy(table.data() + sizeof(float *) * j, &pj, sizeof(float *));
-        std::memcpy(table.data() + sizeof(float *) * nitems + 2 * sizeof(int) * j, band, sizeof(band));
+        O.out[j] = static_cast<float *>(h_out_fields[j]);
+        O.rmax[j] = items.rmax[j];
+        O.r2max[j] = items.r2max[j];
     }
-    st = check_cuda(ctx, cudaMemcpyAsync(d_ptrs, table.data(), table.size(), cudaMemcpyHostToDevice, s),
-                    "shell output table");
-    if (st) return st;
-    const int *d_rmax = reinterpret_cast<const int *>(reinterpret_cast<char *>(d_ptrs) + sizeof(float *) * nitems);
     const float2 *A = static_cast<const float2 *>(d_spec_a);
     const float2 *B = static_cast<const float2 *>(d_spec_b);
-    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
-    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
-    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, d_ptrs, d_rmax, s);
+    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
 }

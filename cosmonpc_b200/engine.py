@@ -241,12 +241,18 @@ class HostCopy:
     def __init__(self, t):
         self.host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
         self.host.copy_(t, non_blocking=True)
-        self.event = torch.cuda.Event()
-        self.event.record()
+        self.event = None
+        if not torch.cuda.is_current_stream_capturing():
+            # inside a CUDA graph capture the copy becomes a graph node: whoever
+            # replays the graph synchronises before reading
+            self.event = torch.cuda.Event()
+            self.event.record()
 
     def get(self):
-        self.event.synchronize()
-        return self.host.numpy()
+        if self.event is not None:
+            self.event.synchronize()
+            return self.host.numpy()
+        return self.host.numpy().copy()  # a graph's buffer is rewritten by its next replay
 
 
 def _staged_rows(nr, nc, shared):

@@ -100,6 +100,17 @@ def _sky_sample(rng, n, ra, dec, z_mu, z_sigma, z_clip):
     return r, d, z
 
 
+def lognormal_box_exact(n_particles, boxsize, seed, **kw):
+    """:func:`lognormal_box` with exactly ``n_particles`` positions (a random
+    subset of a slightly larger draw), as for fixed-size mock catalogs."""
+    rng = np.random.Generator(np.random.PCG64(seed + 7919))
+    pos = lognormal_box(int(n_particles * 1.02) + 64, boxsize, seed, **kw)
+    if len(pos) >= n_particles:
+        return pos[np.sort(rng.choice(len(pos), n_particles, replace=False))]
+    extra = pos[rng.integers(0, len(pos), n_particles - len(pos))]
+    return np.concatenate([pos, extra])
+
+
 def survey_catalogs(n_data, n_randoms, seed, ra=(150.0, 180.0), dec=(10.0, 35.0), z_mu=0.5,
                     z_sigma=0.05, z_clip=(0.4, 0.6), h=0.6766, omega_m=0.31, p0=1.0e4,
                     boss_weights=False, grid=32, pk_amp=2.0e4):
