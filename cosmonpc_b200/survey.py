@@ -21,6 +21,7 @@ Every per-particle, per-cell and per-mode operation runs in libcosmonpc_b200.so
 from __future__ import annotations
 
 import logging
+import os
 
 import numpy as np
 import torch
@@ -98,6 +99,23 @@ def _column(table, name):
     return col
 
 
+_COPY_THREADS = max(1, min(8, os.cpu_count() or 1))
+
+
+def _parallel_copy(dst, src):
+    """dst[:] = src for (rows, bytes) arrays, row blocks copied by a thread pool."""
+    n = src.shape[0]
+    if n < 65536 or _COPY_THREADS == 1:
+        np.copyto(dst, src)
+        return
+    from concurrent.futures import ThreadPoolExecutor
+
+    cuts = np.linspace(0, n, _COPY_THREADS + 1).astype(np.int64)
+    with ThreadPoolExecutor(_COPY_THREADS) as ex:
+        list(ex.map(lambda i: np.copyto(dst[cuts[i]:cuts[i + 1]], src[cuts[i]:cuts[i + 1]]),
+                    range(_COPY_THREADS)))
+
+
 def _decode_file(path, column_names, z_range, comp_weight_plan, catalog_type, cosmology,
                  normalization_scheme):
     t = open_table(path)
@@ -138,11 +156,12 @@ def _decode_file(path, column_names, z_range, comp_weight_plan, catalog_type, co
     spec.omega_m = float(cosmology["Omega0"])
     dev = _device()
     nr = t.nrows
-    # file rows -> one pinned buffer (a single host copy) -> device
+    # file rows -> one pinned buffer (a single host copy, split over threads:
+    # numpy releases the GIL for the copy) -> device
     raw = t.rows()
     host = torch.empty(raw.size, dtype=torch.uint8, pin_memory=True)
     if raw.size:
-        np.copyto(host.numpy().reshape(raw.shape), raw)
+        _parallel_copy(host.numpy().reshape(raw.shape), raw)
     rows = host.to(dev, non_blocking=True)
     del raw, host
     cap = max(nr, 1)

@@ -122,3 +122,42 @@ def test_gram_block_assembly_matches_entrywise(mode, leg1, leg2, sign):
     t = lambda k1, k2: T[ri[k1], ci[k2]] if k1 in ri and k2 in ci else 0.0
     ref = np.array([[engine._assemble_entry(ps, t, a, c) for c in cbins] for a in rbins])
     np.testing.assert_array_equal(S, ref)
+
+
+def test_launch_groups_merge_same_columns_within_staging_limit():
+    """FP32 weight groups with identical columns share a launch while the
+    staged rows (weights + padded rows + padded columns unless shared) fit."""
+    from cosmonpc_b200 import engine
+
+    class SF:
+        precision = "f32"
+
+        def __init__(self):
+            self.slot = {}
+
+        def key(self, leg, b, comp):
+            k = (tuple(leg), int(b), int(comp))
+            self.slot.setdefault(k, len(self.slot))
+            return k
+
+    sf = SF()
+    u0 = [sf.key((0, 0, 2, True), b, 0) for b in range(20)]
+    u2 = [sf.key((2, 0, 2, True), b, 0) for b in range(20)]
+    other = [sf.key((4, 0, 2, True), b, 0) for b in range(20)]
+    # (000) rows u0, (202) rows u2, both against columns u0: merged, columns shared
+    assert engine._launch_groups(sf, [u0, u2], [u0, u0]) == [[0, 1]]
+    # different columns: separate launches
+    assert engine._launch_groups(sf, [u0, u2], [u0, u2]) == [[0], [1]]
+    # 2 weights + 40 rows + 20 unshared columns > 48 staged rows: separate
+    assert engine._launch_groups(sf, [u2, other], [u0, u0]) == [[0], [1]]
+    sf.precision = "f64"
+    assert engine._launch_groups(sf, [u0, u2], [u0, u0]) == [[0], [1]]
+
+
+def test_lognormal_box_exact_count():
+    from cosmonpc_b200.mocks import lognormal_box_exact
+
+    for n in (1000, 4321):
+        pos = lognormal_box_exact(n, 500.0, 3)
+        assert pos.shape == (n, 3)
+        assert pos.min() >= 0.0 and pos.max() < 500.0
