@@ -436,6 +436,33 @@ def main():
     _lib.timer = None
     value = t_fast / (args.steps * world)
 
+    # ---- cross-mock amortisation (opt-in): the data-independent unit-spectrum
+    #      S3 shells kept across the data vectors of this shape class
+    from cosmonpc_b200 import engine as _engine
+
+    _engine.UNIT_SHELL_CACHE = True
+    try:
+        run_vectors(args.warmup, pos_dev)
+        barrier()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        res_amort = run_vectors(args.steps, pos_dev)
+        a1.record()
+        barrier()
+        t_amort = max_over_ranks(a0.elapsed_time(a1) / 1000.0) / (args.steps * world)
+    finally:
+        _engine.UNIT_SHELL_CACHE = False
+        _engine.clear_unit_shell_cache()
+    amort_err = 0.0
+    for a, b in zip(res_amort, res_fast):
+        for k in ("B_sugi", "Bk_raw", "Shot_noise"):
+            amort_err = max(amort_err, float(np.max(np.abs(np.asarray(a[k]) - np.asarray(b[k])))
+                                             / np.max(np.abs(np.asarray(b[k])))))
+    amortized = {"value": t_amort, "unit": UNIT, "max_rel_err_vs_value_path": amort_err,
+                 "note": "the FFT S3 unit-spectrum shells (data-independent: nmesh, boxsize, bins, lm) "
+                         "synthesised once and kept across data vectors of one shape class"}
+
     # ---- end to end through the public API from pinned host memory
     e2e = None
     if not args.no_e2e:
@@ -515,6 +542,7 @@ def main():
                        (3 * W["k_bins"]) * W["nmesh"] ** 3 * 4 / 1e9),
                    "parallelism": "replicas x%d" % world},
         "e2e": e2e,
+        "amortized": amortized,
         "serial": {"value": t_serial, "unit": UNIT,
                    "note": "one data vector at a time, host algebra not overlapped with the next vector"},
         "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),

@@ -266,7 +266,10 @@ def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat
     if s3_groups:
         all_sp = [ps for (_, sp) in s3_groups for ps in sp]
         bsf, capf = _plan_blocks(all_sp, k_bins, n, precision, block_size, diagonal, free_bytes)
-        sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
+        if engine.UNIT_SHELL_CACHE and bsf >= k_bins:
+            sfu = engine.unit_shells(n, L, k_edge, precision, capf)
+        else:
+            sfu = engine.ShellFields(n, L, k_edge, precision, None, None, capacity=capf)
         outs = engine.pair_sums(s3_groups, sfu, k_bins, diagonal, bsf)
         s3fft = {ci: outs[gi] for ci, gi in s3_index.items()}
         del sfu

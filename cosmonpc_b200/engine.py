@@ -164,6 +164,7 @@ class ShellFields:
         self._scratch = None
         self.slot = {}
         self.free = list(range(self.capacity))[::-1]
+        self.persistent = False  # fields survive release calls (unit-shell cache)
 
     @property
     def scratch(self):
@@ -177,10 +178,14 @@ class ShellFields:
         return (tuple(leg), int(b), int(comp))
 
     def release_all(self):
+        if self.persistent:
+            return
         self.slot.clear()
         self.free = list(range(self.capacity))[::-1]
 
     def release(self, keys):
+        if self.persistent:
+            return
         for k in keys:
             s = self.slot.pop(k, None)
             if s is not None:
@@ -190,6 +195,11 @@ class ShellFields:
         """Synthesise every (leg, bin, comp) in ``keys`` not yet resident."""
         ctx = _lib.Context.get()
         todo = [k for k in dict.fromkeys(keys) if k not in self.slot]
+        if len(todo) > len(self.free) and self.persistent:
+            # a persistent cache holding other shells: start over with this set
+            self.slot.clear()
+            self.free = list(range(self.capacity))[::-1]
+            todo = list(dict.fromkeys(keys))
         if len(todo) > len(self.free):
             raise MemoryError("shell-field cache too small for this block")
         harm_index = {}
@@ -542,9 +552,48 @@ def contract_multi(Gs, sf, rows_list, cols):
 # FP64: src(0) = sum_k src(k) and F(0) = sum_{k in bin} conj?(Y(khat)) are mode
 # sums evaluated in FP64 from the spectra.
 
+# ------------------------------------------- cross-mock amortisation (opt-in)
+# The FFT S3 shells c2r(conj Y_lm * mask_bin) of a unit spectrum and their
+# x = 0 values depend only on (nmesh, boxsize, bins, lm): with UNIT_SHELL_CACHE
+# they are synthesised once per shape class and reused by later data vectors
+# (one class kept at a time).  Off by default: every call then synthesises them,
+# as the reference does.
+UNIT_SHELL_CACHE = False
+_unit_shells = {}
+_unit_origin = {}
+
+
+def clear_unit_shell_cache():
+    _unit_shells.clear()
+    _unit_origin.clear()
+
+
+def unit_shells(n, boxsize, edges, precision, capacity):
+    """The persistent unit-spectrum ShellFields of this geometry (UNIT_SHELL_CACHE)."""
+    key = (int(n), float(boxsize), tuple(float(e) for e in edges), precision, torch.cuda.current_device())
+    sf = _unit_shells.get(key)
+    if sf is None or sf.capacity < capacity:
+        clear_unit_shell_cache()
+        sf = ShellFields(n, boxsize, edges, precision, None, None, capacity=capacity)
+        sf.persistent = True
+        _unit_shells[key] = sf
+    return sf
+
+
 def unit_shell_origin(n, boxsize, edges, precision, legs):
     """{leg: HostCopy of complex F(0) per bin} for unit-spectrum shell legs
     (l, m, 2, conj): F(0) = sum over the bin's full-space modes of Y or conj Y."""
+    if UNIT_SHELL_CACHE:
+        key = (int(n), float(boxsize), tuple(float(e) for e in edges), precision, tuple(dict.fromkeys(legs)),
+               torch.cuda.current_device())
+        hit = _unit_origin.get(key)
+        if hit is None:
+            hit = _unit_origin[key] = _unit_shell_origin(n, boxsize, edges, precision, legs)
+        return hit
+    return _unit_shell_origin(n, boxsize, edges, precision, legs)
+
+
+def _unit_shell_origin(n, boxsize, edges, precision, legs):
     ctx = _lib.Context.get()
     code = PRECISION[precision][0]
     unit = ctx.operand(None)

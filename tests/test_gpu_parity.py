@@ -319,3 +319,28 @@ def test_mock_graphs_match_eager():
                 assert rel_err(bk[key], ref[key]) < 1e-6, key
     with pytest.raises(ValueError):
         graphs.submit(cats[0][:-1])
+
+
+def test_unit_shell_cache_matches_fresh_shells():
+    """With the opt-in unit-shell cache the FFT S3 shells of a full data vector
+    are synthesised once and reused: later calls equal calls without it."""
+    from cosmonpc_b200 import api, engine
+    from cosmonpc_b200.mocks import lognormal_box
+
+    pos = lognormal_box(200000, 800.0, 31)
+    kw = dict(nmesh=64, boxsize=800.0, sampler="tsc", interlaced=True, k_min=0.01, k_max=0.11, k_bins=8,
+              angu_configs=[(0, 0, 0), (2, 0, 2)], data_vector_mode="full", shotnoise_mode="both",
+              precision="f32")
+    ref = api.bk_sugi_box_vector(pos, None, **kw)
+    engine.UNIT_SHELL_CACHE = True
+    try:
+        runs = [api.bk_sugi_box_vector(pos, None, **kw) for _ in range(3)]
+        assert engine._unit_shells and engine._unit_origin
+    finally:
+        engine.UNIT_SHELL_CACHE = False
+        engine.clear_unit_shell_cache()
+    for got in runs:
+        for a, b in zip(got, ref):
+            for key in ("B_sugi", "Bk_raw", "Shot_noise"):
+                assert rel_err(a[key], b[key]) < 1e-6, key
+            assert rel_err(a["SN_terms"]["SN3_FFT"], b["SN_terms"]["SN3_FFT"]) < 1e-6
