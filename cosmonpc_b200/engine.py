@@ -88,12 +88,22 @@ def finish_delta(pm, scale, comp, k0, band=0.0):
 
 
 def kbin_counts(n, boxsize, edges):
+    """Mode counts and sum |k| per bin (geometry only: kept per shape class
+    while UNIT_SHELL_CACHE is on)."""
+    key = None
+    if UNIT_SHELL_CACHE:
+        key = (int(n), float(boxsize), tuple(float(e) for e in edges), torch.cuda.current_device())
+        hit = _kbin_cache.get(key)
+        if hit is not None:
+            return hit
     ctx = _lib.Context.get()
     dev = _device()
     nb = len(edges) - 1
     counts = torch.empty(nb, dtype=torch.float64, device=dev)
     ksum = torch.empty(nb, dtype=torch.float64, device=dev)
     ctx.kbin_counts(n, float(boxsize), edges, counts, ksum)
+    if key is not None:
+        _kbin_cache[key] = (counts, ksum)
     return counts, ksum
 
 
@@ -553,19 +563,21 @@ def contract_multi(Gs, sf, rows_list, cols):
 # sums evaluated in FP64 from the spectra.
 
 # ------------------------------------------- cross-mock amortisation (opt-in)
-# The FFT S3 shells c2r(conj Y_lm * mask_bin) of a unit spectrum and their
-# x = 0 values depend only on (nmesh, boxsize, bins, lm): with UNIT_SHELL_CACHE
-# they are synthesised once per shape class and reused by later data vectors
-# (one class kept at a time).  Off by default: every call then synthesises them,
-# as the reference does.
+# The FFT S3 shells c2r(conj Y_lm * mask_bin) of a unit spectrum, their
+# x = 0 values and the bins' mode counts depend only on (nmesh, boxsize, bins,
+# lm): with UNIT_SHELL_CACHE they are computed once per shape class and reused
+# by later data vectors (one shell class kept at a time).  Off by default:
+# every call then computes them, as the reference does.
 UNIT_SHELL_CACHE = False
 _unit_shells = {}
 _unit_origin = {}
+_kbin_cache = {}
 
 
 def clear_unit_shell_cache():
     _unit_shells.clear()
     _unit_origin.clear()
+    _kbin_cache.clear()
 
 
 def unit_shells(n, boxsize, edges, precision, capacity):
