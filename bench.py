@@ -379,16 +379,25 @@ def main():
     def step_resident():
         return api.bk_sugi_box_vector(pos_dev, None, precision="f32", **common)
 
+    side = torch.cuda.Stream()
+
     def run_vectors(k, pos):
         """k data vectors back to back: each one's device work is enqueued
-        before the previous one's host algebra runs (the deferred API)."""
+        before the previous one's host algebra runs (the deferred API), odd
+        vectors on a second stream (with its own library context) so that two
+        vectors' kernels can overlap; the current stream waits for both."""
+        cur = torch.cuda.current_stream()
+        side.wait_stream(cur)
         prev = None
-        for _ in range(k):
-            f = api.bk_sugi_box_vector(pos, None, precision="f32", deferred=True, **common)
+        for i in range(k):
+            with torch.cuda.stream(side if i % 2 else cur):
+                f = api.bk_sugi_box_vector(pos, None, precision="f32", deferred=True, **common)
             if prev is not None:
                 prev()
             prev = f
-        return prev()
+        out = prev()
+        cur.wait_stream(side)
+        return out
 
     def barrier():
         if dist is not None:

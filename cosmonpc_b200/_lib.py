@@ -219,7 +219,10 @@ def _esz(dtype):
 
 
 class Context:
-    """One library context (cuFFT plan cache + scratch) per CUDA device."""
+    """One library context (cuFFT plan cache + scratch) per CUDA device and
+    stream: work queued on the default stream (and CUDA graph captures) uses the
+    device's primary context, every other stream gets its own, so data vectors
+    queued on different streams can run concurrently without sharing scratch."""
 
     _per_device = {}
 
@@ -239,11 +242,16 @@ class Context:
         if not torch.cuda.is_available():
             raise RuntimeError("cosmonpc_b200 needs a CUDA device; none is available")
         dev = torch.cuda.current_device() if device is None else int(device)
-        ctx = cls._per_device.get(dev)
+        key = dev
+        if not torch.cuda.is_current_stream_capturing():
+            s = torch.cuda.current_stream(dev).cuda_stream
+            if s != torch.cuda.default_stream(dev).cuda_stream:
+                key = (dev, s)
+        ctx = cls._per_device.get(key)
         if ctx is None:
             with torch.cuda.device(dev):
                 ctx = cls(dev)
-            cls._per_device[dev] = ctx
+            cls._per_device[key] = ctx
         return ctx
 
     def close(self):

@@ -95,7 +95,8 @@ def kbin_counts(n, boxsize, edges):
         key = (int(n), float(boxsize), tuple(float(e) for e in edges), torch.cuda.current_device())
         hit = _kbin_cache.get(key)
         if hit is not None:
-            return hit
+            torch.cuda.current_stream().wait_event(hit[2])  # written on another stream, maybe
+            return hit[0], hit[1]
     ctx = _lib.Context.get()
     dev = _device()
     nb = len(edges) - 1
@@ -103,7 +104,9 @@ def kbin_counts(n, boxsize, edges):
     ksum = torch.empty(nb, dtype=torch.float64, device=dev)
     ctx.kbin_counts(n, float(boxsize), edges, counts, ksum)
     if key is not None:
-        _kbin_cache[key] = (counts, ksum)
+        done = torch.cuda.Event()
+        done.record()
+        _kbin_cache[key] = (counts, ksum, done)
     return counts, ksum
 
 
@@ -175,6 +178,7 @@ class ShellFields:
         self.slot = {}
         self.free = list(range(self.capacity))[::-1]
         self.persistent = False  # fields survive release calls (unit-shell cache)
+        self.ready = None        # event after the last synthesis (persistent fields)
 
     @property
     def scratch(self):
@@ -205,8 +209,13 @@ class ShellFields:
         """Synthesise every (leg, bin, comp) in ``keys`` not yet resident."""
         ctx = _lib.Context.get()
         todo = [k for k in dict.fromkeys(keys) if k not in self.slot]
+        if self.persistent and self.ready is not None:
+            # fields another stream may still be writing
+            torch.cuda.current_stream().wait_event(self.ready)
         if len(todo) > len(self.free) and self.persistent:
-            # a persistent cache holding other shells: start over with this set
+            # a persistent cache holding other shells: start over with this set,
+            # once no stream still reads the old ones
+            torch.cuda.synchronize()
             self.slot.clear()
             self.free = list(range(self.capacity))[::-1]
             todo = list(dict.fromkeys(keys))
@@ -243,6 +252,9 @@ class ShellFields:
                     ctx.c2r(self.code, self.n, 1, self.scratch[j], self.fields[s], self.stride)
             for k, s in zip(batch, slots):
                 self.slot[k] = s
+        if self.persistent and todo:
+            self.ready = torch.cuda.Event()
+            self.ready.record()
 
 
 def band_limited_field(n, boxsize, spec, kmax_band, precision, racah=True):
@@ -585,6 +597,8 @@ def unit_shells(n, boxsize, edges, precision, capacity):
     key = (int(n), float(boxsize), tuple(float(e) for e in edges), precision, torch.cuda.current_device())
     sf = _unit_shells.get(key)
     if sf is None or sf.capacity < capacity:
+        if _unit_shells:
+            torch.cuda.synchronize()  # the old fields may still be read on another stream
         clear_unit_shell_cache()
         sf = ShellFields(n, boxsize, edges, precision, None, None, capacity=capacity)
         sf.persistent = True
