@@ -303,6 +303,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mocks", type=int, default=4, help="mocks per shape class for the mocks/s line (0: skip)")
+    ap.add_argument("--streams", type=int, default=2, help="CUDA streams the back-to-back data vectors rotate over")
     ap.add_argument("--survey", action="store_true",
                     help="time the survey cross workload (512^3, 2e6 data, 4e7 randoms) instead; one JSON line")
     ap.add_argument("--survey-scale", type=float, default=1.0, help="catalog size factor of --survey")
@@ -379,24 +380,29 @@ def main():
     def step_resident():
         return api.bk_sugi_box_vector(pos_dev, None, precision="f32", **common)
 
-    side = torch.cuda.Stream()
+    sides = [torch.cuda.Stream() for _ in range(max(0, args.streams - 1))]
 
     def run_vectors(k, pos):
         """k data vectors back to back: each one's device work is enqueued
-        before the previous one's host algebra runs (the deferred API), odd
-        vectors on a second stream (with its own library context) so that two
-        vectors' kernels can overlap; the current stream waits for both."""
+        before the previous one's host algebra runs (the deferred API), the
+        vectors rotating over --streams CUDA streams (each with its own library
+        context) so that their kernels can overlap; the current stream waits
+        for all of them."""
         cur = torch.cuda.current_stream()
-        side.wait_stream(cur)
-        prev = None
+        ring = [cur] + sides
+        for s in sides:
+            s.wait_stream(cur)
+        pending = []
+        out = None
         for i in range(k):
-            with torch.cuda.stream(side if i % 2 else cur):
-                f = api.bk_sugi_box_vector(pos, None, precision="f32", deferred=True, **common)
-            if prev is not None:
-                prev()
-            prev = f
-        out = prev()
-        cur.wait_stream(side)
+            with torch.cuda.stream(ring[i % len(ring)]):
+                pending.append(api.bk_sugi_box_vector(pos, None, precision="f32", deferred=True, **common))
+            if len(pending) >= max(2, len(ring)):  # one stream: still one vector queued ahead
+                out = pending.pop(0)()
+        while pending:
+            out = pending.pop(0)()
+        for s in sides:
+            cur.wait_stream(s)
         return out
 
     def barrier():
