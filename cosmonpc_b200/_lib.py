@@ -235,10 +235,14 @@ class Context:
             raise CnpcError("cnpc_ctx_create(%d) failed: %s" % (device, self.lib.cnpc_status_string(st).decode()))
         self.h = h
 
+    _override = []  # contexts pinned by context_scope (innermost last)
+
     @classmethod
     def get(cls, device=None):
         import torch
 
+        if cls._override and device is None:
+            return cls._override[-1]
         if not torch.cuda.is_available():
             raise RuntimeError("cosmonpc_b200 needs a CUDA device; none is available")
         dev = torch.cuda.current_device() if device is None else int(device)
@@ -253,6 +257,22 @@ class Context:
                 ctx = cls(dev)
             cls._per_device[key] = ctx
         return ctx
+
+    @classmethod
+    def scope(cls, ctx):
+        """Within ``with Context.scope(ctx):`` every call uses ``ctx`` (a CUDA
+        graph captured inside keeps that context's workspaces)."""
+        import contextlib
+
+        @contextlib.contextmanager
+        def _scope():
+            cls._override.append(ctx)
+            try:
+                yield ctx
+            finally:
+                cls._override.pop()
+
+        return _scope()
 
     def close(self):
         if self.h:

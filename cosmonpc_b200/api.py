@@ -147,33 +147,45 @@ class MockGraphs:
     :func:`mock_pk_bk`)."""
 
     def __init__(self, npart, nmesh, boxsize, slots=2, **kw):
+        from . import _lib
+
         self.kw = dict(kw, nmesh=nmesh, boxsize=boxsize)
         self.slots = []
         self.count = 0
         dev = torch.device("cuda", torch.cuda.current_device())
         for _ in range(slots):
+            # each slot: its own stream and library context, so replays of
+            # different slots share no workspace and can overlap
+            ctx = _lib.Context(dev.index)
+            stream = torch.cuda.Stream(dev)
             pos = torch.empty((int(npart), 3), dtype=torch.float64, device=dev)
             pos.uniform_(0.0, float(boxsize) * (1.0 - 1e-12))
-            for _ in range(2):  # plans, workspaces and pinned buffers at their final sizes
-                mock_pk_bk(pos, None, **self.kw)
-            torch.cuda.synchronize()
-            graph = torch.cuda.CUDAGraph()
-            try:
-                with torch.cuda.graph(graph, capture_error_mode="relaxed"):
-                    fin = mock_pk_bk(pos, None, deferred=True, **self.kw)
-            except Exception as e:  # a host synchronisation or allocation inside the work
-                raise RuntimeError("mock pipeline could not be captured: %s" % e) from e
-            self.slots.append((pos, graph, fin))
+            stream.wait_stream(torch.cuda.current_stream(dev))
+            with _lib.Context.scope(ctx):
+                with torch.cuda.stream(stream):
+                    for _ in range(2):  # plans, workspaces and pinned buffers at their final sizes
+                        mock_pk_bk(pos, None, **self.kw)
+                stream.synchronize()
+                graph = torch.cuda.CUDAGraph()
+                try:
+                    with torch.cuda.graph(graph, stream=stream, capture_error_mode="relaxed"):
+                        fin = mock_pk_bk(pos, None, deferred=True, **self.kw)
+                except Exception as e:  # a host synchronisation or allocation inside the work
+                    raise RuntimeError("mock pipeline could not be captured: %s" % e) from e
+            self.slots.append((pos, graph, fin, stream, ctx))
 
     def submit(self, pos):
-        inp, graph, fin = self.slots[self.count % len(self.slots)]
+        inp, graph, fin, stream, _ = self.slots[self.count % len(self.slots)]
         self.count += 1
         if tuple(pos.shape) != tuple(inp.shape):
             raise ValueError("catalog shape %s differs from the captured %s" % (tuple(pos.shape), tuple(inp.shape)))
-        inp.copy_(pos, non_blocking=True)
-        graph.replay()
-        done = torch.cuda.Event()
-        done.record()
+        stream.wait_stream(torch.cuda.current_stream())  # pos was written on the caller's stream
+        with torch.cuda.stream(stream):
+            inp.copy_(pos, non_blocking=True)
+            graph.replay()
+            done = torch.cuda.Event()
+            done.record()
+        pos.record_stream(stream)
 
         def finalize():
             done.synchronize()
