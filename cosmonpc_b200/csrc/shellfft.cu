@@ -20,7 +20,6 @@
 // T-point DFTs.  Twiddles come from an FP64-computed table rounded to FP32.
 #include <cmath>
 #include <cstring>
-#include <vector>
 
 #include "bins.cuh"
 
@@ -203,15 +202,13 @@ __device__ __forceinline__ unsigned team_mask(int T) {
     return (((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1)));
 }
 
-// Passes 1 and 2: transform kKC in-band columns along one axis.
-//  SYNTH (pass 1): block (s, chunk, item) synthesises its columns over n_x
-//    from the source spectrum, transforms along x, writes A[x][s][chunk].
-//  !SYNTH (pass 2): block (x, chunk, item) loads A[x][s][chunk] over s,
-//    transforms along y, writes B[x][y][chunk].
-template <int T, bool SYNTH>
+// Pass 1: block (s, chunk, item) synthesises kKC in-band columns over n_x
+// from the source spectrum, transforms them along x and writes
+// A[x][s][chunk].
+template <int T>
 __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     const float2 *__restrict__ Aspec, const float2 *__restrict__ Bspec, int n, double L, EdgeSet edges,
-    HarmTable harm, ShellItemsDev items, const float2 *__restrict__ src, float2 *__restrict__ dst) {
+    HarmTable harm, ShellItemsDev items, float2 *__restrict__ dst) {
     constexpr int M = 16 * T, N = 2 * M, H = M / 2;
     constexpr int KC = (kKC < H) ? kKC : H;
     constexpr int LDC = KC + 1;
@@ -225,11 +222,11 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     const int nitems = items.n;
     const int item = blockIdx.x % nitems;
     const int chunk = (blockIdx.x / nitems) % NCH;
-    const int row = blockIdx.x / (nitems * NCH);  // s - 1 (pass 1) or x (pass 2)
+    const int row = blockIdx.x / (nitems * NCH);  // s - 1
     const int kz0 = chunk * KC;
-    if (SYNTH && !tile_live(row + 1 - H, kz0, items.r2max[item])) return;
+    if (!tile_live(row + 1 - H, kz0, items.r2max[item])) return;
     fill_twiddles(tw, N);
-    if (SYNTH) {
+    {
         for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
         __syncthreads();
         const cnpc_shell_item it = items.it[item];
@@ -269,12 +266,6 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
             }
             in[xs * LDC + (nz - kz0)] = v;
         }
-    } else {
-        const float2 *a = src + ((size_t)item * N + row) * M * H;  // A[x = row]
-        for (int e = threadIdx.x; e < M * KC; e += blockDim.x) {
-            const int sl = e / KC, c = e % KC;
-            in[sl * LDC + c] = sl == 0 ? make_float2(0.f, 0.f) : a[(size_t)sl * H + kz0 + c];
-        }
     }
     __syncthreads();
     const int team = threadIdx.x / T, t = threadIdx.x % T, nteams = kColThreads / T;
@@ -300,15 +291,9 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
             }
     }
     __syncthreads();
-    float2 *d;
-    size_t stride;
-    if (SYNTH) {  // A[x][s][kz]
-        d = dst + (size_t)item * N * M * H + (size_t)(row + 1) * H + kz0;
-        stride = (size_t)M * H;
-    } else {      // B[x][y][kz]
-        d = dst + ((size_t)item * N + row) * N * H + kz0;
-        stride = H;
-    }
+    // A[x][s][kz]
+    float2 *d = dst + (size_t)item * N * M * H + (size_t)(row + 1) * H + kz0;
+    const size_t stride = (size_t)M * H;
     for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
         const int p = e / KC, c = e % KC;
         d[p * stride + c] = out[p * LDC + c];
@@ -460,15 +445,14 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     constexpr int KC = kKC < H ? kKC : H;
     constexpr int NCH = H / KC;
     const size_t sc = column_smem<T>(), sr = yz_smem<T>();
-    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T, true>,
+    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc), "shell smem");
     if (st) return st;
     st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)sr), "shell smem");
     if (st) return st;
     const int ni = items.n;
-    shell_column_kernel<T, true><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, nullptr,
-                                                                             workA);
+    shell_column_kernel<T><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, workA);
     shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, O);
     return check_launch(ctx, "shell_fields kernels");
 }
