@@ -119,8 +119,9 @@ static int launch_paint(cnpc_ctx *ctx, const double *pos, const double *w, int64
 // (P+1) x (P+1) column window behind it (P+1 covers the shifted grid), so
 // |sum| <= (max window count) x max|mass| x wmax^3 with wmax the largest 1-D
 // weight of the window (e <= 100).  One particle's deposit is then resolved to
-// (max window count) x 2^-31 of itself; a tile whose window count exceeds
-// 4096 (coarser than 2^-19) accumulates in FP32 instead.
+// (max window count) x 2^-31 of itself, while sums are exact; a tile whose
+// window count exceeds 65536 (coarser than 2^-15 of one deposit) accumulates in
+// FP32 instead.
 constexpr int kTile = 16;
 constexpr int kRegion = kTile + 4;  // nodes [b - 1, b + 3] of a base node b in the tile
 constexpr int kRegionCells = kRegion * kRegion * kRegion;
@@ -308,7 +309,7 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         const double room = 2147483647.0 - (double)s_cmax;
         int e = 100;
         if (bound > 0.0) e = min(100, ilogb(room / bound));
-        RegionAcc acc{reg, ldexpf(1.f, e), s_cmax <= 4096};
+        RegionAcc acc{reg, ldexpf(1.f, e), s_cmax <= 65536};
         for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
             const double4 q = sorted[i];
             int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};

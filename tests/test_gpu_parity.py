@@ -220,12 +220,13 @@ def test_tensor_core_gram_matches_fp64(ncell, na, nb, shared):
         assert err < 4 * err_ff + 1e-7, (err, err_ff)
 
 
-@pytest.mark.parametrize("case", ["clustered", "heavy_one_tile", "light_weights"])
+@pytest.mark.parametrize("case", ["clustered", "heavy_weights", "light_weights", "overfull_cell"])
 def test_tiled_paint_fixed_point_scales(case):
-    """The tiled FP32 paint's per-tile fixed-point scale: a clustered catalog,
-    one tile holding every particle with weights 1e3 (window counts above 4096:
-    FP32 region), and weights of 1e-9 (scale 2^60 and more), against the FP64
-    oracle paint."""
+    """The tiled FP32 paint's per-tile fixed-point scale against the FP64
+    oracle paint: a clustered catalog, weights of 1e3 and of 1e-9 (scale 2^60
+    and more), and 150000 particles in one cell (window count above 65536: the
+    tile accumulates in FP32, so the check is at the level of FP32 sums of
+    1.5e5 deposits)."""
     import torch
     from cosmonpc_b200 import _lib
     from oracle.pmesh_lite import paint_mass
@@ -236,9 +237,12 @@ def test_tiled_paint_fixed_point_scales(case):
         centres = rng.random((40, 3)) * L
         pos = (centres[rng.integers(0, 40, 120000)] + rng.normal(0, 6.0, (120000, 3))) % L
         w = 0.5 + rng.random(len(pos))
-    elif case == "heavy_one_tile":
-        pos = 100.0 + rng.random((60000, 3)) * 150.0  # inside one 16^3-cell tile (cells 10..25)
+    elif case == "heavy_weights":
+        pos = 100.0 + rng.random((60000, 3)) * 150.0
         w = 1e3 * (0.5 + rng.random(len(pos)))
+    elif case == "overfull_cell":
+        pos = 205.0 + rng.random((150000, 3)) * 9.0  # inside cell (20, 20, 20)
+        w = 0.5 + rng.random(len(pos))
     else:
         pos = rng.random((60000, 3)) * L
         w = 1e-9 * (0.5 + rng.random(len(pos)))
@@ -249,8 +253,9 @@ def test_tiled_paint_fixed_point_scales(case):
     for k, shift in enumerate((0.0, 0.5)):
         ref = paint_mass(g + shift, w, [n] * 3, window)
         got = mesh[k].double().cpu().numpy()
-        assert np.max(np.abs(got - ref)) < 2e-6 * np.max(ref), (case, k)
-        assert abs(got.sum() - w.sum()) < 1e-6 * w.sum()
+        tol = 2e-4 if case == "overfull_cell" else 2e-6
+        assert np.max(np.abs(got - ref)) < tol * np.max(ref), (case, k)
+        assert abs(got.sum() - w.sum()) < (1e-4 if case == "overfull_cell" else 1e-6) * w.sum()
 
 
 @pytest.mark.parametrize("ngs,rows,nb,shared", [(2, (20, 20), 20, True), (3, (5, 9, 11), 8, False),
