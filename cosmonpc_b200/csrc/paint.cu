@@ -127,6 +127,10 @@ constexpr int kRegion = kTile + 4;  // nodes [b - 1, b + 3] of a base node b in 
 constexpr int kRegionCells = kRegion * kRegion * kRegion;
 
 __device__ inline int wrapi(int64_t v, int n) {
+    // nodes are within one box length of [0, n) almost always: no 64-bit division
+    if (v >= 0 && v < n) return (int)v;
+    if (v < 0 && v >= -(int64_t)n) return (int)v + n;
+    if (v >= n && v < 2 * (int64_t)n) return (int)(v - n);
     int r = (int)(v % n);
     return r < 0 ? r + n : r;
 }
@@ -264,6 +268,7 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
                                   int tpa, int n, T *mesh, T *mesh_shifted) {
     extern __shared__ int reg[];  // [2][kRegionCells]
     __shared__ int colc[kRegion * kRegion];
+    __shared__ int wrap_t[3][kRegion];  // wrapped mesh index of each region index, per axis
     __shared__ unsigned s_mbits;
     __shared__ int s_cmax;
     const int nreg = mesh_shifted ? 2 : 1;
@@ -275,6 +280,12 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0;
         for (int i = threadIdx.x; i < kRegion * kRegion; i += blockDim.x) colc[i] = 0;
         if (threadIdx.x == 0) s_mbits = 0u, s_cmax = 0;
+        if (threadIdx.x < 3 * kRegion) {
+            // region origin of this tile: tile origin - 1
+            const int ax = threadIdx.x / kRegion, ri = threadIdx.x % kRegion;
+            const int tcoord = ax == 0 ? tile / (tpa * tpa) : (ax == 1 ? (tile / tpa) % tpa : tile % tpa);
+            wrap_t[ax][ri] = wrapi((int64_t)tcoord * kTile - 1 + ri, n);
+        }
         __syncthreads();
         // bound of any node's sum: particles per first-node column, max |mass|
         float mloc = 0.f;
@@ -322,16 +333,13 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         }
         __syncthreads();
         const double unscale = ldexp(1.0, -e);
-        // wrapped origin of the region: tile origin - 1
-        const int tz = tile % tpa, ty = (tile / tpa) % tpa, tx = tile / (tpa * tpa);
-        const int ox = tx * kTile - 1, oy = ty * kTile - 1, oz = tz * kTile - 1;
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
             const int word = reg[i];
             if (word == 0) continue;
             const float v = acc.fixed ? (float)((double)word * unscale) : __int_as_float(word);
             const int r = i % kRegionCells;
             const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
-            const size_t cell = ((size_t)wrapi(ox + rx, n) * n + wrapi(oy + ry, n)) * n + wrapi(oz + rz, n);
+            const size_t cell = ((size_t)wrap_t[0][rx] * n + wrap_t[1][ry]) * n + wrap_t[2][rz];
             atomicAdd((i < kRegionCells ? mesh : mesh_shifted) + cell, (T)v);
         }
     }
