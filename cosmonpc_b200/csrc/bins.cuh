@@ -59,9 +59,19 @@ struct BandIter {
             return mode_of(u, n);
         }
         const int w = 2 * R + 1, nzc = R + 1;
-        const int iz = (int)(u % nzc);
-        const int64_t r = u / nzc;
-        const int jy = (int)(r % w), jx = (int)(r / w);
+        int iz, jy, jx;
+        if (u < ((int64_t)1 << 31)) {
+            uint32_t rz, ry;
+            const uint32_t r = udiv31((uint32_t)u, (uint32_t)nzc, &rz);
+            jx = (int)udiv31(r, (uint32_t)w, &ry);
+            iz = (int)rz;
+            jy = (int)ry;
+        } else {
+            iz = (int)(u % nzc);
+            const int64_t r = u / nzc;
+            jy = (int)(r % w);
+            jx = (int)(r / w);
+        }
         Mode m;
         m.nx = jx - R;
         m.ny = jy - R;

@@ -28,13 +28,41 @@ struct Mode {
     int mult;        // full-space modes represented: 1 on the iz = 0 and iz = n/2 planes
 };
 
+// q = u / d and *rem = u % d for 0 <= u < 2^31, d >= 1, without an integer
+// division: trunc(u * RN(1/d)) in FP64 is within one of the quotient (the
+// reciprocal and the product are accurate to 2^-53 relative), and one
+// correction step makes it exact.  The reciprocal of a loop-invariant d is
+// hoisted out of the caller's loop.
+__device__ __forceinline__ uint32_t udiv31(uint32_t u, uint32_t d, uint32_t *rem) {
+    uint32_t q = (uint32_t)((double)u * (1.0 / (double)d));
+    int64_t r = (int64_t)u - (int64_t)q * d;
+    if (r < 0) {
+        --q;
+        r += d;
+    } else if (r >= d) {
+        ++q;
+        r -= d;
+    }
+    *rem = (uint32_t)r;
+    return q;
+}
+
 __device__ inline Mode mode_of(int64_t t, int n) {
     const int nz2 = n / 2 + 1;
     Mode m;
-    int iz = (int)(t % nz2);
-    int64_t r = t / nz2;
-    int iy = (int)(r % n);
-    int ix = (int)(r / n);
+    int iz, iy, ix;
+    if (t < ((int64_t)1 << 31)) {  // every mode of meshes up to 1024^3
+        uint32_t rz, ry;
+        const uint32_t r = udiv31((uint32_t)t, (uint32_t)nz2, &rz);
+        ix = (int)udiv31(r, (uint32_t)n, &ry);
+        iz = (int)rz;
+        iy = (int)ry;
+    } else {
+        iz = (int)(t % nz2);
+        const int64_t r = t / nz2;
+        iy = (int)(r % n);
+        ix = (int)(r / n);
+    }
     m.nx = ix >= n / 2 ? ix - n : ix;
     m.ny = iy >= n / 2 ? iy - n : iy;
     m.nz = iz;

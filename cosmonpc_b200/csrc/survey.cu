@@ -308,12 +308,10 @@ __global__ void interlace_split_kernel(const cpx_t<T> *s1, const cpx_t<T> *s2, i
     __syncthreads();
     const double H = L / n;
     const double inv_n3 = 1.0 / ((double)n * n * n);
-    const int nz2 = n / 2 + 1;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
-        const int iz = (int)(t % nz2);
-        const int64_t r = t / nz2;
-        const int iy = (int)(r % n), ix = (int)(r / n);
+        const Mode md = mode_of(t, n);  // FFT-order indices; recover the array indices
+        const int ix = md.nx < 0 ? md.nx + n : md.nx, iy = md.ny < 0 ? md.ny + n : md.ny, iz = md.nz;
         const int nx = fft_index_k(ix, n), ny = fft_index_k(iy, n), nzk = fft_index_k(iz, n);
         // phase of k and of -k: (kx H + ky H + kz H) / 2 (mesh_generator.py:211-218)
         const double ph = 0.5 * ((ax.kx(nx) * H + ax.kx(ny) * H) + ax.kx(nzk) * H);
@@ -367,9 +365,19 @@ __global__ void xspace_harmonic_kernel(const T *re, const T *im, int n, double L
     const int64_t cells = (int64_t)n * n * n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += stride) {
-        const int iz = (int)(c % n);
-        const int64_t r = c / n;
-        const int iy = (int)(r % n), ix = (int)(r / n);
+        int iz, iy, ix;
+        if (c < ((int64_t)1 << 31)) {
+            uint32_t rz, ry;
+            const uint32_t r = udiv31((uint32_t)c, (uint32_t)n, &rz);
+            ix = (int)udiv31(r, (uint32_t)n, &ry);
+            iz = (int)rz;
+            iy = (int)ry;
+        } else {
+            iz = (int)(c % n);
+            const int64_t r = c / n;
+            iy = (int)(r % n);
+            ix = (int)(r / n);
+        }
         const double x = xt[ix], y = xt[n + iy], z = xt[2 * n + iz];
         const double rn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
         const double2 yv = harmonic_eval<double>(h, __ddiv_rn(x, rn), __ddiv_rn(y, rn), __ddiv_rn(z, rn), false);
