@@ -3,6 +3,7 @@
 // interlaced +1/2-cell mesh is painted in the same pass.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "common.cuh"
 #include "internal.h"
@@ -197,26 +198,22 @@ __global__ void tile_scatter_kernel(const double *__restrict__ pos, const double
     }
 }
 
-__device__ inline void red_shared_add(float *addr, float v) {
-    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "f"(v) : "memory");
+// no memory clobber: the region is only read after a __syncthreads
+__device__ inline void red_shared_add_nc(int *addr, int v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "r"(v));
 }
-__device__ inline void red_shared_add(int *addr, int v) {
-    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "r"(v) : "memory");
+__device__ inline void red_shared_add_nc(float *addr, float v) {
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(addr)), "f"(v));
 }
 
 // Region accumulator: fixed point (scale 2^e) or, for a tile too heavy for
-// 32 bits, FP32 in the same words.
-struct RegionAcc {
-    int *reg;
-    float scale;
-    bool fixed;
-    __device__ inline void add(int idx, float v) const {
-        if (fixed)
-            red_shared_add(reg + idx, __float2int_rn(v * scale));
-        else
-            red_shared_add(reinterpret_cast<float *>(reg) + idx, v);
-    }
-};
+// 32 bits, FP32 in the same words (FIXED picks one at compile time).
+template <bool FIXED> __device__ __forceinline__ void region_add(int *reg, int idx, float v, float scale) {
+    if (FIXED)
+        red_shared_add_nc(reg + idx, __float2int_rn(v * scale));
+    else
+        red_shared_add_nc(reinterpret_cast<float *>(reg) + idx, v);
+}
 
 // largest 1-D weight of the window: NGP/CIC 1, TSC 3/4, PCS 2/3
 template <int P> __device__ constexpr float window_wmax() { return P <= 2 ? 1.f : (P == 3 ? 0.75f : 0.6666667f); }
@@ -236,8 +233,8 @@ template <int P> __device__ inline int axis_first(double g, float *w) {
 }
 
 // Deposit into a shared region whose index 0 is the unwrapped node org.
-template <int P>
-__device__ inline void deposit_region(const RegionAcc &acc, const int *org, double gx, double gy, double gz,
+template <int P, bool FIXED>
+__device__ inline void deposit_region(int *reg, float scale, const int *org, double gx, double gy, double gz,
                                       float mass) {
     float wx[P], wy[P], wz[P];
     const int bx = axis_first<P>(gx, wx) - org[0];
@@ -250,7 +247,7 @@ __device__ inline void deposit_region(const RegionAcc &acc, const int *org, doub
         for (int b = 0; b < P; ++b) {
             const float wab = mass * wx[a] * wy[b];
 #pragma unroll
-            for (int c = 0; c < P; ++c) acc.add(base + (a * kRegion + b) * kRegion + c, wab * wz[c]);
+            for (int c = 0; c < P; ++c) region_add<FIXED>(reg, base + (a * kRegion + b) * kRegion + c, wab * wz[c], scale);
         }
     }
 }
@@ -320,23 +317,29 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         const double room = 2147483647.0 - (double)s_cmax;
         int e = 100;
         if (bound > 0.0) e = min(100, ilogb(room / bound));
-        RegionAcc acc{reg, ldexpf(1.f, e), s_cmax <= 65536};
-        for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
-            const double4 q = sorted[i];
-            int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};
-            deposit_region<P>(acc, org, q.x, q.y, q.z, (float)q.w);
-            if (mesh_shifted) {
-                const RegionAcc acc2{reg + kRegionCells, acc.scale, acc.fixed};
-                deposit_region<P>(acc2, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5), __dadd_rn(q.z, 0.5),
-                                  (float)q.w);
+        const float scale = ldexpf(1.f, e);
+        const bool fixed = s_cmax <= 65536;
+        auto deposit_all = [&](auto fixed_tag) {
+            constexpr bool F = decltype(fixed_tag)::value;
+            for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+                const double4 q = sorted[i];
+                int org[3] = {region_origin(q.x, n), region_origin(q.y, n), region_origin(q.z, n)};
+                deposit_region<P, F>(reg, scale, org, q.x, q.y, q.z, (float)q.w);
+                if (mesh_shifted)
+                    deposit_region<P, F>(reg + kRegionCells, scale, org, __dadd_rn(q.x, 0.5), __dadd_rn(q.y, 0.5),
+                                         __dadd_rn(q.z, 0.5), (float)q.w);
             }
-        }
+        };
+        if (fixed)
+            deposit_all(std::true_type{});
+        else
+            deposit_all(std::false_type{});
         __syncthreads();
         const double unscale = ldexp(1.0, -e);
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
             const int word = reg[i];
             if (word == 0) continue;
-            const float v = acc.fixed ? (float)((double)word * unscale) : __int_as_float(word);
+            const float v = fixed ? (float)((double)word * unscale) : __int_as_float(word);
             const int r = i % kRegionCells;
             const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
             const size_t cell = ((size_t)wrap_t[0][rx] * n + wrap_t[1][ry]) * n + wrap_t[2][rz];
