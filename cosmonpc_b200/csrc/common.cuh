@@ -97,7 +97,9 @@ __device__ inline double knorm_exact(const Mode &m, double boxsize, double *kx, 
 __device__ inline int find_bin(double v, const double *e, int nedges) {
     if (!(v >= e[0]) || !(v < e[nedges - 1])) return -1;
     const int nb = nedges - 1;
-    int b = (int)((v - e[0]) * nb / (e[nb] - e[0]));
+    // first guess from the mean bin width (a loop-invariant reciprocal, hoisted
+    // by the compiler); the two walks below make the bin exact
+    int b = (int)((v - e[0]) * ((double)nb / (e[nb] - e[0])));
     b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
     while (b > 0 && v < e[b]) --b;
     while (b < nb - 1 && v >= e[b + 1]) ++b;
