@@ -47,6 +47,39 @@ __device__ inline void warp_bin_add(double *s, int bin, double v) {
     }
 }
 
+// Sum V values per bin over the lanes of a warp, value i of bin b into
+// s[b + i * stride] (all 32 lanes must call; bin < 0 means "no contribution").
+// Consecutive modes along n_z meet the bins in increasing order, so equal bins
+// sit in runs of adjacent lanes: a segmented inclusive scan sums each run and
+// the run's last lane adds it, at a cost that does not grow with the number of
+// bins a warp meets.  Any bin pattern gives the right sums (a bin split over
+// several runs is added once per run).
+template <int V>
+__device__ inline void warp_run_add(double *s, int stride, int bin, double (&v)[V], int nv = V) {
+    const unsigned full = 0xffffffffu;
+    if (__ballot_sync(full, bin >= 0) == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(full, bin, 1);
+    const unsigned heads = __ballot_sync(full, lane == 0 || prev != bin);
+    // first lane of this lane's run: the highest head at or below it (bit 0 is a head)
+    const int start = 31 - __clz(heads & (full >> (31 - lane)));
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const bool take = lane - o >= start;
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            if (i >= nv) break;
+            const double y = __shfl_up_sync(full, v[i], o);
+            if (take) v[i] += y;
+        }
+    }
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (tail && bin >= 0)
+#pragma unroll
+        for (int i = 0; i < V; ++i)
+            if (i < nv) atomicAdd(&s[bin + i * stride], v[i]);
+}
+
 // Modes of the half spectrum with every |n_d| <= R (R < n/2): a compact index
 // u over n_x, n_y in [-R, R], n_z in [0, R].  Shell sums only see modes below
 // their last edge, so they iterate over that cube (R = -1: every mode).

@@ -69,8 +69,8 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
             bin = find_bin(kn, edges.e, edges.n);
             mult = m.mult;
         }
-        warp_bin_add(bins, bin, mult);
-        warp_bin_add(bins + nb, bin, mult * kn);
+        double v[2] = {mult, mult * kn};
+        warp_run_add<2>(bins, nb, bin, v);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
@@ -117,17 +117,25 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                     mu = (kx / kn) * poles.los[0] + (ky / kn) * poles.los[1] + (kz / kn) * poles.los[2];
             }
         }
-        for (int q = 0; q < poles.n; ++q) {
-            // Legendre P_l(mu) by the three-term recurrence
-            const int l = poles.l[q];
-            double p0 = 1.0, p1 = mu;
-            double pl = (l == 0) ? 1.0 : mu;
-            for (int j = 1; j < l; ++j) {
-                pl = ((2 * j + 1) * mu * p1 - j * p0) / (j + 1);
-                p0 = p1;
-                p1 = pl;
+        // poles in groups of four (a warp-uniform loop)
+        for (int q0 = 0; q0 < poles.n; q0 += 4) {
+            const int nq = poles.n - q0 < 4 ? poles.n - q0 : 4;
+            double v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q >= nq) break;
+                // Legendre P_l(mu) by the three-term recurrence
+                const int l = poles.l[q0 + q];
+                double p0 = 1.0, p1 = mu;
+                double pl = (l == 0) ? 1.0 : mu;
+                for (int j = 1; j < l; ++j) {
+                    pl = ((2 * j + 1) * mu * p1 - j * p0) / (j + 1);
+                    p0 = p1;
+                    p1 = pl;
+                }
+                v[q] = pv * pl;
             }
-            warp_bin_add(bins + q * nb, bin, pv * pl);
+            warp_run_add<4>(bins + q0 * nb, nb, bin, v, nq);
         }
     }
     __syncthreads();
@@ -187,7 +195,8 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                 source[t] = mk<T>((T)0, (T)0);
             }
         }
-        warp_bin_add(bins, bin, val);
+        double v[1] = {val};
+        warp_run_add<1>(bins, 0, bin, v);
         if (source) warp_bin_add(bins, in_band ? nb : -1, tot);
     }
     __syncthreads();

@@ -506,8 +506,8 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
                 acci *= weight;
             }
         }
-        warp_bin_add(bins, bin, accr);
-        warp_bin_add(bins + nb, bin, acci);
+        double v[2] = {accr, acci};
+        warp_run_add<2>(bins, nb, bin, v);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
