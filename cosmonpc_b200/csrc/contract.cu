@@ -286,6 +286,8 @@ constexpr int kFfWarps = 8;
 constexpr int kFfChunk = 256;  // cells per block chunk (32 per warp)
 constexpr int kFfRow = 36;     // padded slab row (32 cells + 4)
 constexpr int kFfFold = 4;     // chunks per FP32 partial (128 cells per lane)
+constexpr int kFfMaxRows = 80;  // staged rows: <= 4 weights + 48 A + 24 B
+constexpr int kFfTable = kFfMaxRows * 8;  // bytes of the row-source table ahead of the slabs
 
 __device__ inline void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
@@ -312,24 +314,30 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
     const int warp = threadIdx.x >> 5;
     const int nrows = P.nunion;  // staged rows: G, A window, separate B window
     const int slab = nrows * kFfRow;
-    float *const buf0 = reinterpret_cast<float *>(smem_raw) + (size_t)warp * NBUF * slab;
+    // the block's table of staged-row sources (nullptr: padding row), then the slabs
+    const float **rowsrc = reinterpret_cast<const float **>(smem_raw);
+    float *const buf0 = reinterpret_cast<float *>(smem_raw + kFfTable) + (size_t)warp * NBUF * slab;
     const int64_t nchunk_all = (P.ncell + kFfChunk - 1) / kFfChunk;
     const int nchunk = blockIdx.x < nchunk_all ? (int)((nchunk_all - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+    for (int u = threadIdx.x; u < nrows; u += blockDim.x) {
+        const int f = P.union_field[u];
+        rowsrc[u] = f >= 0 ? fields + (int64_t)f * P.field_stride : (f == -1 ? nullptr : (MG ? X.g[-2 - f] : g));
+    }
+    __syncthreads();
 
-    // stream this warp's 32-cell slab of chunk k into buffer b
+    // stream this warp's 32-cell slab of chunk k into buffer b: lane l copies
+    // the 16 bytes (l % 8) of rows l / 8 + 4 j
+    const int part = lane & 7, row0 = lane >> 3;
     auto issue = [&](int k, int b) {
-        const int64_t c0 = ((int64_t)blockIdx.x + (int64_t)k * gridDim.x) * kFfChunk + warp * 32;
-        float *dst = buf0 + b * slab;
-        for (int idx = lane; idx < nrows * 8; idx += 32) {
-            const int row = idx >> 3, part = idx & 7;
-            const int f = P.union_field[row];
-            if (f == -1) continue;  // padding row: only feeds discarded outputs
-            const int64_t cell = c0 + part * 4;
-            float *d = dst + row * kFfRow + part * 4;
-            const float *src = f >= 0 ? fields + (int64_t)f * P.field_stride : (MG ? X.g[-2 - f] : g);
-            if (cell < P.ncell)  // ncell is a multiple of 4, so the 16 bytes are all valid
-                cp_async16(d, src + cell);
-            else
+        const int64_t cell = ((int64_t)blockIdx.x + (int64_t)k * gridDim.x) * kFfChunk + warp * 32 + part * 4;
+        float *d = buf0 + b * slab + row0 * kFfRow + part * 4;
+        if (cell < P.ncell) {  // ncell is a multiple of 4, so the 16 bytes are all valid
+            for (int row = row0; row < nrows; row += 4, d += 4 * kFfRow) {
+                const float *src = rowsrc[row];
+                if (src != nullptr) cp_async16(d, src + cell);  // padding rows only feed discarded outputs
+            }
+        } else {
+            for (int row = row0; row < nrows; row += 4, d += 4 * kFfRow)
                 *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         cp_async_commit();
@@ -445,7 +453,7 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
     const int b_base = b_off >= 0 ? ngs + b_off : (int)rows.size();
     if (b_off < 0)
         for (int j = 0; j < pl->wc; ++j) rows.push_back(j < nb ? b[j] : -1);
-    if ((int)rows.size() > kMaxUnion) return false;
+    if ((int)rows.size() > kFfMaxRows) return false;
     P.nunion = (int)rows.size();
     for (int u = 0; u < P.nunion; ++u) P.union_field[u] = rows[u];
     P.g_row = 0;
@@ -455,8 +463,8 @@ static bool ff_plan(int64_t ncell, int64_t stride, const int *a, int na, const i
     P.field_stride = stride;
     // two blocks per SM: ~110 KB of slabs each
     const size_t per_buf = (size_t)kFfWarps * P.nunion * kFfRow * sizeof(float);
-    pl->nbuf = (int)std::min<size_t>(4, (110 * 1024) / per_buf);
-    pl->smem = pl->nbuf * per_buf;
+    pl->nbuf = (int)std::min<size_t>(4, (110 * 1024 - kFfTable) / per_buf);
+    pl->smem = kFfTable + pl->nbuf * per_buf;
     return pl->nbuf >= 2;
 }
 
