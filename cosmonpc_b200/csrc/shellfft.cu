@@ -118,34 +118,44 @@ __device__ __forceinline__ void idft16(float2 *v) {
     for (int i = 0; i < 16; ++i) v[i] = o[i];
 }
 
-// Exchange slots of one team: 16 rows of T + 1 (the pad makes the transposed
-// reads conflict-free), and a team stride of 9 (mod 16) float2 so that the
-// four teams of a warp fall on disjoint bank pairs two by two.
+// Exchange slots of one team: 16 rows of T float2, element (k1, c) at
+// k1 T + (c ^ ((k1 / (16 / T)) % T)), and a team stride of T (mod 16) float2.
+// The row writes (fixed k1, c = t) and the transposed reads (k1 = t 16/T + q,
+// fixed c) of the teams of a warp then hit every bank pair exactly twice: no
+// bank conflicts for T = 2, 4, 8.
 template <int T> struct Exch {
-    static constexpr int kRow = T + 1;
-    static constexpr int kStride = 16 * (T + 1) + 9;
+    static constexpr int kStride = 17 * T;
 };
+
+// Per-thread twiddles of team_fft, [k1 - 1][t] = W_M^{t k1} (k1 = 1..15): the
+// T threads of a team read T consecutive slots.
+template <int T> __host__ __device__ constexpr int team_twiddles() { return 15 * T; }
+template <int T> __device__ __forceinline__ void fill_team_twiddles(float2 *twt, const float2 *tw) {
+    for (int e = threadIdx.x; e < 15 * T; e += blockDim.x) {
+        const int k1 = e / T + 1, t = e % T;
+        twt[e] = tw[2 * ((t * k1) % (16 * T))];
+    }
+}
 
 // Team FFT of size M = 16 T (inverse).  On entry thread t of the team holds
 // u[j] = x[T j + t]; on exit it holds X[k1 + 16 k2] for k1 = t (16/T) + q
 // (q < 16/T), k2 < T, stored as u[q * T + k2].  ex: the team's exchange slots
-// (Exch<T>); tw: W_n table (n = 2M entries; W_M^j = tw[2 j]).
+// (Exch<T>); twt: the per-thread twiddle table (fill_team_twiddles).
 template <int T>
-__device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const float2 *tw, unsigned mask) {
-    constexpr int R = Exch<T>::kRow;
+__device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const float2 *twt, unsigned mask) {
+    constexpr int Q = 16 / T;
     idft16(u);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) u[k1] = cmul(u[k1], tw[2 * ((t * k1) % (16 * T))]);
+    for (int k1 = 1; k1 < 16; ++k1) u[k1] = cmul(u[k1], twt[(k1 - 1) * T + t]);
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) ex[k1 * R + t] = u[k1];
+    for (int k1 = 0; k1 < 16; ++k1) ex[k1 * T + (t ^ ((k1 / Q) % T))] = u[k1];
     __syncwarp(mask);
-    constexpr int Q = 16 / T;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int k1 = t * Q + q;
         float2 w[T];
 #pragma unroll
-        for (int i = 0; i < T; ++i) w[i] = ex[k1 * R + i];
+        for (int i = 0; i < T; ++i) w[i] = ex[k1 * T + (i ^ t)];
         if (T == 2) idft2(w[0], w[1]);
         if (T == 4) idft4(w[0], w[1], w[2], w[3]);
         if (T == 8) idft8(w);
@@ -218,7 +228,8 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     float2 *out = in + M * LDC;                      // [N][LDC]
     float2 *tw = out + N * LDC;                      // [N]
     float2 *ex = tw + N;                             // [teams][Exch<T>::kStride]
-    double *kt = reinterpret_cast<double *>(ex + (kColThreads / T) * Exch<T>::kStride);  // [n + 1]
+    float2 *twt = ex + (kColThreads / T) * Exch<T>::kStride;                  // [15 T]
+    double *kt = reinterpret_cast<double *>(twt + team_twiddles<T>());        // [n + 1]
     const int nitems = items.n;
     const int item = blockIdx.x % nitems;
     const int chunk = (blockIdx.x / nitems) % NCH;
@@ -229,6 +240,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     {
         for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
         __syncthreads();
+        fill_team_twiddles<T>(twt, tw);  // first read after the barrier below
         const cnpc_shell_item it = items.it[item];
         const cnpc_harmonic &hm = harm.h[it.harmonic];
         const int s = row + 1;
@@ -281,7 +293,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
             if (r) v = cmul(v, tw[slot]);
             u[j] = v;
         }
-        team_fft<T>(u, t, tex, tw, mask);
+        team_fft<T>(u, t, tex, twt, mask);
 #pragma unroll
         for (int q = 0; q < 16 / T; ++q)
 #pragma unroll
@@ -313,7 +325,8 @@ template <int T> struct YZLayout {
     static constexpr int M = 16 * T, N = 2 * M, H = M / 2, LD = H + 1;
     static constexpr int TEAMS = kYZThreads / T;
     static constexpr int kEx = N;                                    // after the twiddles
-    static constexpr int kB = ((kEx + TEAMS * Exch<T>::kStride + 1) / 2) * 2;
+    static constexpr int kTwt = kEx + TEAMS * Exch<T>::kStride;      // team twiddles
+    static constexpr int kB = ((kTwt + team_twiddles<T>() + 1) / 2) * 2;
     static constexpr int kTotal = kB + M * LD;                       // float2
 };
 
@@ -337,7 +350,10 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     const int item = blockIdx.x % nitems;
     const int ry = (blockIdx.x / nitems) & 1;
     const int x = blockIdx.x / (2 * nitems);
+    float2 *twt = tw + YL::kTwt;
     fill_twiddles(tw, N);
+    __syncthreads();
+    fill_team_twiddles<T>(twt, tw);
     __syncthreads();
     const int team = threadIdx.x / T, t = threadIdx.x % T;
     const unsigned mask = team_mask(T);
@@ -358,7 +374,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             if (ry) v = cmul(v, tw[slot]);
             u[j] = v;
         }
-        team_fft<T>(u, t, tex, tw, mask);
+        team_fft<T>(u, t, tex, twt, mask);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
 #pragma unroll
@@ -401,7 +417,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             float2 u[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) u[j] = rz ? cmul(v[j], tw[T * j + t]) : v[j];
-            team_fft<T>(u, t, tex, tw, mask);
+            team_fft<T>(u, t, tex, twt, mask);
 #pragma unroll
             for (int i = 0; i < 16; ++i) res[rz][i] = u[i];
         }
@@ -432,7 +448,8 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
 // ------------------------------------------------------------ dispatch
 template <int T> static size_t column_smem() {
     const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
-    return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride) +
+    return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride +
+                             team_twiddles<T>()) +
            sizeof(double) * (N + 1);
 }
 template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLayout<T>::kTotal; }
