@@ -29,6 +29,14 @@ inline int grid_for(cnpc_ctx *ctx, int64_t work, int threads, int per_sm = 8) {
     return (int)(want < cap ? want : cap);
 }
 
+// Copy the edges to shared memory (a __syncthreads() follows before use):
+// find_bin indexes them at run time, which on a by-value kernel parameter is a
+// constant-bank load through the slow address-divergence path for every probe.
+__device__ inline double *edges_to_shared(double *s, const EdgeSet &es) {
+    for (int i = threadIdx.x; i < es.n; i += blockDim.x) s[i] = es.e[i];
+    return s;
+}
+
 // Sum v into bins s[bin] over the lanes of a warp (all 32 lanes must call;
 // bin < 0 means "no contribution").
 __device__ inline void warp_bin_add(double *s, int bin, double v) {

@@ -230,6 +230,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     float2 *ex = tw + N;                             // [teams][Exch<T>::kStride]
     float2 *twt = ex + (kColThreads / T) * Exch<T>::kStride;                  // [15 T]
     double *kt = reinterpret_cast<double *>(twt + team_twiddles<T>());        // [n + 1]
+    double *se = kt + (n + 1);                                                 // [edges.n]
     const int nitems = items.n;
     const int item = blockIdx.x % nitems;
     const int chunk = (blockIdx.x / nitems) % NCH;
@@ -239,10 +240,13 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     fill_twiddles(tw, N);
     {
         for (int i = threadIdx.x; i <= n; i += blockDim.x) kt[i] = kcomp(i - n / 2, L);
+        // edges and the harmonic are read at run-time indices: shared copies
+        edges_to_shared(se, edges);
+        __shared__ cnpc_harmonic hm;
+        const cnpc_shell_item it = items.it[item];
+        if (threadIdx.x == 0) hm = harm.h[it.harmonic];
         __syncthreads();
         fill_team_twiddles<T>(twt, tw);  // first read after the barrier below
-        const cnpc_shell_item it = items.it[item];
-        const cnpc_harmonic &hm = harm.h[it.harmonic];
         const int s = row + 1;
         const int ny = s - H;
         const int iy = ny < 0 ? ny + n : ny;
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
                 const int ix = nx < 0 ? nx + n : nx;
                 const double kx = kt[nx + n / 2], ky = kt[ny + n / 2], kz = kt[nz + n / 2];
                 const double kn = knorm_from(kx, ky, kz);
-                if (find_bin(kn, edges.e, edges.n) == it.bin) {
+                if (find_bin(kn, se, edges.n) == it.bin) {
                     const bool origin = kn == 0.0;
                     const double ik = origin ? 0.0 : 1.0 / kn;
                     float2 Y = harmonic_eval<float>(hm, (float)(kx * ik), (float)(ky * ik), (float)(kz * ik), origin);
@@ -446,11 +450,11 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
 }
 
 // ------------------------------------------------------------ dispatch
-template <int T> static size_t column_smem() {
+template <int T> static size_t column_smem(int nedges) {
     const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
     return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride +
                              team_twiddles<T>()) +
-           sizeof(double) * (N + 1);
+           sizeof(double) * (N + 1 + nedges);
 }
 template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLayout<T>::kTotal; }
 
@@ -461,7 +465,7 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     constexpr int M = 16 * T, N = 2 * M, H = M / 2;
     constexpr int KC = kKC < H ? kKC : H;
     constexpr int NCH = H / KC;
-    const size_t sc = column_smem<T>(), sr = yz_smem<T>();
+    const size_t sc = column_smem<T>(es.n), sr = yz_smem<T>();
     int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc), "shell smem");
     if (st) return st;

@@ -53,6 +53,7 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
     double *bins = sm + (n + 1);
     const int nb = edges.n - 1;
+    const double *e = edges_to_shared(bins + 2 * nb, edges);
     for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -66,7 +67,7 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
             int64_t tt;
             const Mode m = bi.mode(t, &tt);
             kn = knorm_from(ax.kx(m.nx), ax.kx(m.ny), ax.kx(m.nz));
-            bin = find_bin(kn, edges.e, edges.n);
+            bin = find_bin(kn, e, edges.n);
             mult = m.mult;
         }
         double v[2] = {mult, mult * kn};
@@ -95,6 +96,7 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
     double *bins = sm + (n + 1);
     const int nb = edges.n - 1;
+    const double *e = edges_to_shared(bins + poles.n * nb, edges);
     for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -109,7 +111,7 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
             const Mode m = bi.mode(t, &tt);
             const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
             const double kn = knorm_from(kx, ky, kz);
-            bin = find_bin(kn, edges.e, edges.n);
+            bin = find_bin(kn, e, edges.n);
             if (bin >= 0) {
                 const cpx_t<T> va = a[tt], vb = b[tt];
                 pv = m.mult * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
@@ -155,6 +157,9 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
     const int nb = edges.n - 1;
     // with a source, bins[nb] collects the full-space sum of the source (its x = 0 value)
     const int nbt = source ? nb + 1 : nb;
+    const double *e = edges_to_shared(bins + nbt, edges);
+    __shared__ cnpc_harmonic s_y;  // read at run-time indices by harmonic_eval
+    if (threadIdx.x == 0) s_y = yl0;
     for (int i = threadIdx.x; i < nbt; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -169,7 +174,7 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
             const Mode m = mode_of(t, n);
             const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
             const double kn = knorm_from(kx, ky, kz);
-            bin = find_bin(kn, edges.e, edges.n);
+            bin = find_bin(kn, e, edges.n);
             const bool keep = !(band > 0.0) || kn < band;
             if (bin >= 0 || (source && keep)) {
                 const cpx_t<T> va = a[t], vb = b[t];
@@ -187,7 +192,7 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
                     if (use_y) {
                         const bool origin = kn == 0.0;
                         const double ik = origin ? 0.0 : 1.0 / kn;
-                        y = harmonic_eval<double>(yl0, kx * ik, ky * ik, kz * ik, origin).x;
+                        y = harmonic_eval<double>(s_y, kx * ik, ky * ik, kz * ik, origin).x;
                     }
                     val = m.mult * pr * y;
                 }
@@ -212,6 +217,12 @@ __global__ void shell_spectra_kernel(const cpx_t<T> *A, const cpx_t<T> *B, int n
     extern __shared__ double tbl[];
     AxisTable ax;
     fill_axis_table(ax, tbl, n, L, CNPC_COMP_NONE, 1);
+    // edges, harmonics and items in shared memory: all are read at run-time indices
+    const double *e = edges_to_shared(tbl + (n + 1), edges);
+    cnpc_harmonic *sh = reinterpret_cast<cnpc_harmonic *>(tbl + (n + 1) + CNPC_MAX_EDGES);
+    cnpc_shell_item *si = reinterpret_cast<cnpc_shell_item *>(sh + harm.n);
+    for (int i = threadIdx.x; i < harm.n; i += blockDim.x) sh[i] = harm.h[i];
+    for (int i = threadIdx.x; i < items.n; i += blockDim.x) si[i] = items.it[i];
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const cpx_t<T> zero = mk<T>((T)0, (T)0);
@@ -219,7 +230,7 @@ __global__ void shell_spectra_kernel(const cpx_t<T> *A, const cpx_t<T> *B, int n
         const Mode m = mode_of(t, n);
         const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
         const double kn = knorm_from(kx, ky, kz);
-        const int bin = find_bin(kn, edges.e, edges.n);
+        const int bin = find_bin(kn, e, edges.n);
         if (bin < 0) {
             for (int j = 0; j < items.n; ++j) out[(int64_t)j * nh + t] = zero;
             continue;
@@ -228,10 +239,10 @@ __global__ void shell_spectra_kernel(const cpx_t<T> *A, const cpx_t<T> *B, int n
         const double ik = origin ? 0.0 : 1.0 / kn;
         const T x = (T)(kx * ik), y = (T)(ky * ik), z = (T)(kz * ik);
         for (int j = 0; j < items.n; ++j) {
-            const cnpc_shell_item it = items.it[j];
+            const cnpc_shell_item it = si[j];
             cpx_t<T> v = zero;
             if (it.bin == bin) {
-                const cnpc_harmonic &h = harm.h[it.harmonic];
+                const cnpc_harmonic &h = sh[it.harmonic];
                 cpx_t<T> Y = harmonic_eval<T>(h, x, y, z, origin);
                 if (it.conj) Y.y = -Y.y;
                 // phi = Re Y / Im Y (even l) or i Im Y / -i Re Y (odd l)
@@ -302,7 +313,7 @@ int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges
     const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
     const int64_t nh = bi.count;
     const int threads = 256;
-    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, (n + 1 + 2 * nb) * sizeof(double), s>>>(
+    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, (n + 1 + 2 * nb + nedges) * sizeof(double), s>>>(
         n, boxsize, es, d_counts, d_ksum, bi);
     return check_launch(ctx, "kbin_counts_kernel");
 }
@@ -331,7 +342,7 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
     const int64_t nh = bi.count;
     const int threads = 256;
-    const size_t smem = sizeof(double) * (n + 1 + nb * npoles);
+    const size_t smem = sizeof(double) * (n + 1 + nb * npoles + nedges);
     if (dtype == CNPC_F32)
         pk_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ps, d_sums, bi);
@@ -365,7 +376,7 @@ int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     if (st) return st;
     const int64_t nh = half_modes(n);
     const int threads = 256;
-    const size_t smem = sizeof(double) * (2 * (n + 1) + nbt);
+    const size_t smem = sizeof(double) * (2 * (n + 1) + nbt + nedges);
     if (dtype == CNPC_F32)
         sn_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, volume_sq, sn0, window,
@@ -413,12 +424,14 @@ int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize, const vo
     const int64_t nh = half_modes(n);
     const int threads = 256;
     cudaStream_t s = (cudaStream_t)stream;
+    const size_t smem = (n + 1 + CNPC_MAX_EDGES) * sizeof(double) + nharmonics * sizeof(cnpc_harmonic) +
+                        nitems * sizeof(cnpc_shell_item);  // < 48 KB for n <= 2048
     if (dtype == CNPC_F32)
-        shell_spectra_kernel<float><<<grid_for(ctx, nh, threads), threads, (n + 1) * sizeof(double), s>>>(
+        shell_spectra_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, es, ht, itab,
             (float2 *)d_out, nh);
     else
-        shell_spectra_kernel<double><<<grid_for(ctx, nh, threads), threads, (n + 1) * sizeof(double), s>>>(
+        shell_spectra_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, es, ht, itab,
             (double2 *)d_out, nh);
     return check_launch(ctx, "shell_spectra_kernel");

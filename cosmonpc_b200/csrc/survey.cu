@@ -219,6 +219,9 @@ struct YlmSet {
 __global__ void particle_sums_kernel(int64_t np, const double *pos, const double *w, const double *wfkp,
                                      const double *nz, YlmSet ylm, double *partial) {
     const int nsum = CNPC_PSUM_COUNT + 2 * ylm.n;
+    __shared__ cnpc_harmonic s_h[CNPC_MAX_HARMONICS];  // read at run-time indices
+    for (int q = threadIdx.x; q < ylm.n; q += blockDim.x) s_h[q] = ylm.h[q];
+    __syncthreads();
     double acc[CNPC_PSUM_COUNT + 2 * CNPC_MAX_HARMONICS];
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = 0; i < nsum; ++i) acc[i] = 0.0;
@@ -239,7 +242,7 @@ __global__ void particle_sums_kernel(int64_t np, const double *pos, const double
             const double xh = x / r, yh = y / r, zh = z / r;
             const double w3 = wf * wf * wf;
             for (int q = 0; q < ylm.n; ++q) {
-                const double2 yv = harmonic_eval<double>(ylm.h[q], xh, yh, zh, false);
+                const double2 yv = harmonic_eval<double>(s_h[q], xh, yh, zh, false);
                 acc[CNPC_PSUM_COUNT + 2 * q] += w3 * yv.x;
                 acc[CNPC_PSUM_COUNT + 2 * q + 1] -= w3 * yv.y;  // conj(Y)
             }
@@ -361,6 +364,8 @@ __global__ void xspace_harmonic_kernel(const T *re, const T *im, int n, double L
         const double off = __dadd_rn(__ddiv_rn(half, (double)n), bc[d]);
         xt[i] = __dadd_rn(xi, off);
     }
+    __shared__ cnpc_harmonic s_h;  // read at run-time indices by harmonic_eval
+    if (threadIdx.x == 0) s_h = h;
     __syncthreads();
     const int64_t cells = (int64_t)n * n * n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -380,7 +385,7 @@ __global__ void xspace_harmonic_kernel(const T *re, const T *im, int n, double L
         }
         const double x = xt[ix], y = xt[n + iy], z = xt[2 * n + iz];
         const double rn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
-        const double2 yv = harmonic_eval<double>(h, __ddiv_rn(x, rn), __ddiv_rn(y, rn), __ddiv_rn(z, rn), false);
+        const double2 yv = harmonic_eval<double>(s_h, __ddiv_rn(x, rn), __ddiv_rn(y, rn), __ddiv_rn(z, rn), false);
         const double yr = yv.x, yi = conj ? -yv.y : yv.y;
         const double fr = (double)re[c], fi = im ? (double)im[c] : 0.0;
         out_re[c] = (T)(scale * (fr * yr - fi * yi));
@@ -461,6 +466,9 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
     const int ntab = 1 + __popc(kinds & 0xeu);
     double *bins = sm + ntab * (n + 1);
     const int nb = edges.n - 1;
+    const double *e = edges_to_shared(bins + 2 * nb, edges);
+    __shared__ cnpc_harmonic s_z;  // read at run-time indices by harmonic_eval
+    if (threadIdx.x == 0) s_z = zh;
     for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -475,7 +483,7 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
             const Mode m = bi.mode(t, &tt);
             const double kx = ct.k[m.nx + ct.half], ky = ct.k[m.ny + ct.half], kz = ct.k[m.nz + ct.half];
             const double kn = knorm_from(kx, ky, kz);
-            bin = find_bin(kn, edges.e, edges.n);
+            bin = find_bin(kn, e, edges.n);
             if (bin >= 0) {
                 double2 uk, um, vk, vm;
                 load_operand<T>(u, tt, ct.factor(u.comp, m.nx, m.ny, m.nz), &uk, &um);
@@ -485,7 +493,7 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
                 int parity = 1;
                 if (has_z) {
                     const bool origin = kn == 0.0;
-                    const double2 z = harmonic_eval<double>(zh, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
+                    const double2 z = harmonic_eval<double>(s_z, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
                                                             origin ? 0.0 : kz / kn, origin);
                     zr = z.x;
                     zi = conj_z ? -z.y : z.y;
@@ -561,6 +569,8 @@ __global__ void hermitian_accumulate_kernel(OperandDev x, int n, double L, int p
     extern __shared__ double sm[];
     CompTables ct;
     fill_comp_tables(ct, sm, n, L, p, kinds);
+    __shared__ cnpc_harmonic s_z;  // read at run-time indices by harmonic_eval
+    if (threadIdx.x == 0) s_z = zh;
     __syncthreads();
     const int parity = (zh.l & 1) ? -1 : 1;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -569,7 +579,7 @@ __global__ void hermitian_accumulate_kernel(OperandDev x, int n, double L, int p
         const double kx = ct.k[m.nx + ct.half], ky = ct.k[m.ny + ct.half], kz = ct.k[m.nz + ct.half];
         const double kn = knorm_from(kx, ky, kz);
         const bool origin = kn == 0.0;
-        const double2 y = harmonic_eval<double>(zh, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
+        const double2 y = harmonic_eval<double>(s_z, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
                                                 origin ? 0.0 : kz / kn, origin);
         double2 xk, xm;
         load_operand<T>(x, t, ct.factor(x.comp, m.nx, m.ny, m.nz), &xk, &xm);
@@ -835,7 +845,7 @@ int cnpc_survey_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window
     const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
     const int64_t nh = bi.count;
     const int threads = 256;
-    const size_t smem = sizeof(double) * (ntab * (n + 1) + 2 * nb);
+    const size_t smem = sizeof(double) * (ntab * (n + 1) + 2 * nb + nedges);
     if (dtype == CNPC_F32)
         survey_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
             du, dv, n, boxsize, window, kinds, sbar_re, sbar_im, h_z ? 1 : 0, zh, conj_z, weight, es, d_sums, bi);
