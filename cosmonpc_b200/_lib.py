@@ -29,7 +29,7 @@ EXPORTED = (
     "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
-    "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g",
+    "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -94,6 +94,8 @@ _SIGS = {
     "cnpc_pk_bins": [_vp, _i, _i, _d, _vp, _vp, _dp, _i, _ip, _i, _dp, _vp, _vp],
     "cnpc_sn_bins": [_vp, _i, _i, _d, _vp, _vp, _d, _d, _i, ctypes.POINTER(Harmonic), _dp, _i,
                      _vp, _vp, _d, _vp],
+    "cnpc_sn_bins_multi": [_vp, _i, _i, _d, _vp, _vp, _d, _i, _i, _dp, ctypes.POINTER(ctypes.POINTER(Harmonic)),
+                           _dp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _d, _vp],
     "cnpc_shell_spectra": [_vp, _i, _i, _d, _vp, _vp, _dp, _i, ctypes.POINTER(Harmonic), _i,
                            ctypes.POINTER(ShellItem), _i, _vp, _vp],
     "cnpc_contract_gram": [_vp, _i, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
@@ -163,7 +165,7 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
                     "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
-                    "gram_tc": 2, "gram_multi_g": 2}
+                    "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1}
 launch_count = 0
 
 
@@ -355,6 +357,23 @@ class Context:
         _count("sn_bins")
         _tstop("sn_bins", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype)
                * ((1 if a.data_ptr() == b.data_ptr() else 2) + (1 if source is not None else 0)))
+
+    def sn_bins_multi(self, dtype, n, boxsize, a, b, vsq, window, sn0s, yl0s, edges, sums, sources, band=0.0):
+        """cnpc_sn_bins_multi: len(sn0s) (1 or 2) configurations in one pass;
+        yl0s[c] / sources[c] may be None."""
+        nc = len(sn0s)
+        e, ep = _darr(edges)
+        s0 = (ctypes.c_double * nc)(*[float(x) for x in sn0s])
+        ys = (ctypes.POINTER(Harmonic) * nc)(*[ctypes.pointer(y) if y is not None else None for y in yl0s])
+        ds = (_vp * nc)(*[t.data_ptr() for t in sums])
+        ss = (_vp * nc)(*[t.data_ptr() if t is not None else None for t in sources])
+        e0 = _tstart()
+        st = self.lib.cnpc_sn_bins_multi(self.h, dtype, n, boxsize, _ptr(a), _ptr(b), vsq, window, nc, s0, ys,
+                                         ep, len(e), ds, ss, band, self.stream())
+        self._check(st, "cnpc_sn_bins_multi")
+        _count("sn_bins_multi")
+        _tstop("sn_bins", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype)
+               * ((1 if a.data_ptr() == b.data_ptr() else 2) + sum(1 for x in sources if x is not None)))
 
     def shell_spectra(self, dtype, n, boxsize, a, b, edges, harmonics, items, out):
         e, ep = _darr(edges)

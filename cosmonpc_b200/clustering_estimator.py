@@ -203,34 +203,47 @@ def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat
     src_fields = {}
     src_origin = {}
     cfg_info = []
+    jobs, sum_keys, src_keys = [], set(), set()
     for (l1, l2, L_) in angu_configs:
         sn0 = N_gal["a"] if (correlation_mode == "auto" and [l1, l2, L_] == [0, 0, 0]) else 0.0
         cfg_info.append(sn0)
         if tracer_type == "abc":
             continue
         key = (L_, sn0)
-        need_sum = key not in sn_sums
-        need_src = shotnoise_mode in ("fft", "both") and tracer_type != "abb" and sn0 not in src_fields
+        need_sum = key not in sum_keys
+        need_src = shotnoise_mode in ("fft", "both") and tracer_type != "abb" and sn0 not in src_keys
         if not (need_sum or need_src):
             continue
-        # one pass gives the k3-bin sums, the source spectrum and its x = 0 value
-        d = torch.empty(2 * (k3_bins + 1), dtype=torch.float64, device=dev)
-        yl0 = angular.harmonic(L_, 0, True) if (L_ != 0 and need_sum) else None
-        src_spec = torch.empty(spec["a"].shape, dtype=cdt, device=dev) if need_src else None
-        ctx.sn_bins(code, n, L, spec["a"], other, float(V) ** 2,
-                    float(sn0) if correlation_mode == "auto" else 0.0, window, yl0, k3_edge, d,
-                    source=src_spec, band=2.0 * k_max if need_src else 0.0)
         if need_sum:
-            sn_sums[key] = engine.HostCopy(d)
+            sum_keys.add(key)
         if need_src:
-            fld = torch.empty(n * n * n, dtype=rdt, device=dev)
-            ctx.c2r(code, n, 1, src_spec, fld)
-            del src_spec
-            if precision == "f32":
-                # x = 0 cell added in FP64 (engine.origin_correction)
-                src_origin[sn0] = engine.HostCopy(d[2 * k3_bins:])
-                fld.narrow(0, 0, 1).zero_()
-            src_fields[sn0] = fld
+            src_keys.add(sn0)
+        jobs.append((key, L_, sn0, need_sum, need_src))
+    # one pass over the modes per two configurations gives their k3-bin sums,
+    # source spectra and the sources' x = 0 values
+    for j0 in range(0, len(jobs), 2):
+        group = jobs[j0:j0 + 2]
+        ds = [torch.empty(2 * (k3_bins + 1), dtype=torch.float64, device=dev) for _ in group]
+        yls = [angular.harmonic(L_, 0, True) if (L_ != 0 and need_sum) else None
+               for (_, L_, _, need_sum, _) in group]
+        srcs = [torch.empty(spec["a"].shape, dtype=cdt, device=dev) if need_src else None
+                for (*_, need_src) in group]
+        any_src = any(x is not None for x in srcs)
+        ctx.sn_bins_multi(code, n, L, spec["a"], other, float(V) ** 2, window,
+                          [float(sn0) if correlation_mode == "auto" else 0.0 for (_, _, sn0, _, _) in group],
+                          yls, k3_edge, ds, srcs, band=2.0 * k_max if any_src else 0.0)
+        for (key, _, sn0, need_sum, need_src), d, src_spec in zip(group, ds, srcs):
+            if need_sum:
+                sn_sums[key] = engine.HostCopy(d)
+            if need_src:
+                fld = torch.empty(n * n * n, dtype=rdt, device=dev)
+                ctx.c2r(code, n, 1, src_spec, fld)
+                if precision == "f32":
+                    # x = 0 cell added in FP64 (engine.origin_correction)
+                    src_origin[sn0] = engine.HostCopy(d[2 * k3_bins:])
+                    fld.narrow(0, 0, 1).zero_()
+                src_fields[sn0] = fld
+        del srcs
 
     # ---- signal: G_00 = Re c2r(delta) band-limited to |k| < 2 k_max (the only
     #      modes the triple sums see), shell fields, pair sums (ce:867-1061)

@@ -146,67 +146,101 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
 }
 
 // ------------------------------------------------------- shot-noise sums
-template <typename T>
-__global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, double vsq,
-                               double sn0, int p, int use_y, cnpc_harmonic yl0, EdgeSet edges,
-                               double *sums, cpx_t<T> *source, double band, int64_t nh) {
+// Up to kSnMaxCfg shot-noise configurations share one pass over the modes
+// (the decode, |k|, bin and spectrum loads); each has its own sn0, Y_L0,
+// sums and source.
+constexpr int kSnMaxCfg = 2;
+struct SnCfg {
+    double sn0[kSnMaxCfg];
+    int use_y[kSnMaxCfg];
+    cnpc_harmonic yl0[kSnMaxCfg];
+    double *sums[kSnMaxCfg];
+    void *source[kSnMaxCfg];
+};
+
+template <typename T, int NC>
+__global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, double vsq, int p,
+                               EdgeSet edges, const SnCfg cfg, double band, int64_t nh) {
     extern __shared__ double sm[];
+    bool any_sn0 = false, any_src = false;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        any_sn0 |= cfg.sn0[c] != 0.0;
+        any_src |= cfg.source[c] != nullptr;
+    }
     AxisTable ax;
-    fill_axis_table(ax, sm, n, L, sn0 != 0.0 ? CNPC_COMP_BKNOISE : CNPC_COMP_NONE, p);
+    fill_axis_table(ax, sm, n, L, any_sn0 ? CNPC_COMP_BKNOISE : CNPC_COMP_NONE, p);
+    // per configuration nb + 1 bins: the shell sums, then the full-space sum of
+    // its source (the source's x = 0 value)
     double *bins = sm + 2 * (n + 1);
-    const int nb = edges.n - 1;
-    // with a source, bins[nb] collects the full-space sum of the source (its x = 0 value)
-    const int nbt = source ? nb + 1 : nb;
-    const double *e = edges_to_shared(bins + nbt, edges);
-    __shared__ cnpc_harmonic s_y;  // read at run-time indices by harmonic_eval
-    if (threadIdx.x == 0) s_y = yl0;
-    for (int i = threadIdx.x; i < nbt; i += blockDim.x) bins[i] = 0.0;
+    const int nb = edges.n - 1, nbt = nb + 1;
+    const double *e = edges_to_shared(bins + NC * nbt, edges);
+    __shared__ cnpc_harmonic s_y[NC];  // read at run-time indices by harmonic_eval
+    if (threadIdx.x < NC) s_y[threadIdx.x] = cfg.yl0[threadIdx.x];
+    for (int i = threadIdx.x; i < NC * nbt; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
+    double tot[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) tot[c] = 0.0;
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
          base += wstride) {
         const int64_t t = base + lane;
         int bin = -1;
-        double val = 0.0, tot = 0.0;
-        bool in_band = false;
+        double val[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) val[c] = 0.0;
         if (t < nh) {
             const Mode m = mode_of(t, n);
             const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
             const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, e, edges.n);
             const bool keep = !(band > 0.0) || kn < band;
-            if (bin >= 0 || (source && keep)) {
+            if (bin >= 0 || (any_src && keep)) {
                 const cpx_t<T> va = a[t], vb = b[t];
-                double pr = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+                const double pr0 = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
                 const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
-                if (sn0 != 0.0) pr -= sn0 * (ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz));
-                if (source) {
-                    source[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
-                    // the stored source is Hermitian on |k| < band: mult * Re sums the full space
-                    in_band = keep;
-                    tot = m.mult * (double)(T)pr;
-                }
-                if (bin >= 0) {
-                    double y = 1.0;
-                    if (use_y) {
-                        const bool origin = kn == 0.0;
-                        const double ik = origin ? 0.0 : 1.0 / kn;
-                        y = harmonic_eval<double>(s_y, kx * ik, ky * ik, kz * ik, origin).x;
+                const double w = any_sn0 ? ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz) : 0.0;
+                const bool origin = kn == 0.0;
+                const double ik = origin ? 0.0 : 1.0 / kn;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    double pr = pr0;
+                    if (cfg.sn0[c] != 0.0) pr -= cfg.sn0[c] * w;
+                    if (cfg.source[c]) {
+                        static_cast<cpx_t<T> *>(cfg.source[c])[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+                        // the stored source is Hermitian on |k| < band: mult * Re sums the full space
+                        if (keep) tot[c] += m.mult * (double)(T)pr;
                     }
-                    val = m.mult * pr * y;
+                    if (bin >= 0) {
+                        double y = 1.0;
+                        if (cfg.use_y[c]) y = harmonic_eval<double>(s_y[c], kx * ik, ky * ik, kz * ik, origin).x;
+                        val[c] = m.mult * pr * y;
+                    }
                 }
-            } else if (source) {
-                source[t] = mk<T>((T)0, (T)0);
+            } else if (any_src) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (cfg.source[c]) static_cast<cpx_t<T> *>(cfg.source[c])[t] = mk<T>((T)0, (T)0);
             }
         }
-        double v[1] = {val};
-        warp_run_add<1>(bins, 0, bin, v);
-        if (source) warp_bin_add(bins, in_band ? nb : -1, tot);
+        warp_run_add<NC>(bins, nbt, bin, val);
+    }
+    // source sums: per thread, then per warp, into bin nb of each configuration
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        if (!cfg.source[c]) continue;
+        double x = tot[c];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0 && x != 0.0) atomicAdd(&bins[c * nbt + nb], x);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nbt; i += blockDim.x)
-        if (bins[i] != 0.0) atomicAdd(&sums[2 * i], bins[i]);
+    for (int i = threadIdx.x; i < NC * nbt; i += blockDim.x) {
+        const int c = i / nbt, j = i - c * nbt;
+        if (bins[i] != 0.0 && (j < nb || cfg.source[c])) atomicAdd(&cfg.sums[c][2 * j], bins[i]);
+    }
 }
 
 // --------------------------------------------------------- shell spectra
@@ -352,40 +386,69 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     return check_launch(ctx, "pk_bins_kernel");
 }
 
+static int run_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                       const void *d_spec_b, double volume_sq, int window, int ncfg, const double *h_sn0,
+                       const cnpc_harmonic *const *h_yl0, const double *h_edges, int nedges,
+                       double *const *d_sums, void *const *d_source, double band_kmax, cnpc_stream_t stream) {
+    int st = check_common(ctx, dtype, n, boxsize);
+    if (st) return st;
+    CNPC_REQUIRE(ctx, d_spec_a && d_spec_b && h_sn0 && h_yl0 && d_sums && d_source, "null argument");
+    CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
+    CNPC_REQUIRE(ctx, ncfg >= 1 && ncfg <= kSnMaxCfg, "ncfg must be 1..2");
+    EdgeSet es;
+    st = load_edges(ctx, h_edges, nedges, &es);
+    if (st) return st;
+    SnCfg cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    const int nb = nedges - 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int c = 0; c < ncfg; ++c) {
+        CNPC_REQUIRE(ctx, d_sums[c] != nullptr, "null sums");
+        cfg.sn0[c] = h_sn0[c];
+        if (h_yl0[c]) {
+            cfg.yl0[c] = *h_yl0[c];
+            cfg.use_y[c] = 1;
+            CNPC_REQUIRE(ctx, cfg.yl0[c].l >= 0 && cfg.yl0[c].l <= 8 && cfg.yl0[c].m == 0, "Y_L0 harmonic expected");
+        }
+        cfg.sums[c] = d_sums[c];
+        cfg.source[c] = d_source[c];
+        const int nbt = d_source[c] ? nb + 1 : nb;
+        st = check_cuda(ctx, cudaMemsetAsync(d_sums[c], 0, sizeof(double) * 2 * nbt, s), "memset");
+        if (st) return st;
+    }
+    const int64_t nh = half_modes(n);
+    const int threads = 256;
+    const size_t smem = sizeof(double) * (2 * (n + 1) + ncfg * (nb + 1) + nedges);
+    const int grid = grid_for(ctx, nh, threads);
+#define CNPC_SN_LAUNCH(T_, NC_)                                                                          \
+    sn_bins_kernel<T_, NC_><<<grid, threads, smem, s>>>((const cpx_t<T_> *)d_spec_a,                     \
+                                                       (const cpx_t<T_> *)d_spec_b, n, boxsize, volume_sq, \
+                                                       window, es, cfg, band_kmax, nh)
+    if (dtype == CNPC_F32) {
+        if (ncfg == 1) CNPC_SN_LAUNCH(float, 1);
+        else CNPC_SN_LAUNCH(float, 2);
+    } else {
+        if (ncfg == 1) CNPC_SN_LAUNCH(double, 1);
+        else CNPC_SN_LAUNCH(double, 2);
+    }
+#undef CNPC_SN_LAUNCH
+    return check_launch(ctx, "sn_bins_kernel");
+}
+
 int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
                  const void *d_spec_b, double volume_sq, double sn0, int window,
                  const cnpc_harmonic *h_yl0, const double *h_edges, int nedges, double *d_sums,
                  void *d_source, double band_kmax, cnpc_stream_t stream) {
-    int st = check_common(ctx, dtype, n, boxsize);
-    if (st) return st;
-    CNPC_REQUIRE(ctx, d_spec_a && d_spec_b && d_sums, "null argument");
-    CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
-    EdgeSet es;
-    st = load_edges(ctx, h_edges, nedges, &es);
-    if (st) return st;
-    cnpc_harmonic y;
-    std::memset(&y, 0, sizeof(y));
-    if (h_yl0) {
-        y = *h_yl0;
-        CNPC_REQUIRE(ctx, y.l >= 0 && y.l <= 8 && y.m == 0, "Y_L0 harmonic expected");
-    }
-    const int nb = nedges - 1;
-    const int nbt = d_source ? nb + 1 : nb;
-    cudaStream_t s = (cudaStream_t)stream;
-    st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nbt, s), "memset");
-    if (st) return st;
-    const int64_t nh = half_modes(n);
-    const int threads = 256;
-    const size_t smem = sizeof(double) * (2 * (n + 1) + nbt + nedges);
-    if (dtype == CNPC_F32)
-        sn_bins_kernel<float><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            (const float2 *)d_spec_a, (const float2 *)d_spec_b, n, boxsize, volume_sq, sn0, window,
-            h_yl0 ? 1 : 0, y, es, d_sums, (float2 *)d_source, band_kmax, nh);
-    else
-        sn_bins_kernel<double><<<grid_for(ctx, nh, threads), threads, smem, s>>>(
-            (const double2 *)d_spec_a, (const double2 *)d_spec_b, n, boxsize, volume_sq, sn0,
-            window, h_yl0 ? 1 : 0, y, es, d_sums, (double2 *)d_source, band_kmax, nh);
-    return check_launch(ctx, "sn_bins_kernel");
+    return run_sn_bins(ctx, dtype, n, boxsize, d_spec_a, d_spec_b, volume_sq, window, 1, &sn0, &h_yl0, h_edges,
+                       nedges, &d_sums, &d_source, band_kmax, stream);
+}
+
+int cnpc_sn_bins_multi(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                       const void *d_spec_b, double volume_sq, int window, int ncfg, const double *h_sn0,
+                       const cnpc_harmonic *const *h_yl0, const double *h_edges, int nedges,
+                       double *const *d_sums, void *const *d_source, double band_kmax, cnpc_stream_t stream) {
+    return run_sn_bins(ctx, dtype, n, boxsize, d_spec_a, d_spec_b, volume_sq, window, ncfg, h_sn0, h_yl0, h_edges,
+                       nedges, d_sums, d_source, band_kmax, stream);
 }
 
 int cnpc_shell_spectra(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,

@@ -170,6 +170,18 @@ int cnpc_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
                  const cnpc_harmonic *h_yl0, const double *h_edges, int nedges,
                  double *d_sums, void *d_source, double band_kmax, cnpc_stream_t stream);
 
+/* cnpc_sn_bins for ncfg = 1 or 2 configurations of the bk_sugi box loop over
+ * angular configurations (ce:1187-1210, :1405-1434) in one pass over the
+ * modes: configuration c has its own sn0 h_sn0[c], harmonic h_yl0[c] (NULL:
+ * 1), d_sums[c] and d_source[c] (NULL: no source), each with the layout and
+ * meaning of cnpc_sn_bins; the spectra, volume_sq, window, edges and
+ * band_kmax are shared. */
+int cnpc_sn_bins_multi(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_spec_a,
+                       const void *d_spec_b, double volume_sq, int window, int ncfg,
+                       const double *h_sn0, const cnpc_harmonic *const *h_yl0,
+                       const double *h_edges, int nedges, double *const *d_sums,
+                       void *const *d_source, double band_kmax, cnpc_stream_t stream);
+
 /* Shell spectra: replaces (ylm_weighted_cfield * mask_i) before .c2r() in
  * clustering_estimator.py:898-969, :1012-1050, :1215-1219.  For each item j,
  * writes half spectrum j of d_out (n*n*(n/2+1) complex each):

@@ -258,6 +258,52 @@ def test_tiled_paint_fixed_point_scales(case):
         assert abs(got.sum() - w.sum()) < (1e-4 if case == "overfull_cell" else 1e-6) * w.sum()
 
 
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("cross", [False, True])
+def test_sn_bins_multi_matches_single_calls(dtype, cross):
+    """cnpc_sn_bins_multi (two shot-noise configurations in one pass: sn0 with
+    Y_00 and a source, sn0 = 0 with Y_20 and a source) against one
+    cnpc_sn_bins call per configuration: the same source spectra bit for bit,
+    the same shell sums and source totals up to summation order."""
+    import torch
+    from cosmonpc_b200 import _lib, angular
+
+    n, L = 48, 600.0
+    code = _lib.F64 if dtype == "f64" else _lib.F32
+    cdt = torch.complex128 if dtype == "f64" else torch.complex64
+    g = torch.Generator(device="cuda").manual_seed(7 + cross)
+    shape = (n, n, n // 2 + 1)
+    a = torch.randn(shape, dtype=cdt, device="cuda", generator=g)
+    b = torch.randn(shape, dtype=cdt, device="cuda", generator=g) if cross else a
+    kf = 2 * np.pi / L
+    edges = np.linspace(2 * kf, 17.5 * kf, 12)
+    band = 14.2 * kf
+    nb = len(edges) - 1
+    ctx = _lib.Context.get()
+    cfgs = [(1234.5, None), (0.0, angular.harmonic(2, 0, True))]
+    sums_m = [torch.empty(2 * (nb + 1), dtype=torch.float64, device="cuda") for _ in cfgs]
+    src_m = [torch.empty(shape, dtype=cdt, device="cuda") for _ in cfgs]
+    ctx.sn_bins_multi(code, n, L, a, b, 3.5, 3, [c[0] for c in cfgs], [c[1] for c in cfgs], edges,
+                      sums_m, src_m, band=band)
+    for (sn0, y), sm, srm in zip(cfgs, sums_m, src_m):
+        s1 = torch.empty(2 * (nb + 1), dtype=torch.float64, device="cuda")
+        sr1 = torch.empty(shape, dtype=cdt, device="cuda")
+        ctx.sn_bins(code, n, L, a, b, 3.5, sn0, 3, y, edges, s1, source=sr1, band=band)
+        assert torch.equal(torch.view_as_real(srm), torch.view_as_real(sr1))
+        scale = s1[0::2].abs().max().item()
+        assert scale > 0
+        assert ((sm[0::2] - s1[0::2]).abs().max().item()) <= 1e-12 * scale
+    # a configuration without source next to one with a source
+    s_ns = torch.empty(2 * nb, dtype=torch.float64, device="cuda")
+    s_src = torch.empty(2 * (nb + 1), dtype=torch.float64, device="cuda")
+    sr = torch.empty(shape, dtype=cdt, device="cuda")
+    ctx.sn_bins_multi(code, n, L, a, b, 3.5, 3, [0.0, 1234.5], [cfgs[1][1], None], edges, [s_ns, s_src],
+                      [None, sr], band=band)
+    assert torch.equal(torch.view_as_real(sr), torch.view_as_real(src_m[0]))
+    scale = sums_m[1][0::2].abs().max().item()
+    assert (s_ns[0::2] - sums_m[1][0::2][:nb]).abs().max().item() <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("ngs,rows,nb,shared", [(2, (20, 20), 20, True), (3, (5, 9, 11), 8, False),
                                                 (1, (17,), 7, False), (4, (10, 10, 10, 10), 20, True)])
 def test_multi_weight_gram_matches_separate_launches(ngs, rows, nb, shared):
