@@ -207,10 +207,14 @@ __device__ inline void red_shared_add_nc(float *addr, float v) {
 }
 
 // Region accumulator: fixed point (scale 2^e) or, for a tile too heavy for
-// 32 bits, FP32 in the same words (FIXED picks one at compile time).
+// 32 bits, FP32 in the same words (FIXED picks one at compile time).  The
+// fixed-point word is RN(v 2^e) from one FMA: with |v 2^e| <= 2^22, adding
+// 1.5 2^23 rounds to an integer in the low mantissa bits (no F2I).
+constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kRoundMagicBits = 0x4B400000;
 template <bool FIXED> __device__ __forceinline__ void region_add(int *reg, int idx, float v, float scale) {
     if (FIXED)
-        red_shared_add_nc(reg + idx, __float2int_rn(v * scale));
+        red_shared_add_nc(reg + idx, __float_as_int(__fmaf_rn(v, scale, kRoundMagic)) - kRoundMagicBits);
     else
         red_shared_add_nc(reinterpret_cast<float *>(reg) + idx, v);
 }
@@ -313,10 +317,12 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
         // (1 + 2^-20): FP32 products of rounded weights may exceed wmax^3 by a few ulps
         const double bound =
             (double)s_cmax * (double)__uint_as_float(s_mbits) * (double)(wa * wa * wa) * (1.0 + 0x1p-20);
-        // rounding adds at most 1/2 per deposit, one deposit per particle of the window
+        // rounding adds at most 1/2 per deposit, one deposit per particle of the window;
+        // one deposit stays within 2^22 (region_add's rounding)
         const double room = 2147483647.0 - (double)s_cmax;
+        const double one = (double)__uint_as_float(s_mbits) * (double)(wa * wa * wa) * (1.0 + 0x1p-20);
         int e = 100;
-        if (bound > 0.0) e = min(100, ilogb(room / bound));
+        if (bound > 0.0) e = min(100, min(ilogb(room / bound), ilogb(4194304.0 / one)));
         const float scale = ldexpf(1.f, e);
         const bool fixed = s_cmax <= 65536;
         auto deposit_all = [&](auto fixed_tag) {
