@@ -30,6 +30,7 @@ EXPORTED = (
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
     "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
+    "cnpc_forward_finish_band",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -90,6 +91,7 @@ _SIGS = {
     "cnpc_fft_r2c": [_vp, _i, _i, _i, _vp, _i64, _vp, _vp],
     "cnpc_fft_c2r": [_vp, _i, _i, _i, _vp, _vp, _i64, _vp],
     "cnpc_forward_finish": [_vp, _i, _i, _d, _vp, _vp, _d, _i, _i, _d, _d, _vp],
+    "cnpc_forward_finish_band": [_vp, _i, _i, _d, _vp, _vp, _d, _i, _i, _d, _d, _vp, _d, _vp],
     "cnpc_kbin_counts": [_vp, _i, _d, _dp, _i, _vp, _vp, _vp],
     "cnpc_pk_bins": [_vp, _i, _i, _d, _vp, _vp, _dp, _i, _ip, _i, _dp, _vp, _vp],
     "cnpc_sn_bins": [_vp, _i, _i, _d, _vp, _vp, _d, _d, _i, ctypes.POINTER(Harmonic), _dp, _i,
@@ -165,7 +167,7 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
                     "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
-                    "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1}
+                    "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1, "forward_finish_band": 1}
 launch_count = 0
 
 
@@ -327,6 +329,15 @@ class Context:
         self._check(st, "cnpc_forward_finish")
         _count("forward_finish")
         _tstop("forward_finish", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * (3 if spec2 is not None else 2))
+
+    def forward_finish_band(self, dtype, n, boxsize, spec, spec2, scale, comp, window, k0, band, band_out,
+                            band_out_k):
+        e0 = _tstart()
+        st = self.lib.cnpc_forward_finish_band(self.h, dtype, n, boxsize, _ptr(spec), _ptr(spec2), scale,
+                                               comp, window, k0, band, _ptr(band_out), band_out_k, self.stream())
+        self._check(st, "cnpc_forward_finish_band")
+        _count("forward_finish_band")
+        _tstop("forward_finish", e0, n * n * (n // 2 + 1) * 2 * _esz(dtype) * (4 if spec2 is not None else 3))
 
     def kbin_counts(self, n, boxsize, edges, counts, ksum):
         e, ep = _darr(edges)

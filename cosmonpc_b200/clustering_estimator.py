@@ -181,11 +181,17 @@ def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat
 
     # ---- overdensity spectra: r2c(rho/dV - NZ), compensated (ce:808-837)
     k_edge = np.linspace(k_min, k_max, k_bins + 1)
+    # G_00's spectrum: the triple sums see it only at |k| < 2 k_max, so the
+    # forward finish of that tracer also writes its band-limited copy
+    g_letter = "a" if correlation_mode == "auto" else ("c" if tracer_type == "abc" else "b")
     spec = {}
     for t in letters:
         m = meshes[t]
         k0 = (m.sum_w / float(N3)) / vol_per_cell - NZ[t]
-        spec[t] = engine.finish_delta(m, 1.0 / vol_per_cell, _lib.COMP_SINC, k0)
+        if t == g_letter:
+            spec[t], g_spec = engine.finish_delta_band(m, 1.0 / vol_per_cell, _lib.COMP_SINC, k0, 2.0 * k_max)
+        else:
+            spec[t] = engine.finish_delta(m, 1.0 / vol_per_cell, _lib.COMP_SINC, k0)
     dev = spec["a"].device
 
     # ---- mode counts on k and k3 bins (ce:858-865, :1063-1074)
@@ -247,8 +253,9 @@ def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat
 
     # ---- signal: G_00 = Re c2r(delta) band-limited to |k| < 2 k_max (the only
     #      modes the triple sums see), shell fields, pair sums (ce:867-1061)
-    g_letter = "a" if correlation_mode == "auto" else ("c" if tracer_type == "abc" else "b")
-    G = engine.band_limited_field(n, L, spec[g_letter], 2.0 * k_max, precision)
+    G = torch.empty(n * n * n, dtype=rdt, device=dev)
+    ctx.c2r(code, n, 1, g_spec, G)
+    del g_spec
     specs, per_cfg = [], []
     for (l1, l2, L_) in angu_configs:
         cfgs, tj = angular.magnetic_configs_box(l1, l2, L_)

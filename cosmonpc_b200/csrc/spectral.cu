@@ -11,7 +11,7 @@ namespace cnpc {
 template <typename T>
 __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int n, double L,
                                       double inv_n3, double scale, int comp, int p, double k0,
-                                      double band, int64_t nh) {
+                                      double band, cpx_t<T> *band_out, double band_out_k, int64_t nh) {
     extern __shared__ double tbl[];
     AxisTable ax;
     fill_axis_table(ax, tbl, n, L, comp, p);
@@ -41,6 +41,8 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
         }
         if (band > 0.0 && kn >= band) re = im = 0.0;
         spec[t] = mk<T>((T)re, (T)im);
+        // band_out may be spec2: its element t was read above by this thread
+        if (band_out) band_out[t] = kn < band_out_k ? mk<T>((T)re, (T)im) : mk<T>((T)0, (T)0);
     }
 }
 
@@ -305,14 +307,15 @@ using namespace cnpc;
 
 extern "C" {
 
-int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
-                        const void *d_spec2, double scale, int comp, int window, double k0_value,
-                        double band_kmax, cnpc_stream_t stream) {
+int cnpc_forward_finish_band(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
+                             const void *d_spec2, double scale, int comp, int window, double k0_value,
+                             double band_kmax, void *d_band_out, double band_out_kmax, cnpc_stream_t stream) {
     int st = check_common(ctx, dtype, n, boxsize);
     if (st) return st;
     CNPC_REQUIRE(ctx, d_spec != nullptr, "null spectrum");
     CNPC_REQUIRE(ctx, comp >= 0 && comp <= 3, "bad compensation kind");
     CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
+    CNPC_REQUIRE(ctx, d_band_out != d_spec, "band output must not be the spectrum");
     const int64_t nh = half_modes(n);
     const double inv_n3 = 1.0 / ((double)n * n * n);
     cudaStream_t s = (cudaStream_t)stream;
@@ -322,12 +325,19 @@ int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d
     if (dtype == CNPC_F32)
         forward_finish_kernel<float><<<blocks, threads, tsm, s>>>(
             (float2 *)d_spec, (const float2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
-            k0_value, band_kmax, nh);
+            k0_value, band_kmax, (float2 *)d_band_out, band_out_kmax, nh);
     else
         forward_finish_kernel<double><<<blocks, threads, tsm, s>>>(
             (double2 *)d_spec, (const double2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
-            k0_value, band_kmax, nh);
+            k0_value, band_kmax, (double2 *)d_band_out, band_out_kmax, nh);
     return check_launch(ctx, "forward_finish_kernel");
+}
+
+int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
+                        const void *d_spec2, double scale, int comp, int window, double k0_value,
+                        double band_kmax, cnpc_stream_t stream) {
+    return cnpc_forward_finish_band(ctx, dtype, n, boxsize, d_spec, d_spec2, scale, comp, window, k0_value,
+                                    band_kmax, nullptr, 0.0, stream);
 }
 
 int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges, int nedges,

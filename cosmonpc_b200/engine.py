@@ -87,6 +87,22 @@ def finish_delta(pm, scale, comp, k0, band=0.0):
     return pm.raw[0]
 
 
+def finish_delta_band(pm, scale, comp, k0, band_out_k):
+    """finish_delta that also returns the finished spectrum zeroed at
+    |k| >= band_out_k, written into the consumed +1/2-cell twin spectrum when
+    the mesh is interlaced (a new buffer otherwise)."""
+    if pm.used:
+        raise ValueError("painted mesh already consumed by an estimator")
+    pm.used = True
+    ctx = _lib.Context.get()
+    code = PRECISION[pm.precision][0]
+    spec2 = pm.raw[1] if pm.interlaced else None
+    out = spec2 if spec2 is not None else torch.empty_like(pm.raw[0])
+    ctx.forward_finish_band(code, pm.n, pm.boxsize, pm.raw[0], spec2, float(scale), comp, pm.window,
+                            float(k0), 0.0, out, float(band_out_k))
+    return pm.raw[0], out
+
+
 def kbin_counts(n, boxsize, edges):
     """Mode counts and sum |k| per bin (geometry only: kept per shape class
     while UNIT_SHELL_CACHE is on)."""
@@ -255,15 +271,6 @@ class ShellFields:
         if self.persistent and todo:
             self.ready = torch.cuda.Event()
             self.ready.record()
-
-
-def band_limited_field(n, boxsize, spec, kmax_band, precision, racah=True):
-    """Real field c2r(spec * 1[|k| < kmax_band]) (a copy; spec is left intact)."""
-    sf = ShellFields(n, boxsize, [0.0, float(kmax_band)], precision, spec, None, capacity=1, fft_batch=1)
-    sf.ensure([sf.key((0, 0, 0, False), 0, 0)])
-    out = sf.fields[0]
-    sf._scratch = None
-    return out
 
 
 class HostCopy:

@@ -139,6 +139,16 @@ int cnpc_forward_finish(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d
                         const void *d_spec2, double scale, int comp, int window,
                         double k0_value, double band_kmax, cnpc_stream_t stream);
 
+/* cnpc_forward_finish that also writes the finished spectrum, zeroed at
+ * |k| >= band_out_kmax, to d_band_out: the band-limited copy of the
+ * overdensity spectrum that the bk_sugi box estimator transforms into G_00
+ * (ce:843-851; the triple sums see G_00 only at |k| < 2 k_max).  d_band_out may be d_spec2 (each element is read before it
+ * is overwritten); it must not be d_spec. */
+int cnpc_forward_finish_band(cnpc_ctx *ctx, int dtype, int n, double boxsize, void *d_spec,
+                             const void *d_spec2, double scale, int comp, int window,
+                             double k0_value, double band_kmax, void *d_band_out,
+                             double band_out_kmax, cnpc_stream_t stream);
+
 /* -------------------------------------------------------- k-bin statistics
  * get_kbin_count (math_evaluator.py:452-481): full-space mode counts and sum
  * of |k| per bin [e_b, e_{b+1}), |k| computed in FP64 as

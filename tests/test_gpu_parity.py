@@ -259,6 +259,37 @@ def test_tiled_paint_fixed_point_scales(case):
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("aliased", [True, False])
+def test_forward_finish_band_copy(dtype, aliased):
+    """cnpc_forward_finish_band: the finished spectrum equals cnpc_forward_finish
+    bit for bit, and the band copy (written over the twin spectrum, or to a
+    separate buffer) is that spectrum zeroed at |k| >= the band, |k| as the
+    oracle computes it."""
+    import torch
+    from cosmonpc_b200 import _lib
+    from oracle.box import KGeom
+
+    n, L = 32, 400.0
+    code = _lib.F64 if dtype == "f64" else _lib.F32
+    cdt = torch.complex128 if dtype == "f64" else torch.complex64
+    g = torch.Generator(device="cuda").manual_seed(3)
+    shape = (n, n, n // 2 + 1)
+    s1 = torch.randn(shape, dtype=cdt, device="cuda", generator=g)
+    s2 = torch.randn(shape, dtype=cdt, device="cuda", generator=g)
+    ctx = _lib.Context.get()
+    ref = s1.clone()
+    ctx.forward_finish(code, n, L, ref, s2.clone(), 0.7, _lib.COMP_SINC, 3, 1.25)
+    band = 9.5 * 2 * np.pi / L
+    a, b = s1.clone(), s2.clone()
+    out = b if aliased else torch.empty_like(a)
+    ctx.forward_finish_band(code, n, L, a, b, 0.7, _lib.COMP_SINC, 3, 1.25, 0.0, out, band)
+    assert torch.equal(torch.view_as_real(a), torch.view_as_real(ref))
+    kn = torch.from_numpy(np.ascontiguousarray(KGeom(n, L).knorm[:, :, :n // 2 + 1])).cuda()
+    expect = torch.where(kn < band, ref, torch.zeros_like(ref))
+    assert torch.equal(torch.view_as_real(out), torch.view_as_real(expect))
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
 @pytest.mark.parametrize("cross", [False, True])
 def test_sn_bins_multi_matches_single_calls(dtype, cross):
     """cnpc_sn_bins_multi (two shot-noise configurations in one pass: sn0 with
