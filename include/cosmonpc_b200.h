@@ -170,8 +170,9 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
 /* Shot-noise shell sums for calculate_bk_sugi_box (ce:1405-1434) and the
  * S3-FFT source spectrum (ce:1187-1210):
  *   P(k) = V^2 a(k) conj(b(k)) - sn0 * W_bknoise(k)
- *   d_sums[2*bin + {0,1}] = sum_{bin} P(k) * Y_L0(khat)   (complex, FP64)
- * with harmonic h_yl0 (NULL: 1).  If d_source is non-NULL, P(k) (without Y)
+ *   d_sums[2*bin] = sum_{bin} Re P(k) * Y_L0(khat)   (FP64; d_sums[2*bin+1] = 0)
+ * with harmonic h_yl0 (NULL: 1): half-spectrum modes carry their full-space
+ * multiplicity, so the real part is the full-space sum for even L.  If d_source is non-NULL, P(k) (without Y)
  * is also written there, zeroed at |k| >= band_kmax when band_kmax > 0, and
  * d_sums[2*(nedges-1)] receives the full-space sum of that source (its value
  * at x = 0 after the c2r), so d_sums then holds nedges pairs. */
