@@ -123,56 +123,95 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU baseline
-def cpu_baseline_estimate(workload, seed):
-    """Time the oracle port (numpy/scipy, all host threads) on a bounded sample
-    of the workload and extrapolate to one data vector by operation counts.
+class CpuBaseline:
+    """The oracle port (numpy/scipy, all host threads) timed on bounded samples
+    of the workload and extrapolated to one data vector by operation counts.
 
-    The reference computes each angular configuration in its own run_stats
-    call (paint + forward transforms each), with F-field and pair counts per
-    config as in clustering_estimator.py:867-995 and :1182-1384."""
-    import numpy as np
+    The reference computes each angular configuration in its own run_stats call
+    (an interlaced paint and the forward transforms each), with shell-field and
+    triple-sum counts per configuration as in clustering_estimator.py:867-995
+    and :1182-1384.  The interlaced paint is timed once (``paint_s``); every
+    sample then times one forward transform, two shell fields and three triple
+    sums of the full-size mesh."""
 
-    from cosmonpc_b200.mocks import BASE_SEED, lognormal_box
-    from oracle import angular as oang
-    from oracle import box as obox
-    from oracle.pmesh_lite import _ifftn
+    def __init__(self, workload, seed):
+        import numpy as np
 
-    n, L = workload["nmesh"], workload["boxsize"]
-    pos = lognormal_box(workload["n_particles"], L, seed)
-    w = np.ones(len(pos))
-    t0 = time.perf_counter()
-    field = obox.paint_field(pos, w, n, L, workload["sampler"], workload["interlaced"])
-    t_paint = time.perf_counter() - t0
-    geo = obox.KGeom(n, L)
-    t0 = time.perf_counter()
-    c = obox._fwd(field)
-    t_fft = time.perf_counter() - t0
-    edges = np.linspace(workload["k_min"], workload["k_max"], workload["k_bins"] + 1)
-    mask = np.logical_and(geo.knorm >= edges[3], geo.knorm < edges[4])
-    y = oang.ylm_function(2, 0, True)(*geo.khat)
-    t0 = time.perf_counter()
-    F1 = _ifftn(c * y * mask) * float(n) ** 3
-    F2 = _ifftn(c * mask) * float(n) ** 3
-    t_field = (time.perf_counter() - t0) / 2
-    G = np.real(_ifftn(c))
-    t0 = time.perf_counter()
-    for _ in range(3):
-        np.sum(G * F1 * F2)
-    t_pair = (time.perf_counter() - t0) / 3
-    B = workload["k_bins"]
-    ncfg = len(workload["angu_configs"])
-    fields, pairs = 0, 0
-    for (l1, l2, L_) in workload["angu_configs"]:
-        f = B if (l1 == l2) else 2 * B
-        p = B * (B + 1) // 2 if (l1 == l2) else B * B
-        fields += f * (2 if workload["shotnoise_mode"] in ("fft", "both") else 1)
-        pairs += p * (2 if workload["shotnoise_mode"] in ("fft", "both") else 1)
-    ffts = ncfg * (1 + 2 + 1)  # r2c(delta), c2r(G), c2r(S3 source) + the paint's combine counted in t_paint
-    total = ncfg * t_paint + ffts * t_fft + fields * t_field + pairs * t_pair
-    sample = (f"oracle port, 1 interlaced paint of {len(pos)} particles + 1 forward FFT + 2 shell fields + "
-              f"3 triple sums at {n}^3, extrapolated to {ncfg} configs x (paint + {ffts // ncfg} FFTs) + "
-              f"{fields} shell fields + {pairs} triple sums")
-    return total, sample, os.cpu_count()
+        from cosmonpc_b200.mocks import lognormal_box
+        from oracle import box as obox
+
+        self.W = workload
+        n, L = workload["nmesh"], workload["boxsize"]
+        pos = lognormal_box(workload["n_particles"], L, seed)
+        w = np.ones(len(pos))
+        self.np = len(pos)
+        t0 = time.perf_counter()
+        self.field = obox.paint_field(pos, w, n, L, workload["sampler"], workload["interlaced"])
+        self.paint_s = time.perf_counter() - t0
+        self.geo = obox.KGeom(n, L)
+        B = workload["k_bins"]
+        fields, pairs = 0, 0
+        per = 2 if workload["shotnoise_mode"] in ("fft", "both") else 1
+        for (l1, l2, L_) in workload["angu_configs"]:
+            fields += (B if l1 == l2 else 2 * B) * per
+            pairs += (B * (B + 1) // 2 if l1 == l2 else B * B) * per
+        self.ncfg = len(workload["angu_configs"])
+        self.ffts = self.ncfg * 4  # r2c(delta), c2r(G), r2c/c2r of the S3 source, per configuration
+        self.fields, self.pairs = fields, pairs
+        # one sample covers this fraction of a data vector's work (paint excluded)
+        self.units = 1 + 2 + 3
+
+    def sample(self):
+        """Seconds per data vector extrapolated from one timed sample."""
+        import numpy as np
+
+        from oracle import angular as oang
+        from oracle import box as obox
+        from oracle.pmesh_lite import _ifftn
+
+        n, W, geo = self.W["nmesh"], self.W, self.geo
+        t0 = time.perf_counter()
+        c = obox._fwd(self.field)
+        t_fft = time.perf_counter() - t0
+        edges = np.linspace(W["k_min"], W["k_max"], W["k_bins"] + 1)
+        mask = np.logical_and(geo.knorm >= edges[3], geo.knorm < edges[4])
+        y = oang.ylm_function(2, 0, True)(*geo.khat)
+        t0 = time.perf_counter()
+        F1 = _ifftn(c * y * mask) * float(n) ** 3
+        F2 = _ifftn(c * mask) * float(n) ** 3
+        t_field = (time.perf_counter() - t0) / 2
+        G = np.real(_ifftn(c))
+        t0 = time.perf_counter()
+        for _ in range(3):
+            np.sum(G * F1 * F2)
+        t_pair = (time.perf_counter() - t0) / 3
+        return self.ncfg * self.paint_s + self.ffts * t_fft + self.fields * t_field + self.pairs * t_pair
+
+    def describe(self):
+        return (f"oracle port (numpy/scipy, {os.cpu_count()} host threads) at {self.W['nmesh']}^3: one interlaced "
+                f"paint of {self.np} particles ({self.paint_s:.1f} s, timed once), then per sample 1 forward FFT + "
+                f"2 shell fields + 3 triple sums, extrapolated to {self.ncfg} configs x (paint + "
+                f"{self.ffts // self.ncfg} FFTs) + {self.fields} shell fields + {self.pairs} triple sums")
+
+    def data_vector_fraction(self):
+        """Share of one data vector's FFT, shell-field and triple-sum work one sample runs."""
+        return self.units / float(self.ffts + self.fields + self.pairs)
+
+
+def cpu_baseline_estimate(workload, seed, samples=1):
+    cb = CpuBaseline(workload, seed)
+    vals = [cb.sample() for _ in range(samples)]
+    return sum(vals) / len(vals), cb.describe(), os.cpu_count()
+
+
+def config_of(W, world):
+    """The ``config`` object of both arms' JSON lines (identical settings)."""
+    return {"workload": "bk_sugi box full %d^3, %.0e lognormal particles, %s interlaced, %d bins %.2f-%.2f, "
+                        "(000)+(202) [(022) = transpose], shotnoise %s"
+                        % (W["nmesh"], W["n_particles"], W["sampler"].upper(), W["k_bins"], W["k_min"], W["k_max"],
+                           W["shotnoise_mode"]),
+            "l2": "working set > L2 (shell fields %.1f GB)" % ((3 * W["k_bins"]) * W["nmesh"] ** 3 * 4 / 1e9),
+            "parallelism": "replicas x%d" % world}
 
 
 # ------------------------------------------------------- survey workload
@@ -307,6 +346,8 @@ def main():
     ap.add_argument("--survey", action="store_true",
                     help="time the survey cross workload (512^3, 2e6 data, 4e7 randoms) instead; one JSON line")
     ap.add_argument("--survey-scale", type=float, default=1.0, help="catalog size factor of --survey")
+    ap.add_argument("--survey-steps", type=int, default=1,
+                    help="timed run_stats rounds of the survey workload in the default line (0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -335,20 +376,23 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
+        cb = CpuBaseline(workload, seed)
         vals = []
-        info = None
         for i in range(args.warmup + args.steps):
-            v, sample, cores = cpu_baseline_estimate(workload, seed)
+            v = cb.sample()
             if i >= args.warmup:
                 vals.append(v)
-            info = (sample, cores)
         value = sum(vals) / len(vals)
+        frac = cb.data_vector_fraction()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "bk_sugi box full 256^3, 4e6 lognormal particles, PCS interlaced, "
-                                       "20 bins 0.01-0.20, (000)+(202), shotnoise both"},
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[1], "kind": "port", "sample": info[0]},
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(workload, args.gpus),
+                "step_note": "each step is one bounded sample (%.4f of a data vector's transform and triple-sum "
+                             "work) extrapolated to a whole data vector; %.3f data vectors' worth of that work "
+                             "was timed in all" % (frac, frac * args.steps),
+                "data_vectors_timed": frac * args.steps,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                 "sample": cb.describe()},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -545,34 +589,44 @@ def main():
     if world == 1 and not args.no_cpu:
         cv, sample, cores = cpu_baseline_estimate(W, seed)
         cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    survey = None
+    if world == 1 and args.survey_steps > 0:
+        t, nd, nr = _survey_runs(BASE_SEED + 4, args.survey_steps, args.survey_scale)
+        f32 = sum(v for k, v in t.items() if k.endswith("f32"))
+        f64 = sum(v for k, v in t.items() if k.endswith("f64"))
+        survey = {"value": f32, "unit": "s/data-vector", "plain_f64": f64, "speedup": f64 / f32,
+                  "catalogs": {"data": nd, "randoms": nr}, "per_call_s": t,
+                  "workload": "survey cross, 512^3, L3500, TSC interlaced, mixed-mesh: pk cross [0,2,4] + "
+                              "bk_sugi aab (000) and (202) diagonal; three run_stats calls, FITS reads included"}
+    mocks_short = None
+    if mocks is not None:
+        mocks_short = {k: mocks[k] for k in ("value", "unit", "plain_value", "speedup", "mocks")}
+    # the summary keys come last, so that a tail of the line still holds them
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_fast / args.steps * 1000.0, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 accumulation", "data": "synthetic",
-        "config": {"workload": "bk_sugi box full %d^3, %.0e lognormal particles, %s interlaced, %d bins %.2f-%.2f, "
-                               "(000)+(202) [(022) = transpose], shotnoise %s"
-                               % (W["nmesh"], W["n_particles"], W["sampler"].upper(), W["k_bins"], W["k_min"],
-                                  W["k_max"], W["shotnoise_mode"]),
-                   "l2": "working set > L2 (shell fields %.1f GB)" % (
-                       (3 * W["k_bins"]) * W["nmesh"] ** 3 * 4 / 1e9),
-                   "parallelism": "replicas x%d" % world},
-        "e2e": e2e,
+        "config": config_of(W, world),
+        "kernels": kernels,
+        "mocks_detail": mocks,
+        "plain_rel_err_by_key": rel_by_key,
+        "survey": survey,
         "amortized": amortized,
         "serial": {"value": t_serial, "unit": UNIT,
                    "note": "one data vector at a time, host algebra not overlapped with the next vector"},
-        "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),
-                      "max_rel_err_fast_vs_plain": max_rel, "rel_err_by_key": rel_by_key},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": launches * args.steps,
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (TRAFFIC_RATIO[dom_name] * nbytes / cnt) if dom_name in TRAFFIC_RATIO else None,
                      "traffic_note": "bytes per launch: the kernel's ncu (dram__bytes_read.sum + "
-                                     "dram__bytes_write.sum) / algorithmic-bytes ratio (gram: 128^3 capture, "
-                                     "shell_fields: 256^3 capture) times this launch's algorithmic bytes"},
-        "kernels": kernels,
-        "mocks": mocks,
-        "gpu_launches": launches * args.steps,
-        "clocks": clk.summary(),
-        "cpu_baseline": cpu,
+                                     "dram__bytes_write.sum) / algorithmic-bytes ratio times this launch's "
+                                     "algorithmic bytes"},
+        "e2e": e2e,
+        "mocks": mocks_short,
+        "plain_f64": {"value": plain, "unit": UNIT, "speedup": (plain / value if plain else None),
+                      "max_rel_err_fast_vs_plain": max_rel},
     }
     print(json.dumps(line))
     if dist is not None:

@@ -30,7 +30,7 @@ EXPORTED = (
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
     "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
-    "cnpc_forward_finish_band",
+    "cnpc_forward_finish_band", "cnpc_ctx_set_wait_limit", "cnpc_ctx_take_status",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -43,6 +43,11 @@ PSUM_COUNT = 5
 
 class CnpcError(RuntimeError):
     """A CUDA / cuFFT failure reported by the library."""
+
+
+class DeviceTimeout(CnpcError):
+    """A bounded device-side wait gave up (CNPC_ETIMEOUT): the outputs of the
+    call that waited are NaN and the context stays usable."""
 
 
 class ShellItem(ctypes.Structure):
@@ -124,6 +129,8 @@ _SIGS = {
     "cnpc_contract_gram_tc": [_vp, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
     "cnpc_contract_gram_multi_g": [_vp, _i64, ctypes.POINTER(_vp), _i, _vp, _i64, _ip, _ip, _i, _ip, _i, _vp,
                                    _vp],
+    "cnpc_ctx_set_wait_limit": [_vp, _i64],
+    "cnpc_ctx_take_status": [_vp, _vp, _ip],
 }
 
 _lib = None
@@ -293,6 +300,22 @@ class Context:
         if st == CNPC_ENOMEM:
             raise MemoryError("%s: %s" % (what, msg))
         raise CnpcError("%s: %s" % (what, msg))
+
+    def set_wait_limit(self, polls):
+        """Polls a bounded device wait makes before it gives up (0: at once)."""
+        self._check(self.lib.cnpc_ctx_set_wait_limit(self.h, int(polls)), "cnpc_ctx_set_wait_limit")
+
+    def take_status(self, stream=None):
+        """Synchronise ``stream`` (a torch stream; default: the current one), read
+        and clear this context's device status word; raises DeviceTimeout if a
+        bounded wait gave up since the last read."""
+        v = ctypes.c_int(0)
+        sh = self.stream() if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        self._check(self.lib.cnpc_ctx_take_status(self.h, sh, ctypes.byref(v)), "cnpc_ctx_take_status")
+        if v.value == CNPC_ETIMEOUT:
+            raise DeviceTimeout("a bounded device wait gave up (CNPC_ETIMEOUT); the results of the call are NaN")
+        if v.value != CNPC_OK:
+            raise CnpcError("device status word %d" % v.value)
 
     @staticmethod
     def stream():

@@ -45,6 +45,20 @@ int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream) {
     return ensure_buffer(ctx, &ctx->scratch, &ctx->scratch_bytes, bytes, stream);
 }
 
+int ensure_status(cnpc_ctx *ctx) {
+    if (ctx->d_status) return CNPC_OK;
+    int *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, 256);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "status word alloc");
+    e = cudaMemset(p, 0, 256);
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        return check_cuda(ctx, e, "status word clear");
+    }
+    ctx->d_status = p;
+    return CNPC_OK;
+}
+
 static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long real_dist, cufftHandle *out) {
     auto key = std::make_tuple((int)type, n, batch, real_dist);
     auto it = ctx->plans.find(key);
@@ -125,11 +139,37 @@ int cnpc_ctx_destroy(cnpc_ctx *ctx) {
     if (ctx->paint_ws) cudaFree(ctx->paint_ws);
     if (ctx->aux) cudaFree(ctx->aux);
     if (ctx->shell_ws) cudaFree(ctx->shell_ws);
+    if (ctx->d_status) cudaFree(ctx->d_status);
     delete ctx;
     return CNPC_OK;
 }
 
 const char *cnpc_ctx_last_error(cnpc_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int cnpc_ctx_set_wait_limit(cnpc_ctx *ctx, int64_t polls) {
+    CNPC_REQUIRE(ctx, ctx != nullptr, "null context");
+    CNPC_REQUIRE(ctx, polls >= 0, "wait limit must be >= 0");
+    ctx->wait_limit = polls;
+    return CNPC_OK;
+}
+
+int cnpc_ctx_take_status(cnpc_ctx *ctx, cnpc_stream_t stream, int *h_status) {
+    CNPC_REQUIRE(ctx, ctx != nullptr, "null context");
+    CNPC_REQUIRE(ctx, h_status != nullptr, "null status pointer");
+    *h_status = CNPC_OK;
+    if (!ctx->d_status) return CNPC_OK;  // no bounded wait has run in this context
+    cudaStream_t s = (cudaStream_t)stream;
+    int v = 0;
+    int st = check_cuda(ctx, cudaMemcpyAsync(&v, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s),
+                        "status word read");
+    if (st) return st;
+    st = check_cuda(ctx, cudaStreamSynchronize(s), "status word read");
+    if (st) return st;
+    st = check_cuda(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s), "status word clear");
+    if (st) return st;
+    *h_status = v;
+    return CNPC_OK;
+}
 
 int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real, int64_t real_dist,
                  void *d_spec, cnpc_stream_t stream) {

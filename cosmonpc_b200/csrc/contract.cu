@@ -8,9 +8,11 @@
 // copies it with cp.async.bulk (the TMA engine's linear copy) into a
 // double-buffered shared-memory ring; an mbarrier with an expected byte count
 // tells the 16 warps when a stage has landed.  The next chunk streams in while
-// the current one is contracted.  Every mbarrier wait is bounded: a wait that
-// gives up records CNPC_ETIMEOUT in the status word, the block drains its own
-// copies (again bounded) and its outputs become NaN.
+// the current one is contracted.  Every mbarrier wait is bounded (the
+// context's wait limit, in polls): a wait that gives up records CNPC_ETIMEOUT
+// in the status word, the block drains its own copies (bounded by the fixed
+// kWaitLimit, so that no copy is in flight when the block exits) and its
+// outputs become NaN.
 //
 // Accumulation: FP32 fields accumulate TM*TN products per lane in FP32 for
 // about 64 cells, then the warp folds the 32 lane partials with a
@@ -36,6 +38,7 @@ constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up 
 struct GramParams {
     int na, nb, nunion, ncopy, g_row, ct, ntiles, ngroups, flush_chunks, nstages;
     int64_t ncell, field_stride;
+    long long wait_limit;  // polls of a pipeline wait before it gives up
     int a_slot[kMaxRows];
     int b_slot[kMaxRows];
     int union_field[kMaxUnion];
@@ -81,9 +84,10 @@ __device__ inline bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait; returns false if the barrier phase never completed.
-__device__ inline bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (long long i = 0; i < kWaitLimit; ++i)
+// Bounded wait; returns false if the barrier phase did not complete within
+// `limit` polls (0: give up at once).
+__device__ inline bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit = kWaitLimit) {
+    for (long long i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
         if (producer && issued < nchunk && !abort_flag) {
             const int sp = issued % NST;
             if (issued >= NST &&
-                !mbar_wait_bounded(&empty_bar[sp], (uint32_t)(((issued / NST) - 1) & 1))) {
+                !mbar_wait_bounded(&empty_bar[sp], (uint32_t)(((issued / NST) - 1) & 1), P.wait_limit)) {
                 abort_flag = 1;
                 atomicExch(status, (int)CNPC_ETIMEOUT);
             } else {
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
                 ++issued;
             }
         }
-        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / NST) & 1))) {
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)((k / NST) & 1), P.wait_limit)) {
             abort_flag = 1;
             if (lane == 0) atomicExch(status, (int)CNPC_ETIMEOUT);
         }
@@ -627,8 +631,11 @@ static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, i
     CNPC_REQUIRE(ctx, P.nstages >= 2, "too many staged rows for the shared-memory ring (max 110)");
     const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
     P.flush_chunks = 1 << 30;  // FP64 accumulators throughout
+    P.wait_limit = ctx->wait_limit;
     int st = check_cuda(ctx, cudaFuncSetAttribute(gram_kernel<T, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem), "gram smem attribute");
+    if (st) return st;
+    st = ensure_status(ctx);
     if (st) return st;
     const int64_t nchunks = (ncell + CHUNK - 1) / CHUNK;
     int64_t nxr = std::min<int64_t>(std::max<int64_t>(1, ctx->num_sms / P.ngroups), nchunks);
@@ -636,8 +643,10 @@ static int run_gram(cnpc_ctx *ctx, int64_t ncell, const T *g, const T *fields, i
     const size_t partial_bytes = (size_t)nblocks * NW * TM * TN * sizeof(double) + 256;
     st = ensure_scratch(ctx, partial_bytes, s);
     if (st) return st;
-    int *status = reinterpret_cast<int *>(static_cast<char *>(ctx->scratch) + ctx->scratch_bytes - 256);
-    gram_kernel<T, NW><<<(unsigned)nblocks, NW * 32, smem, s>>>(g, fields, P, (double *)ctx->scratch, status);
+    // a wait that gives up sets the context's status word (sticky until
+    // cnpc_ctx_take_status) and makes this call's outputs NaN
+    gram_kernel<T, NW><<<(unsigned)nblocks, NW * 32, smem, s>>>(g, fields, P, (double *)ctx->scratch,
+                                                                 ctx->d_status);
     st = check_launch(ctx, "gram_kernel");
     if (st) return st;
     const int nout = na * nb;
@@ -829,6 +838,7 @@ static int noalloc_gram_f64(int64_t ncell, const double *g, const double *fields
     if (P.nstages < 2) return CNPC_EINVAL;
     const size_t smem = (size_t)P.nstages * P.nunion * row_bytes;
     P.flush_chunks = 1 << 30;
+    P.wait_limit = kWaitLimit;
     const size_t per_block = (size_t)NW * TM * TN;
     const int64_t nchunks = (ncell + CHUNK - 1) / CHUNK;
     int64_t nxr = std::min<int64_t>(std::max<int64_t>(1, sms / P.ngroups), nchunks);

@@ -28,6 +28,11 @@ struct cnpc_ctx {
     void *shell_ws = nullptr;
     size_t shell_ws_bytes = 0;
     int num_sms = 148;
+    // status word of the bounded device waits (CNPC_OK or CNPC_ETIMEOUT),
+    // sticky until cnpc_ctx_take_status reads and clears it
+    int *d_status = nullptr;
+    // polls of a bounded mbarrier wait before it gives up
+    long long wait_limit = 1ll << 22;
 };
 
 namespace cnpc {
@@ -37,6 +42,7 @@ int check_cuda(cnpc_ctx *ctx, cudaError_t e, const char *what);
 int check_launch(cnpc_ctx *ctx, const char *what);
 int ensure_scratch(cnpc_ctx *ctx, size_t bytes, cudaStream_t stream);
 int ensure_buffer(cnpc_ctx *ctx, void **buf, size_t *have, size_t bytes, cudaStream_t stream);
+int ensure_status(cnpc_ctx *ctx);
 
 }  // namespace cnpc
 

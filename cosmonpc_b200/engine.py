@@ -436,6 +436,14 @@ class DeferredPairSums:
         self.k_bins = k_bins
         self.diagonal = diagonal
         self.blocks = []
+        # where the sums are computed: a NaN in them is checked against the
+        # context's device status word (a bounded wait that gave up)
+        self.ctx = _lib.Context.get()
+        self.stream = None if torch.cuda.is_current_stream_capturing() else torch.cuda.current_stream()
+
+    def _check_status(self, vals):
+        if np.isnan(vals).any() and self.stream is not None:
+            self.ctx.take_status(self.stream)  # raises DeviceTimeout after a timed-out wait
 
     def add(self, T, rows, cols, bi, bj):
         self.blocks.append((HostCopy(T), rows, cols, bi, bj))
@@ -449,13 +457,16 @@ class DeferredPairSums:
                    for _ in self.pair_specs]
         for hc, rows, cols, bi, bj in self.blocks:
             if cols is None:  # pair-list sums of the diagonal
-                lookup = dict(zip(rows, hc.get()))
+                vals = hc.get()
+                self._check_status(vals)
+                lookup = dict(zip(rows, vals))
                 t = lambda k1, k2: lookup.get((k1, k2), 0.0)
                 for r, ps in enumerate(self.pair_specs):
                     for b in bi:
                         results[r][b] = _assemble_entry(ps, t, b, b)
                 continue
             T = hc.get()
+            self._check_status(T)
             for r, ps in enumerate(self.pair_specs):
                 S = assemble(ps, T, rows, cols, bi, bj)
                 if self.diagonal:

@@ -91,6 +91,21 @@ const char *cnpc_status_string(int status);
 /* Library version as major*10000 + minor*100 + patch. */
 int cnpc_version(void);
 
+/* Failure detection of the device-side waits (no counterpart in the
+ * reference, which has no device code).  The FP64 contraction kernel
+ * (cnpc_contract_gram with CNPC_F64) waits on shared-memory mbarriers for its
+ * staged copies; every such wait gives up after `polls` checks (default
+ * 4194304, about a second; 0 gives up at the first check, which tests the
+ * failure path without hanging anything).  A wait that gives up lets the
+ * block drain its own copies, makes that call's outputs NaN and sets the
+ * context's status word to CNPC_ETIMEOUT. */
+int cnpc_ctx_set_wait_limit(cnpc_ctx *ctx, int64_t polls);
+/* Synchronises `stream`, stores the context's status word in *h_status
+ * (CNPC_OK, or CNPC_ETIMEOUT when a bounded wait gave up since the previous
+ * read) and clears it.  The word is sticky: several calls can be queued
+ * before one read. */
+int cnpc_ctx_take_status(cnpc_ctx *ctx, cnpc_stream_t stream, int *h_status);
+
 /* ------------------------------------------------------------------ paint
  * Replaces pmesh ParticleMesh.paint as called by pm_painter
  * (src/cosmonpc/mesh_generator.py:172-224, :199, :204-205).
@@ -407,14 +422,24 @@ int cnpc_contract_gram_tc(cnpc_ctx *ctx, int64_t ncell, const float *d_g, const 
  * library routine: the per-block partial sums live in one fixed 8 MiB array in
  * the library's device memory, which every GPU that loads the library holds
  * until the process exits.  The caller still owns G, the fields and d_out.
- *  - Limits per call: CNPC_F32 at most 48 rows x 24 columns (one contraction
- *    launch); CNPC_F64 at most 128 x 128 with 1 + pad8(na) [+ pad4(nb) when
- *    b is not a contiguous run of a] <= 110 staged rows.  Larger calls, or
+ *  - Limits per call: CNPC_F32 at most 48 rows x 24 columns with
+ *    1 + pad8(na) [+ pad4(nb) when b is not a contiguous run of a whose
+ *    padded window stays inside a's] <= 48 staged rows (so 40 x 24 with b
+ *    inside a, or 24 x 20 with b separate); CNPC_F64 at most 128 x 128 with
+ *    1 + pad8(na) [+ pad4(nb) likewise] <= 110 staged rows.  Larger calls, or
  *    misaligned fields (16-byte base, field_stride and ncell), return
  *    CNPC_EINVAL.
+ *  - The array bounds the grid: FP32 windows above about 24 x 12 outputs run
+ *    fewer blocks than cnpc_contract_gram (e.g. 163 instead of 2 per SM at
+ *    40 x 20), so they take longer than the regular call.
  *  - The first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress) and caches it; make that first call before any
- *    stream capture.
+ *    stream capture.  The cached address belongs to the device's primary
+ *    context: after cudaDeviceReset (or any teardown of that context) it is
+ *    stale, so do not call this entry point again in that process.
+ *  - A bounded device wait of the FP64 kernel that gives up (see
+ *    cnpc_ctx_set_wait_limit; here the default limit) is reported only
+ *    through NaN in d_out, since there is no context to hold a status word.
  *  - All calls share the array, so calls whose work overlaps on the GPU (on
  *    different streams, or from different threads) race and corrupt each
  *    other's partial sums: serialise them. */

@@ -197,12 +197,18 @@ def pk_box(field_a, field_b, correlation_mode, nmesh, boxsize, k_min, k_max, k_b
 # ------------------------------------------------------------- bk_sugi box
 def bk_sugi_box(field_a, field_b, field_c, correlation_mode, tracer_type, nmesh, boxsize,
                 k_min, k_max, k_bins, angu_config, sampler, data_vector_mode,
-                shotnoise_mode, N_gal, NZ, return_parts=False):
+                shotnoise_mode, N_gal, NZ, return_parts=False, bins=None):
     """``calculate_bk_sugi_box`` (ce:749-1555).
 
     ``N_gal`` / ``NZ`` are dicts keyed by tracer letter.  The shell fields are
     built without blocking: ``block_size`` only decides which fields are held at
     once in the reference (ce:911-981) and does not change the sums.
+
+    ``bins`` (full mode only): evaluate the triple sums of the signal and of the
+    FFT S3 term only for (k1, k2) pairs with both bins in this list; the other
+    entries of those matrices are NaN.  Every entry that is computed equals the
+    unrestricted run's (the sums of one pair do not depend on other bins), so a
+    large mesh can be checked on a fixed subset of its data vector.
     """
     l1, l2, L = angu_config
     n = int(nmesh)
@@ -235,6 +241,7 @@ def bk_sugi_box(field_a, field_b, field_c, correlation_mode, tracer_type, nmesh,
     same_tracer = correlation_mode == "auto" or tracer_type == "aab"
     leg2_src = ca if tracer_type in ("aaa", "aab") else cb
 
+    sel = list(range(k_bins)) if bins is None else sorted(set(int(b) for b in bins))
     if data_vector_mode == "full":
         total = np.zeros((k_bins, k_bins), dtype=np.complex128)
         for ss, (m1, m2, _) in enumerate(cfgs):
@@ -244,21 +251,25 @@ def bk_sugi_box(field_a, field_b, field_c, correlation_mode, tracer_type, nmesh,
             w2 = leg2_src * y2
             eq = same_tracer and l1 == l2 and m1 == m2
             cj = same_tracer and l1 == l2 and m1 == -m2
-            F1 = [_inv(w1 * mk) for mk in masks]
-            sub = np.zeros((k_bins, k_bins), dtype=np.complex128)
+            F1 = {i: _inv(w1 * masks[i]) for i in sel}
+            sub = np.full((k_bins, k_bins), np.nan, dtype=np.complex128)
             if eq or cj:
-                for i in range(k_bins):
-                    for j in range(i, k_bins):
+                for i in sel:
+                    for j in sel:
+                        if j < i:
+                            continue
                         F2 = F1[j] if eq else (-1) ** (m1 + l1) * np.conj(F1[j])
                         sub[i, j] = tj[ss] * np.sum(G * F1[i] * F2)
-                for i in range(k_bins):
-                    for j in range(i + 1, k_bins):
-                        sub[j, i] = sub[i, j] if eq else np.conj(sub[i, j])
+                for i in sel:
+                    for j in sel:
+                        if j > i:
+                            sub[j, i] = sub[i, j] if eq else np.conj(sub[i, j])
             else:
-                F2 = [_inv(w2 * mk) for mk in masks]
-                for i in range(k_bins):
-                    for j in range(k_bins):
+                F2 = {j: _inv(w2 * masks[j]) for j in sel}
+                for i in sel:
+                    for j in sel:
                         sub[i, j] = tj[ss] * np.sum(G * F1[i] * F2[j])
+            del F1
             total += sub if (m1, m2) == (0, 0) else 2 * np.real(sub)
     else:
         total = np.zeros(k_bins, dtype=np.complex128)
@@ -365,13 +376,14 @@ def bk_sugi_box(field_a, field_b, field_c, correlation_mode, tracer_type, nmesh,
                 cj = l1 == l2 and m1 == -m2
                 yc1 = np.conj(angular.ylm_function(l1, m1, True)(*khat))
                 yc2 = np.conj(angular.ylm_function(l2, m2, True)(*khat))
-                S1 = [_inv(yc1 * mk) for mk in masks]
+                use = sel if full else list(range(k_bins))
+                S1 = {i: _inv(yc1 * masks[i]) for i in use}
                 if eq:
                     S2 = S1
                 elif cj:
-                    S2 = [(-1) ** (m1 + l1) * np.conj(s) for s in S1]
+                    S2 = {i: (-1) ** (m1 + l1) * np.conj(v) for i, v in S1.items()}
                 else:
-                    S2 = [_inv(yc2 * mk) for mk in masks]
+                    S2 = {i: _inv(yc2 * masks[i]) for i in use}
                 if not full:
                     sub = np.zeros(k_bins, dtype="complex128")
                     for i in range(k_bins):
@@ -379,15 +391,23 @@ def bk_sugi_box(field_a, field_b, field_c, correlation_mode, tracer_type, nmesh,
                             sub[i] = tj[ss] * np.sum(src * S1[i] * S2[i]) / k_num[i] ** 2
                 else:
                     sub = np.zeros((k_bins, k_bins), dtype="complex128")
+                    if bins is not None:
+                        sub[:] = np.nan
+                        for i in sel:
+                            for j in sel:
+                                sub[i, j] = 0.0
                     sym = eq or cj
-                    for i in range(k_bins):
-                        for j in range(i if sym else 0, k_bins):
+                    for i in sel:
+                        for j in sel:
+                            if sym and j < i:
+                                continue
                             if k_num[i] > 0 and k_num[j] > 0:
                                 sub[i, j] = tj[ss] * np.sum(src * S1[i] * S2[j]) / (k_num[i] * k_num[j])
                     if sym:
-                        for i in range(k_bins):
-                            for j in range(i + 1, k_bins):
-                                sub[j, i] = sub[i, j] if eq else np.conj(sub[i, j])
+                        for i in sel:
+                            for j in sel:
+                                if j > i:
+                                    sub[j, i] = sub[i, j] if eq else np.conj(sub[i, j])
                 s3 += sub if (m1, m2) == (0, 0) else 2.0 * np.real(sub)
             return s3 * (H_ells * N_ells) / N3
 

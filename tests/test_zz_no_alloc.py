@@ -19,8 +19,17 @@ pytestmark = pytest.mark.gpu
 TOL = {"f64": 1e-8, "f32": 1e-5}
 
 
-@pytest.mark.parametrize("precision,na,nb", [("f32", 40, 20), ("f32", 20, 20), ("f64", 40, 20), ("f64", 12, 7)])
-def test_noalloc_matches_gram_twice(precision, na, nb):
+# (rows, columns): columns a run of the rows (staged once), columns outside
+# the rows (staged separately), and a 40 x 24 FP32 window (41 staged rows),
+# where the fixed array, not the SM count, bounds the number of blocks
+CASES = [("f32", list(range(40)), list(range(5, 25))), ("f32", list(range(20)), list(range(20))),
+         ("f32", list(range(16)), list(range(20, 28))), ("f32", list(range(40)), list(range(16, 40))),
+         ("f64", list(range(40)), list(range(5, 25))), ("f64", list(range(12)), list(range(7))),
+         ("f64", list(range(12)), list(range(30, 37)))]
+
+
+@pytest.mark.parametrize("precision,a,b", CASES)
+def test_noalloc_matches_gram_twice(precision, a, b):
     import torch
 
     from cosmonpc_b200 import _lib, engine
@@ -30,11 +39,10 @@ def test_noalloc_matches_gram_twice(precision, na, nb):
     lib = _lib.load()
     n = 64
     ncell = n ** 3
-    gen = torch.Generator(device="cuda").manual_seed(7 + na)
+    na, nb = len(a), len(b)
+    gen = torch.Generator(device="cuda").manual_seed(7 + na + 100 * b[0])
     fields = torch.randn((48, ncell), dtype=rdt, device="cuda", generator=gen)
     G = torch.randn(ncell, dtype=rdt, device="cuda", generator=gen)
-    a = list(range(na))
-    b = list(range(5, 5 + nb)) if na >= 5 + nb else list(range(nb))
     ref = torch.empty((na, nb), dtype=torch.float64, device="cuda")
     ctx.gram(code, ncell, G, fields, ncell, a, b, ref)
     aa = (ctypes.c_int * na)(*a)
