@@ -270,28 +270,34 @@ def _survey_runs(seed, reps, scale=1.0):
 # ----------------------------------------------------------------- main
 def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
     """mocks/s of the fast form (FP32 fields, one paint per mock, the next mock
-    queued before the previous one's results are read) with every mock resident
-    in HBM, and of the plain FP64 per-call path (separate pk and bk calls) on one
+    queued before the previous one's results are read, each class's device work
+    replayed from CUDA graphs captured at the class's largest count) on
+    lognormal mocks of Poisson-varying particle counts (mean 1.5e6) resident in
+    HBM, and of the plain FP64 per-call path (separate pk and bk calls) on one
     mock per class.  With N ranks each rank runs its own per_class mocks per
     class and the rate is the whole job's (N x mocks over the slowest rank)."""
     import torch
 
     from cosmonpc_b200 import api, replicas
-    from cosmonpc_b200.mocks import lognormal_box_exact
+    from cosmonpc_b200.mocks import lognormal_box
 
     M = MOCKS
     fast_s, plain_s, total = 0.0, 0.0, 0
     classes = {}
+    counts_all = []
     for ci, (n, L) in enumerate(MOCK_CLASSES):
-        cats = [torch.from_numpy(lognormal_box_exact(M["n_particles"], L, seed + 1000 * ci + i)).cuda()
+        # mock i of the workload uses seed + i (i = 0..95 over the three classes)
+        cats = [torch.from_numpy(lognormal_box(M["n_particles"], L, seed + per_class * ci + i)).cuda()
                 for i in range(per_class)]
+        counts = [int(c.shape[0]) for c in cats]
+        counts_all += counts
         kw = dict(nmesh=n, boxsize=L, sampler=M["sampler"], interlaced=M["interlaced"], k_min=M["k_min"],
                   k_max=M["k_max"], k_bins=M["k_bins"], poles=M["poles"], angu_configs=M["angu_configs"],
                   data_vector_mode=M["data_vector_mode"], shotnoise_mode=M["shotnoise_mode"])
         api.mock_pk_bk(cats[0], None, precision="f32", **kw)  # warm-up: plans and buffers of this class
         graphs = None
         try:  # the device work of a mock replayed from CUDA graphs (captured outside the timed region)
-            graphs = api.MockGraphs(M["n_particles"], **kw)
+            graphs = api.MockGraphs(max(counts), **kw)
             submit = graphs.submit
             mode = "cuda_graph"
         except RuntimeError:
@@ -318,8 +324,11 @@ def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
         e1.record()
         barrier()
         tp = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
-        classes["%d^3/L%d" % (n, L)] = {"fast_s_per_mock": tf / len(cats), "plain_s_per_mock": tp, "mode": mode}
-        del graphs
+        classes["%d^3/L%d" % (n, L)] = {"fast_s_per_mock": tf / len(cats), "plain_s_per_mock": tp, "mode": mode,
+                                        "counts": [min(counts), max(counts)]}
+        if graphs is not None:
+            graphs.close()
+        del graphs, submit
         fast_s += tf
         plain_s += tp * len(cats)
         total += len(cats)
@@ -327,8 +336,10 @@ def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
     return {"value": replicas.job_rate(total, fast_s, world), "unit": "mocks/s",
             "plain_value": replicas.job_rate(total, plain_s, world),
             "speedup": plain_s / fast_s, "mocks": total, "per_class": classes,
-            "workload": "pk [0,2,4] + bk_sugi (0,0,0) diagonal, 15 bins 0.01-0.16, CIC interlaced, "
-                        "lognormal mocks of exactly 1.5e6 particles; classes 128^3/L1000, 192^3/L1500, 256^3/L2000"}
+            "counts": {"min": min(counts_all), "max": max(counts_all), "mean": sum(counts_all) / len(counts_all)},
+            "workload": "pk [0,2,4] + bk_sugi (0,0,0) diagonal, 15 bins 0.01-0.16, CIC interlaced, lognormal "
+                        "mocks of Poisson-varying counts (mean 1.5e6); classes 128^3/L1000, 192^3/L1500, "
+                        "256^3/L2000"}
 
 
 def main():
@@ -341,7 +352,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mocks", type=int, default=4, help="mocks per shape class for the mocks/s line (0: skip)")
+    ap.add_argument("--mocks", type=int, default=32, help="mocks per shape class for the mocks/s line (0: skip)")
     ap.add_argument("--streams", type=int, default=2, help="CUDA streams the back-to-back data vectors rotate over")
     ap.add_argument("--survey", action="store_true",
                     help="time the survey cross workload (512^3, 2e6 data, 4e7 randoms) instead; one JSON line")
@@ -570,7 +581,7 @@ def main():
     # ---- batched mocks (pk + bk diagonal per mock, three shape classes)
     mocks = None
     if args.mocks > 0:
-        mocks = _mocks_throughput(args.mocks, seed + 100 * rank, barrier, max_over_ranks, world)
+        mocks = _mocks_throughput(args.mocks, BASE_SEED + 5 + 1000 * rank, barrier, max_over_ranks, world)
 
     if rank != 0:
         if dist is not None:
@@ -591,13 +602,27 @@ def main():
         cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     survey = None
     if world == 1 and args.survey_steps > 0:
-        t, nd, nr = _survey_runs(BASE_SEED + 4, args.survey_steps, args.survey_scale)
-        f32 = sum(v for k, v in t.items() if k.endswith("f32"))
-        f64 = sum(v for k, v in t.items() if k.endswith("f64"))
-        survey = {"value": f32, "unit": "s/data-vector", "plain_f64": f64, "speedup": f64 / f32,
-                  "catalogs": {"data": nd, "randoms": nr}, "per_call_s": t,
-                  "workload": "survey cross, 512^3, L3500, TSC interlaced, mixed-mesh: pk cross [0,2,4] + "
-                              "bk_sugi aab (000) and (202) diagonal; three run_stats calls, FITS reads included"}
+        # the 512^3 FP64 survey path needs most of the device: release this
+        # process's pools and contexts and time it in a fresh process
+        import gc
+
+        del pos_dev
+        _engine.clear_unit_shell_cache()
+        _lib.Context.release_all()
+        gc.collect()
+        torch.cuda.empty_cache()
+        proc = subprocess.run([sys.executable, os.path.abspath(__file__), "--survey", "--steps",
+                               str(args.survey_steps), "--survey-scale", str(args.survey_scale)],
+                              capture_output=True, text=True)
+        try:
+            sv = json.loads(proc.stdout.strip().splitlines()[-1])
+            survey = {"value": sv["value"], "unit": sv["unit"], "plain_f64": sv["plain_f64"],
+                      "speedup": sv["speedup"], "catalogs": sv["catalogs"], "per_call_s": sv["per_call_s"],
+                      "workload": "survey cross, 512^3, L3500, TSC interlaced, mixed-mesh: pk cross [0,2,4] + "
+                                  "bk_sugi aab (000) and (202) diagonal; three run_stats calls, FITS reads "
+                                  "included"}
+        except Exception:
+            survey = {"error": (proc.stderr or proc.stdout)[-400:]}
     mocks_short = None
     if mocks is not None:
         mocks_short = {k: mocks[k] for k in ("value", "unit", "plain_value", "speedup", "mocks")}

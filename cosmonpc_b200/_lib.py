@@ -290,6 +290,17 @@ class Context:
             self.lib.cnpc_ctx_destroy(self.h)
             self.h = None
 
+    @classmethod
+    def release_all(cls):
+        """Destroy every cached context (plans, workspaces) after synchronising
+        the device; later calls create fresh ones."""
+        import torch
+
+        torch.cuda.synchronize()
+        for ctx in list(cls._per_device.values()):
+            ctx.close()
+        cls._per_device.clear()
+
     # ----------------------------------------------------------- helpers
     def _check(self, st, what):
         if st == CNPC_OK:

@@ -107,15 +107,18 @@ def pk_box_vector(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max
 
 def mock_pk_bk(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k_bins, poles=(0, 2, 4),
                angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana", precision="f32",
-               rsd=(0, 0, 1), deferred=False):
+               rsd=(0, 0, 1), deferred=False, sum_w=None):
     """Power-spectrum multipoles and bispectrum configurations of one mock from a
     single paint: the interlaced R2C spectra are finished twice (the power
     spectrum and the bispectrum overdensity use different scalings and k = 0
     values).  Returns (pk result dict, [bk result dict per configuration]), or
     with ``deferred`` a function returning them, after the device work of this
     mock is queued, so that the next mock can be queued before the results are
-    read."""
-    wsum = _weight_sum(pos, weight)
+    read.  ``sum_w``: the weight sum when it is known (no device read).  The
+    deferred function takes an optional ``n_gal`` (and ``sn_unit``, see
+    ``clustering_estimator.bk_sugi_box_submit``) for a catalog whose real count
+    differs from the rows painted (zero-weight padding)."""
+    wsum = _weight_sum(pos, weight) if sum_w is None else float(sum_w)
     dpos, dw = _to_device(pos, weight)
     pm = engine.paint(dpos, dw, nmesh, boxsize, sampler, interlaced, precision, sum_w=wsum)
     pm_bk = engine.PaintedMesh(pm.raw.clone(), pm.n, pm.boxsize, pm.sampler, pm.interlaced, pm.N_gal, pm.sum_w,
@@ -129,67 +132,126 @@ def mock_pk_bk(pos, weight, nmesh, boxsize, sampler, interlaced, k_min, k_max, k
                       shotnoise_mode=shotnoise_mode, **common)
     bk = ce.bk_sugi_box_submit({"a": pm_bk}, "auto", "aaa", [tuple(c) for c in angu_configs], attrs,
                                precision=precision, block_size=None)
-    finalize = lambda: (pk(), bk())
+    volume = float(boxsize) ** 3
+
+    def finalize(n_gal=None, sn_unit=None):
+        if n_gal is None:
+            return pk(), bk()
+        return pk(NZ_a=float(n_gal) / volume), bk(n_gal=int(n_gal), sn_unit=sn_unit)
+
     return finalize if deferred else finalize()
 
 
 class MockGraphs:
-    """:func:`mock_pk_bk` for a stream of same-shaped mocks, replayed from CUDA
-    graphs: the device work of one mock (paint, transforms, shell fields,
-    contractions, copies of the sums to pinned host memory) is captured once
-    per slot and replayed for every mock, so the host no longer issues ~100
-    launches per mock.  Catalogs must have ``npart`` particles (no weights)
-    inside the box.  ``submit(pos)`` copies ``pos`` into the slot's input,
-    replays, and returns a function that waits for that replay and returns
-    (pk result, [bk results]); call it before submitting ``slots`` more mocks.
+    """:func:`mock_pk_bk` for a stream of mocks of one shape class (mesh, box,
+    settings) replayed from CUDA graphs: the device work of one mock (paint,
+    transforms, shell fields, contractions, copies of the sums to pinned host
+    memory) is captured once per slot and replayed for every mock, so the host
+    no longer issues ~100 launches per mock.
 
-    Raises RuntimeError when the device work cannot be captured (then use
-    :func:`mock_pk_bk`)."""
+    Catalogs may hold any number of particles up to ``capacity`` (no weights,
+    inside the box): a slot's input is a ``capacity``-row catalog with
+    per-particle weights; a catalog of N particles fills the first N rows with
+    weight 1 and the rest with weight 0 at the origin, so the captured paint
+    deposits exactly the catalog's mass.  The count enters only the host
+    algebra (N_gal, the number density, the normalisation) and the analytic
+    shot-noise sums, which are linear in the count and are moved from the
+    captured one with the sums of a zero spectrum (``sn_unit``, computed once
+    per class).  The FFT S3 term of (0,0,0) depends on the count through its
+    source field, so with shotnoise_mode "fft"/"both" and (0,0,0) every catalog
+    must have exactly ``capacity`` particles.
 
-    def __init__(self, npart, nmesh, boxsize, slots=2, **kw):
+    ``submit(pos)`` copies ``pos`` into the slot's input, replays, and returns a
+    function that waits for that replay and returns (pk result, [bk results]);
+    call it before submitting ``slots`` more mocks.  Raises RuntimeError when
+    the device work cannot be captured (then use :func:`mock_pk_bk`)."""
+
+    def __init__(self, capacity, nmesh, boxsize, slots=2, **kw):
         from . import _lib
 
         self.kw = dict(kw, nmesh=nmesh, boxsize=boxsize)
+        self.capacity = int(capacity)
         self.slots = []
         self.count = 0
+        cfgs = [tuple(c) for c in kw.get("angu_configs", ((0, 0, 0),))]
+        self.fixed_count = kw.get("shotnoise_mode", "ana") != "ana" and (0, 0, 0) in cfgs
         dev = torch.device("cuda", torch.cuda.current_device())
+        self.sn_unit = self._sn_unit(dev)
         for _ in range(slots):
             # each slot: its own stream and library context, so replays of
             # different slots share no workspace and can overlap
             ctx = _lib.Context(dev.index)
             stream = torch.cuda.Stream(dev)
-            pos = torch.empty((int(npart), 3), dtype=torch.float64, device=dev)
+            pos = torch.empty((self.capacity, 3), dtype=torch.float64, device=dev)
             pos.uniform_(0.0, float(boxsize) * (1.0 - 1e-12))
+            w = torch.ones(self.capacity, dtype=torch.float64, device=dev)
             stream.wait_stream(torch.cuda.current_stream(dev))
             with _lib.Context.scope(ctx):
                 with torch.cuda.stream(stream):
                     for _ in range(2):  # plans, workspaces and pinned buffers at their final sizes
-                        mock_pk_bk(pos, None, **self.kw)
+                        mock_pk_bk(pos, w, sum_w=self.capacity, **self.kw)
                 stream.synchronize()
                 graph = torch.cuda.CUDAGraph()
                 try:
                     with torch.cuda.graph(graph, stream=stream, capture_error_mode="relaxed"):
-                        fin = mock_pk_bk(pos, None, deferred=True, **self.kw)
+                        fin = mock_pk_bk(pos, w, deferred=True, sum_w=self.capacity, **self.kw)
                 except Exception as e:  # a host synchronisation or allocation inside the work
                     raise RuntimeError("mock pipeline could not be captured: %s" % e) from e
-            self.slots.append((pos, graph, fin, stream, ctx))
+            self.slots.append((pos, w, graph, fin, stream, ctx))
+
+    def _sn_unit(self, dev):
+        """{L: k3-bin shot-noise sums of a zero spectrum with sn0 = 1} for the
+        configurations whose sums depend on the count ((0,0,0) of an auto run)."""
+        from . import _lib
+
+        kw = self.kw
+        if (0, 0, 0) not in [tuple(c) for c in kw.get("angu_configs", ((0, 0, 0),))]:
+            return {}
+        n, L = int(kw["nmesh"]), float(kw["boxsize"])
+        precision = kw.get("precision", "f32")
+        code, _, cdt = engine.PRECISION[precision]
+        k_min, k_max, k_bins = kw["k_min"], kw["k_max"], kw["k_bins"]
+        k3_edge = np.linspace(2 * k_min, 2 * k_max, k_bins * 2 + 1)[:-1]
+        zero = torch.zeros((n, n, n // 2 + 1), dtype=cdt, device=dev)
+        d = torch.empty(2 * (len(k3_edge) - 1), dtype=torch.float64, device=dev)
+        _lib.Context.get().sn_bins(code, n, L, zero, zero, (L ** 3) ** 2, 1.0, _lib.WINDOW[kw["sampler"]], None,
+                                   k3_edge, d)
+        return {0: d.cpu().numpy()}
+
+    def close(self):
+        """Release the captured graphs, their memory pools and the slots' library
+        contexts (cuFFT plans and workspaces)."""
+        for (_, _, graph, _, stream, ctx) in self.slots:
+            stream.synchronize()
+            del graph
+            ctx.close()
+        self.slots = []
 
     def submit(self, pos):
-        inp, graph, fin, stream, _ = self.slots[self.count % len(self.slots)]
+        inp, w, graph, fin, stream, _ = self.slots[self.count % len(self.slots)]
+        npart = int(pos.shape[0])
+        if pos.ndim != 2 or pos.shape[1] != 3 or npart > self.capacity or npart < 1:
+            raise ValueError("catalog of shape %s does not fit the captured capacity %d"
+                             % (tuple(pos.shape), self.capacity))
+        if self.fixed_count and npart != self.capacity:
+            raise ValueError("with FFT shot noise of (0,0,0) every catalog needs exactly %d particles" % self.capacity)
         self.count += 1
-        if tuple(pos.shape) != tuple(inp.shape):
-            raise ValueError("catalog shape %s differs from the captured %s" % (tuple(pos.shape), tuple(inp.shape)))
         stream.wait_stream(torch.cuda.current_stream())  # pos was written on the caller's stream
         with torch.cuda.stream(stream):
-            inp.copy_(pos, non_blocking=True)
+            inp[:npart].copy_(pos, non_blocking=True)
+            w[:npart].fill_(1.0)
+            if npart < self.capacity:
+                inp[npart:].zero_()
+                w[npart:].zero_()
             graph.replay()
             done = torch.cuda.Event()
             done.record()
         pos.record_stream(stream)
+        sn_unit = self.sn_unit
 
         def finalize():
             done.synchronize()
-            return fin()
+            return fin(n_gal=npart, sn_unit=sn_unit)
 
         return finalize
 

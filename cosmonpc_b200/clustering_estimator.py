@@ -54,8 +54,13 @@ def calculate_power_spectrum_box(rfield_a, rfield_b, correlation_mode, stat_attr
         dsum = torch.empty((len(even), k_bins), dtype=torch.float64, device=ca.device)
         ctx.pk_bins(code, n, L, ca, cb, k_edge, even, rsd, dsum)
         dsum = engine.HostCopy(dsum)
-    finalize = lambda: _pk_box_results(counts, dsum, poles, even, k_bins, correlation_mode, boxsize, nmesh,
-                                       NZ_a, NZ_b, P_shot)
+    def finalize(NZ_a=NZ_a):
+        """``NZ_a``: the number density of a catalog whose device work ran with
+        another count (a padded CUDA-graph capture); only host algebra uses it."""
+        P_shot = 1.0 / NZ_a if correlation_mode == "auto" else 0.0
+        return _pk_box_results(counts, dsum, poles, even, k_bins, correlation_mode, boxsize, nmesh, NZ_a, NZ_b,
+                               P_shot)
+
     return finalize if kwargs.get("deferred") else finalize()
 
 
@@ -297,16 +302,34 @@ def bk_sugi_box_submit(meshes, correlation_mode, tracer_type, angu_configs, stat
             legs = [ps.leg1 for ps in all_sp] + [ps.leg2 for ps in all_sp if ps.mode == "leg"]
             shell_origin = engine.unit_shell_origin(n, L, k_edge, precision, legs)
 
-    return lambda: _bk_box_results(
-        angu_configs, tracer_type, correlation_mode, diagonal, shotnoise_mode, shotnoise_ana_all_eff, k_bins,
-        k_edge, k3_center, nmesh, V, vol_per_cell, N_gal, counts_k, counts_k3, sn_sums, cfg_info, s3fft,
-        s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg)
+    def finalize(n_gal=None, sn_unit=None):
+        """Host algebra once the device work is queued.  ``n_gal`` (auto
+        correlation): the catalog's real count when the device work ran with
+        another one (a padded CUDA-graph capture, zero-weight padding); the
+        analytic shot-noise sums are then moved from the captured sn0 to n_gal
+        with ``sn_unit[L]``, the k3-bin sums of the same kernel for a zero
+        spectrum and sn0 = 1 (the sums are linear in sn0)."""
+        return _bk_box_results(
+            angu_configs, tracer_type, correlation_mode, diagonal, shotnoise_mode, shotnoise_ana_all_eff, k_bins,
+            k_edge, k3_center, nmesh, V, vol_per_cell, N_gal, counts_k, counts_k3, sn_sums, cfg_info, s3fft,
+            s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg, n_gal, sn_unit)
+
+    return finalize
 
 
 def _bk_box_results(angu_configs, tracer_type, correlation_mode, diagonal, shotnoise_mode, shotnoise_ana_all_eff,
                     k_bins, k_edge, k3_center, nmesh, V, vol_per_cell, N_gal, counts_k, counts_k3, sn_sums,
-                    cfg_info, s3fft, s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg):
+                    cfg_info, s3fft, s3_groups, s3_index, src_origin, shell_origin, signal, per_cfg,
+                    n_gal=None, sn_unit=None):
     """Host algebra of bk_sugi_box_multi, run once the device work is queued."""
+    sn_captured = list(cfg_info)
+    if n_gal is not None and n_gal != N_gal["a"]:
+        if correlation_mode != "auto":
+            raise ValueError("a count override is defined for auto correlations only")
+        if shotnoise_mode != "ana" and any(sn_captured):
+            raise ValueError("a count override needs shotnoise_mode 'ana' (the FFT S3 source depends on the count)")
+        N_gal = {"a": int(n_gal)}
+        cfg_info = [float(n_gal) if sn0 else 0.0 for sn0 in sn_captured]
     k_center = 0.5 * (k_edge[1:] + k_edge[:-1])
     k3_bins = len(k3_center)
     ck = counts_k.get()
@@ -325,7 +348,9 @@ def _bk_box_results(angu_configs, tracer_type, correlation_mode, diagonal, shotn
             SN0, SN1, SN2, SN3 = 0.0, 0.0, 0.0, 0.0
         else:
             SN0 = cfg_info[ci]
-            dd = sn_sums[(L_, SN0)].get()[:2 * k3_bins]
+            dd = sn_sums[(L_, sn_captured[ci])].get()[:2 * k3_bins]
+            if SN0 != sn_captured[ci]:
+                dd = dd + (SN0 - sn_captured[ci]) * np.asarray(sn_unit[L_])[:2 * k3_bins]
             total_sum = dd[0::2] + 1j * dd[1::2]
             SN1, SN2 = 0.0, 0.0
             if l1 == L_ and l2 == 0:

@@ -372,19 +372,27 @@ def test_multi_weight_gram_matches_separate_launches(ngs, rows, nb, shared):
         r0 += r
 
 
-def test_mock_graphs_match_eager():
+@pytest.mark.parametrize("shotnoise_mode", ["ana", "both"])
+def test_mock_graphs_match_eager(shotnoise_mode):
     """MockGraphs (the mock pipeline replayed from CUDA graphs, two slots)
-    against eager mock_pk_bk on three fixed-size catalogs in a row; a catalog
-    of another size is refused."""
+    against eager mock_pk_bk on catalogs of uneven (Poisson-varying) particle
+    counts, replayed back to back; a catalog above the capacity is refused, and
+    with FFT shot noise of (0,0,0) only the captured count is accepted."""
     import torch
     from cosmonpc_b200 import api
-    from cosmonpc_b200.mocks import lognormal_box_exact
+    from cosmonpc_b200.mocks import lognormal_box
 
-    n, L, npart = 64, 500.0, 100000
+    n, L = 64, 500.0
     kw = dict(sampler="cic", interlaced=True, k_min=0.01, k_max=0.16, k_bins=15, poles=(0, 2, 4),
-              angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode="ana")
-    graphs = api.MockGraphs(npart, n, L, **kw)
-    cats = [torch.from_numpy(lognormal_box_exact(npart, L, 900 + i)).cuda() for i in range(3)]
+              angu_configs=((0, 0, 0),), data_vector_mode="diagonal", shotnoise_mode=shotnoise_mode)
+    cats = [torch.from_numpy(lognormal_box(100000, L, 900 + i)).cuda() for i in range(4)]
+    counts = [int(c.shape[0]) for c in cats]
+    if shotnoise_mode == "ana":
+        assert len(set(counts)) == len(counts)  # Poisson-varying
+        graphs = api.MockGraphs(max(counts) + 17, n, L, **kw)
+    else:
+        cats = [c[:min(counts)] for c in cats]
+        graphs = api.MockGraphs(min(counts), n, L, **kw)
     pending, got = None, []
     for c in cats:
         fin = graphs.submit(c)
@@ -397,10 +405,18 @@ def test_mock_graphs_match_eager():
         for key in ("P0", "P2", "P4"):
             assert rel_err(pk[key], ref_pk[key]) < 1e-6, key
         for bk, ref in zip(bks, ref_bks):
-            for key in ("B_sugi", "Bk_raw", "Shot_noise"):
-                assert rel_err(bk[key], ref[key]) < 1e-6, key
+            keys = ("B_sugi", "Bk_raw", "Shot_noise") + (("SN3_FFT",) if shotnoise_mode == "both" else ())
+            for key in keys:
+                g = bk["SN_terms"][key] if key == "SN3_FFT" else bk[key]
+                r = ref["SN_terms"][key] if key == "SN3_FFT" else ref[key]
+                assert rel_err(g, r) < 1e-6, key
+            assert bk["I_norm"] == pytest.approx(ref["I_norm"], rel=1e-15)
     with pytest.raises(ValueError):
-        graphs.submit(cats[0][:-1])
+        graphs.submit(torch.cat([cats[0], cats[1]]))
+    if shotnoise_mode == "both":
+        with pytest.raises(ValueError):
+            graphs.submit(cats[0][:-1])
+    graphs.close()
 
 
 def test_unit_shell_cache_matches_fresh_shells():
