@@ -31,6 +31,7 @@ EXPORTED = (
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
     "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
     "cnpc_forward_finish_band", "cnpc_ctx_set_wait_limit", "cnpc_ctx_take_status",
+    "cnpc_contract_gram_tc_multi_g",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -129,6 +130,8 @@ _SIGS = {
     "cnpc_contract_gram_tc": [_vp, _i64, _vp, _vp, _i64, _ip, _i, _ip, _i, _vp, _vp],
     "cnpc_contract_gram_multi_g": [_vp, _i64, ctypes.POINTER(_vp), _i, _vp, _i64, _ip, _ip, _i, _ip, _i, _vp,
                                    _vp],
+    "cnpc_contract_gram_tc_multi_g": [_vp, _i64, ctypes.POINTER(_vp), _i, _vp, _i64, _ip, _ip, _i, _ip, _i, _vp,
+                                      _vp],
     "cnpc_ctx_set_wait_limit": [_vp, _i64],
     "cnpc_ctx_take_status": [_vp, _vp, _ip],
 }
@@ -467,6 +470,19 @@ class Context:
         self._check(st, "cnpc_contract_gram_tc")
         _count("gram_tc")
         _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + 1) * ncell * 4)
+
+    def gram_tc_multi_g(self, ncell, gs, fields, stride, a_idx, a_g, b_idx, out):
+        """Tensor-core FP32 Gram whose row i is weighted by gs[a_g[i]] (one launch)."""
+        a, ap = _iarr(a_idx)
+        ag, agp = _iarr(a_g)
+        b, bp = _iarr(b_idx)
+        garr = (_vp * len(gs))(*[_ptr(t) for t in gs])
+        e0 = _tstart()
+        st = self.lib.cnpc_contract_gram_tc_multi_g(self.h, ncell, garr, len(gs), _ptr(fields), stride, ap, agp,
+                                                    len(a), bp, len(b), _ptr(out), self.stream())
+        self._check(st, "cnpc_contract_gram_tc_multi_g")
+        _count("gram_tc")
+        _tstop("gram", e0, (len(set(a_idx) | set(b_idx)) + len(gs)) * ncell * 4)
 
     def gram_multi_g(self, ncell, gs, fields, stride, a_idx, a_g, b_idx, out):
         """FP32 Gram whose row i is weighted by gs[a_g[i]] (one launch)."""

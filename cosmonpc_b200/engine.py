@@ -136,11 +136,14 @@ FIELD_PAD = 0
 FUSED_SHELLS = True
 
 
-# FP32 Gram blocks on the tensor cores (cnpc_contract_gram_tc, TF32 pairs)
-# instead of the CUDA-core FFMA kernel.  Off by default: at 256^3 with 40 x 20
-# outputs the tcgen05 kernel takes 3.4 ms against 1.0 ms for the FFMA kernel
-# (its MMA stream alone takes 0.75 ms; per-chunk CTA synchronisation and the
-# accumulator folds dominate the rest).
+# FP32 Gram blocks on the tensor cores (cnpc_contract_gram_tc[_multi_g], TF32
+# pairs, A operand in tensor memory) instead of the CUDA-core FFMA kernel.
+# Off by default: at 256^3 with 40 x 20 outputs the tensor-core kernel takes
+# 3.26 ms against 0.85 ms for the FFMA kernel.  Its tensor pipe is 5.6 %
+# active; the CUDA-core operand preparation (G F products and hi/lo splits
+# for 128 TMEM lanes plus 48 B rows per cell, ~74 warp instructions per cell
+# at 0.36 IPC per scheduler) costs more issue slots than the FFMA contraction
+# itself (800 FMAs = 400 packed FFMA2 per cell for 40 x 20).
 GRAM_TC = False
 
 # FP32 Gram blocks of several weight fields (the FFT S3 sums of several
@@ -323,9 +326,9 @@ def contract(G, sf, rows, cols):
 
     tc = sf.precision == "f32" and GRAM_TC
     if sf.precision == "f32":
-        # one FP32 contraction launch covers at most 64 rows x 32 columns on the
+        # one FP32 contraction launch covers at most 40 rows x 24 columns on the
         # tensor cores, 48 x 24 on the CUDA cores
-        rb, cb = (64, 32) if tc else (48, 24)
+        rb, cb = (40, 24) if tc else (48, 24)
         if len(ridx) <= rb and len(cidx) <= cb:
             blocks = [(0, len(ridx), 0, len(cidx))]
         else:
@@ -539,10 +542,13 @@ def _launch_groups(sf, rows_g, cols_g):
     columns share one multi-weight launch while rows <= 48, columns <= 24 and
     at most 4 weights; the rest get a launch each."""
     plan = []
-    if sf.precision != "f32" or not GRAM_MULTI or GRAM_TC:
+    if sf.precision != "f32" or not GRAM_MULTI:
         return [[gi] for gi in range(len(rows_g))]
 
     def fits(members):
+        if GRAM_TC:  # one tensor-core launch: <= 40 rows, <= 24 columns, <= 4 weights
+            nr = sum(len(rows_g[j]) for j in members)
+            return nr <= 40 and len(cols_g[members[0]]) <= 24 and len(members) <= 4
         # the FFMA launch stages G_0..G_k-1, the padded row window and, unless
         # the columns are a run of the rows inside it, the padded column window;
         # two slab buffers per warp must fit (<= 48 staged rows)
@@ -576,7 +582,10 @@ def contract_multi(Gs, sf, rows_list, cols):
         ag += [g] * len(rows)
     cidx = [sf.slot[k] for k in cols]
     T = torch.empty((len(ridx), len(cidx)), dtype=torch.float64, device=_device())
-    ctx.gram_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
+    if GRAM_TC:
+        ctx.gram_tc_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
+    else:
+        ctx.gram_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
     out, r0 = [], 0
     for rows in rows_list:
         out.append(T[r0:r0 + len(rows)])

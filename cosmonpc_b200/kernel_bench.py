@@ -1,7 +1,7 @@
 """Time one library entry point on synthetic device-resident inputs.
 
     python -m cosmonpc_b200.kernel_bench shells --n 256 --items 8 [--reps 5]
-    python -m cosmonpc_b200.kernel_bench gram --n 256 --rows 40 --cols 20
+    python -m cosmonpc_b200.kernel_bench gram --n 256 --rows 40 --cols 20 [--tc]
     python -m cosmonpc_b200.kernel_bench paint --n 256 --particles 4000000 --window 4
 
 Each prints one line: the call, its mean device time (CUDA events over
@@ -52,8 +52,9 @@ def shells(n, items, reps, boxsize=None):
     return {"call": "shell_fields", "n": n, "items": items, "ms": ms, "bytes": items * n ** 3 * 4 + band // 2}
 
 
-def gram(n, rows, cols, reps):
-    """cnpc_contract_gram (FP32): rows x cols outputs, the columns a run of the rows."""
+def gram(n, rows, cols, reps, tc=False):
+    """cnpc_contract_gram (FP32, CUDA cores) or cnpc_contract_gram_tc (tensor
+    cores): rows x cols outputs, the columns a run of the rows."""
     ctx = _lib.Context.get()
     ncell = n ** 3
     g = torch.Generator(device="cuda").manual_seed(1)
@@ -61,8 +62,11 @@ def gram(n, rows, cols, reps):
     w = torch.randn(ncell, device="cuda", generator=g)
     out = torch.empty((rows, cols), dtype=torch.float64, device="cuda")
     a, b = list(range(rows)), list(range(cols))
-    ms = _time(lambda: ctx.gram(_lib.F32, ncell, w, f, ncell, a, b, out), reps)
-    return {"call": "contract_gram", "n": n, "rows": rows, "cols": cols, "ms": ms,
+    if tc:
+        ms = _time(lambda: ctx.gram_tc(ncell, w, f, ncell, a, b, out), reps)
+    else:
+        ms = _time(lambda: ctx.gram(_lib.F32, ncell, w, f, ncell, a, b, out), reps)
+    return {"call": "contract_gram_tc" if tc else "contract_gram", "n": n, "rows": rows, "cols": cols, "ms": ms,
             "bytes": (max(rows, cols) + 1) * ncell * 4}
 
 
@@ -89,12 +93,13 @@ def main(argv=None):
     ap.add_argument("--particles", type=int, default=4_000_000)
     ap.add_argument("--window", type=int, default=4)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--tc", action="store_true", help="gram: the tensor-core kernel")
     args = ap.parse_args(argv)
     build.build()
     if args.what == "shells":
         r = shells(args.n, args.items, args.reps)
     elif args.what == "gram":
-        r = gram(args.n, args.rows, args.cols, args.reps)
+        r = gram(args.n, args.rows, args.cols, args.reps, args.tc)
     else:
         r = paint(args.n, args.particles, args.window, args.reps)
     r["GB_per_s"] = r["bytes"] / (r["ms"] * 1e6)

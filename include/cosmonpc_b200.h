@@ -404,15 +404,30 @@ int cnpc_contract_pairs(cnpc_ctx *ctx, int dtype, int64_t ncell, const void *d_g
                         const void *d_fields, int64_t field_stride, const int *h_a,
                         const int *h_b, int npairs, double *d_out, cnpc_stream_t stream);
 
-/* FP32 Gram contraction on the tensor cores (tcgen05.mma kind::tf32, each FP32
- * operand split into a TF32 hi/lo pair, hi*hi + hi*lo + lo*hi in FP32 TMEM
- * accumulators folded into FP64 every 256 cells): d_out[i*nb + j] = sum_x G F_{h_a[i]}
- * F_{h_b[j]} for na <= 64 rows and nb <= 32 columns.  ncell and field_stride are
- * multiples of 4; G and fields 16-byte aligned.  Same sums as cnpc_contract_gram
- * (clustering_estimator.py:911-981, :1983-2035), product error ~2^-22 relative. */
+/* FP32 Gram contraction on the tensor cores: d_out[i*nb + j] =
+ * sum_x G F_{h_a[i]} F_{h_b[j]} for na <= 40 rows and nb <= 24 columns, the
+ * same sums as cnpc_contract_gram (clustering_estimator.py:911-981,
+ * :1983-2035).  tcgen05.mma kind::tf32 with each FP32 operand split into a
+ * TF32 hi/lo pair (all four products in one M = 128, N = 48 MMA per 8 cells;
+ * the A operand G F_a in tensor memory, written from registers, the B
+ * operand F_b in 128-byte-swizzled shared memory), FP32 accumulators folded
+ * into FP64 every 512 cells; product error ~2^-22 relative.  ncell and
+ * field_stride are multiples of 4; G and fields 16-byte aligned.  Its
+ * bounded waits report through the context's status word
+ * (cnpc_ctx_take_status). */
 int cnpc_contract_gram_tc(cnpc_ctx *ctx, int64_t ncell, const float *d_g, const float *d_fields,
                           int64_t field_stride, const int *h_a, int na, const int *h_b, int nb,
                           double *d_out, cnpc_stream_t stream);
+
+/* cnpc_contract_gram_tc with a weight field per row, in one launch:
+ * d_out[i*nb + j] = sum_x G_{h_ag[i]} F_{h_a[i]} F_{h_b[j]}, ngs <= 4 weight
+ * fields h_gs[0..ngs-1] (device pointers, 16-byte aligned).  The FFT S3 sums
+ * of several angular configurations contract their own source fields with
+ * the same unit-spectrum shells (clustering_estimator.py:1182-1384). */
+int cnpc_contract_gram_tc_multi_g(cnpc_ctx *ctx, int64_t ncell, const float *const *h_gs, int ngs,
+                                  const float *d_fields, int64_t field_stride, const int *h_a,
+                                  const int *h_ag, int na, const int *h_b, int nb, double *d_out,
+                                  cnpc_stream_t stream);
 
 /* Allocation-free form of cnpc_contract_gram.  It has no counterpart in the
  * reference; it exists for callers that must not have a library allocate

@@ -189,12 +189,15 @@ def test_pair_contraction_matches_fp64_sums(dtype, n):
 
 
 @pytest.mark.parametrize("ncell,na,nb,shared", [(4096 + 36, 1, 1, False), (32 ** 3, 8, 8, True),
-                                                (64 ** 3, 40, 20, True), (64 ** 3, 64, 32, False),
-                                                (48 ** 3, 24, 20, False), (64 ** 3 + 100, 17, 9, False)])
+                                                (64 ** 3, 40, 20, True), (64 ** 3, 40, 24, False),
+                                                (48 ** 3, 24, 20, False), (64 ** 3 + 100, 17, 9, False),
+                                                (128 ** 3, 40, 20, True), (100, 3, 2, False)])
 def test_tensor_core_gram_matches_fp64(ncell, na, nb, shared):
-    """cnpc_contract_gram_tc (3xTF32 on tcgen05) against FP64 sums of the same
-    FP32 inputs and against the CUDA-core FFMA Gram, with ragged last chunks,
-    padded rows/columns, shared row/column fields and a padded field stride."""
+    """cnpc_contract_gram_tc (TF32 pairs on tcgen05, A operand in tensor
+    memory) against FP64 sums of the same FP32 inputs and against the CUDA-core
+    FFMA Gram, with ragged last chunks (and a call smaller than one chunk),
+    rows and columns short of the 40 x 24 window, shared row/column fields, a
+    padded field stride, and at 128^3 many accumulator periods per block."""
     import torch
     from cosmonpc_b200 import _lib
 
@@ -333,6 +336,38 @@ def test_sn_bins_multi_matches_single_calls(dtype, cross):
     assert torch.equal(torch.view_as_real(sr), torch.view_as_real(src_m[0]))
     scale = sums_m[1][0::2].abs().max().item()
     assert (s_ns[0::2] - sums_m[1][0::2][:nb]).abs().max().item() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("ngs,rows,nb,shared", [(2, (20, 20), 20, True), (3, (5, 9, 11), 8, False),
+                                                (1, (17,), 7, False), (4, (10, 10, 10, 10), 20, True)])
+def test_tensor_core_multi_weight_gram(ngs, rows, nb, shared):
+    """cnpc_contract_gram_tc_multi_g (a weight field per row, tensor cores)
+    against FP64 sums and against the CUDA-core multi-weight Gram."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    n = 64
+    ncell = n ** 3
+    rng = np.random.default_rng(ngs * 1000 + nb)
+    na = sum(rows)
+    nf = na + (0 if shared else nb)
+    stride = ncell + 4
+    f = torch.from_numpy(rng.standard_normal((nf, stride)).astype(np.float32)).cuda()
+    gs = [torch.from_numpy(rng.standard_normal(ncell).astype(np.float32)).cuda() for _ in range(ngs)]
+    a = list(rng.permutation(na))
+    ag = [g for g, r in enumerate(rows) for _ in range(r)]
+    b = a[:nb] if shared else list(range(na, na + nb))
+    ctx = _lib.Context.get()
+    out = torch.empty((na, nb), dtype=torch.float64, device="cuda")
+    ctx.gram_tc_multi_g(ncell, gs, f, stride, a, ag, b, out)
+    ff = torch.empty_like(out)
+    ctx.gram_multi_g(ncell, gs, f, stride, a, ag, b, ff)
+    fd = f[:, :ncell].double()
+    gw = torch.stack([gs[g].double() for g in ag])
+    ref = (gw * fd[a]) @ fd[b].T
+    scale = (gw.abs() * fd[a].abs()) @ fd[b].abs().T
+    assert ((out - ref).abs() / scale).max().item() < 2e-6
+    assert ((out - ff).abs() / scale).max().item() < 2e-6
 
 
 @pytest.mark.parametrize("ngs,rows,nb,shared", [(2, (20, 20), 20, True), (3, (5, 9, 11), 8, False),
