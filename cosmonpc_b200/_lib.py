@@ -31,7 +31,7 @@ EXPORTED = (
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
     "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
     "cnpc_forward_finish_band", "cnpc_ctx_set_wait_limit", "cnpc_ctx_take_status",
-    "cnpc_contract_gram_tc_multi_g",
+    "cnpc_contract_gram_tc_multi_g", "cnpc_box_catalog",
 )
 
 # survey catalog columns (cnpc_colid) and column types (cnpc_coltype)
@@ -39,6 +39,7 @@ COL_RA, COL_DEC, COL_Z, COL_WEIGHT, COL_SYSTOT, COL_NOZ, COL_CP, COL_FKP, COL_NZ
 CT_ABSENT, CT_F64, CT_F32, CT_I16, CT_I32, CT_I64, CT_U8, CT_BOOL = range(8)
 CT_OF_FITS = {"D": CT_F64, "E": CT_F32, "I": CT_I16, "J": CT_I32, "K": CT_I64, "B": CT_U8, "L": CT_BOOL}
 W_COLUMN, W_ONE, W_BOSS, W_EBOSS = range(4)
+COSMO_FLAT_LCDM, COSMO_PLANCK18 = range(2)
 PSUM_COUNT = 5
 
 
@@ -70,7 +71,17 @@ class CatalogSpec(ctypes.Structure):
 
     _fields_ = [("row_bytes", ctypes.c_int64), ("col", Column * 9), ("weight_rule", ctypes.c_int),
                 ("has_zrange", ctypes.c_int), ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
-                ("h", ctypes.c_double), ("omega_m", ctypes.c_double)]
+                ("h", ctypes.c_double), ("omega_m", ctypes.c_double), ("cosmology", ctypes.c_int)]
+
+
+class ColRef(ctypes.Structure):
+    """Mirror of ``cnpc_colref``."""
+
+    _fields_ = [("d_base", ctypes.c_void_p), ("stride", ctypes.c_int64), ("type", ctypes.c_int),
+                ("big_endian", ctypes.c_int), ("scale", ctypes.c_double), ("zero", ctypes.c_double)]
+
+
+BOX_X, BOX_Y, BOX_Z, BOX_VX, BOX_VY, BOX_VZ, BOX_W, BOX_NCOLS = range(8)
 
 
 class Operand(ctypes.Structure):
@@ -132,6 +143,7 @@ _SIGS = {
                                    _vp],
     "cnpc_contract_gram_tc_multi_g": [_vp, _i64, ctypes.POINTER(_vp), _i, _vp, _i64, _ip, _ip, _i, _ip, _i, _vp,
                                       _vp],
+    "cnpc_box_catalog": [_vp, _i64, ctypes.POINTER(ColRef), _i, _dp, _d, _vp, _vp, _vp],
     "cnpc_ctx_set_wait_limit": [_vp, _i64],
     "cnpc_ctx_take_status": [_vp, _vp, _ip],
 }
@@ -177,7 +189,8 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "catalog_weights": 1, "interlace_split": 1, "xspace_harmonic": 1, "survey_bins": 1,
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
                     "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
-                    "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1, "forward_finish_band": 1}
+                    "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1, "forward_finish_band": 1,
+                    "box_catalog": 1}
 launch_count = 0
 
 
@@ -314,6 +327,15 @@ class Context:
         if st == CNPC_ENOMEM:
             raise MemoryError("%s: %s" % (what, msg))
         raise CnpcError("%s: %s" % (what, msg))
+
+    def box_catalog(self, nrows, cols, apply_rsd, shift, box_length, pos, weight):
+        """cnpc_box_catalog: ``cols`` is a list of BOX_NCOLS ColRef."""
+        arr = (ColRef * BOX_NCOLS)(*cols)
+        sh, shp = _darr(shift if shift is not None else (0.0, 0.0, 0.0))
+        st = self.lib.cnpc_box_catalog(self.h, int(nrows), arr, 1 if apply_rsd else 0, shp, float(box_length),
+                                       _ptr(pos), _ptr(weight), self.stream())
+        self._check(st, "cnpc_box_catalog")
+        _count("box_catalog")
 
     def set_wait_limit(self, polls):
         """Polls a bounded device wait makes before it gives up (0: at once)."""

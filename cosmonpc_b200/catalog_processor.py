@@ -5,8 +5,16 @@ named by ``column_names``; ``x, y, z`` give the position and ``w`` (optional)
 the weight (src/cosmonpc/catalog_processor.py:91-125, :354-386).  One process
 reads the whole file (the reference splits rows over MPI ranks and reduces
 the counts; the totals are identical).
+
+Box ``.fits`` catalogs (src/cosmonpc/catalog_processor.py:388-445): the
+requested columns that exist; positions from X, Y, Z or else x, y, z;
+velocities from VX, VY, VZ or else vx, vy, vz when ``apply_rsd``; weight ``w``.
+The raw rows go to the device unchanged and ``cnpc_box_catalog`` decodes them
+and applies the redshift-space shift of add_rsd (catalog_processor.py:648-693).
 """
 from __future__ import annotations
+
+import math
 
 import numpy as np
 
@@ -19,13 +27,112 @@ def _ext(path):
     return path.split(".")[-1].lower() if path else None
 
 
+def flat_lcdm_efunc(omega_m, z):
+    """E(z) of a flat LCDM cosmology without radiation, evaluated in the order
+    astropy's FlatLambdaCDM(H0, Om0) uses (Tcmb0 = 0, so no photons or
+    neutrinos): sqrt(zp1^2 ((0 zp1 + Om0) zp1 + 0) + Ode0), Ode0 = 1 - Om0."""
+    zp1 = float(z) + 1.0
+    ode0 = 1.0 - float(omega_m)
+    return math.sqrt(zp1 ** 2 * ((0.0 * zp1 + float(omega_m)) * zp1 + 0.0) + ode0)
+
+
+def rsd_shift(cosmology, redshift_box, los):
+    """rsd_factor * los of add_rsd (catalog_processor.py:648-693, box branch):
+    rsd_factor = (1 + z) / (100 E(z)) in (Mpc/h)/(km/s); the reference rejects
+    a line of sight whose norm is not exactly 1."""
+    e = flat_lcdm_efunc(cosmology["Omega0"], redshift_box)
+    factor = (1 + redshift_box) / (e * 100)
+    los = np.array(los)
+    if np.linalg.norm(los) != 1:
+        raise ValueError("LOS must be a 3d unit vector")
+    return factor * los
+
+
+def _pick(names, groups):
+    for axes in groups:
+        if all(a in names for a in axes):
+            return axes
+    return None
+
+
+def read_box_fits(paths, column_names, apply_rsd=False, cosmology=None, redshift_box=None, los=None,
+                  boxsize=None):
+    """Box FITS catalog(s) decoded on the device: (positions (N, 3), weights (N,))
+    as float64 CUDA tensors (files of a list concatenated in order)."""
+    import torch
+
+    from . import _lib
+    from .fits import open_table
+
+    paths = [paths] if isinstance(paths, str) else list(paths)
+    tables = [open_table(p) for p in paths]
+    names = [c for c in column_names if c in tables[0].colnames()] if tables else []
+    pos_axes = _pick(names, [("X", "Y", "Z"), ("x", "y", "z")])
+    vel_axes = _pick(names, [("VX", "VY", "VZ"), ("vx", "vy", "vz")]) if apply_rsd else None
+    shift = None
+    if apply_rsd:
+        if vel_axes is None:
+            # the reference reaches add_rsd with its velocity variable unset
+            raise UnboundLocalError("cannot access local variable 'velocities' where it is not associated "
+                                    "with a value")
+        shift = rsd_shift(cosmology, redshift_box, los)
+    box_length = float(np.asarray(boxsize, dtype=np.float64).reshape(-1)[0]) if boxsize is not None else 0.0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = _lib.Context.get()
+    outs_p, outs_w = [], []
+    for t in tables:
+        raw = t.rows()
+        host = torch.empty(raw.size, dtype=torch.uint8, pin_memory=True)
+        if raw.size:
+            np.copyto(host.numpy().reshape(raw.shape), raw)
+        rows = host.to(dev, non_blocking=True)
+        base = rows.data_ptr()
+
+        def ref(name):
+            if name is None:
+                return _lib.ColRef(None, 0, _lib.CT_ABSENT, 0, 1.0, 0.0)
+            c = t.scalar_column(name)
+            if c.code not in _lib.CT_OF_FITS:
+                raise ValueError(f"column {name}: unsupported FITS type {c.code}")
+            return _lib.ColRef(base + c.offset, t.row_bytes, _lib.CT_OF_FITS[c.code], 1, c.scale, c.zero)
+
+        cols = [ref(pos_axes[d] if pos_axes else None) for d in range(3)]
+        cols += [ref(vel_axes[d] if vel_axes else None) for d in range(3)]
+        cols.append(ref("w" if "w" in names else None))
+        pos = torch.empty((max(t.nrows, 1), 3), dtype=torch.float64, device=dev)[:t.nrows]
+        w = torch.empty(max(t.nrows, 1), dtype=torch.float64, device=dev)[:t.nrows]
+        ctx.box_catalog(t.nrows, cols, apply_rsd, shift, box_length, pos, w)
+        rows.record_stream(torch.cuda.current_stream(dev))
+        outs_p.append(pos)
+        outs_w.append(w)
+    if len(outs_p) == 1:
+        return outs_p[0], outs_w[0]
+    return torch.cat(outs_p), torch.cat(outs_w)
+
+
+def read_box(path, column_names, apply_rsd=False, cosmology=None, redshift_box=None, los=None, boxsize=None):
+    """Box branch of catalog_reader (catalog_processor.py:354-445): ``.npy``
+    catalogs as host arrays (the reference applies no RSD to them), ``.fits``
+    catalogs decoded and shifted on the device."""
+    ext = _ext(path)
+    if ext not in SUPPORTED:
+        raise ValueError(f"Unsupported data file type: {ext}")
+    if ext == "npy":
+        return read_box_npy(path, column_names)
+    if ext == "fits":
+        return read_box_fits(path, column_names, apply_rsd, cosmology, redshift_box, los, boxsize)
+    from .hdf5 import read_box_hdf5
+
+    return read_box_hdf5(path, column_names, apply_rsd, cosmology, redshift_box, los, boxsize)
+
+
 def read_box_npy(path, column_names):
     """Return (positions (N,3) float64, weights (N,) float64) of a box catalog."""
     ext = _ext(path)
     if ext not in SUPPORTED:
         raise ValueError(f"Unsupported data file type: {ext}")
     if ext != "npy":
-        raise NotImplementedError("box catalogs other than .npy are not supported by this build")
+        raise ValueError("read_box_npy reads .npy catalogs")
     assert column_names is not None and len(column_names) >= 3, (
         "For box-like geometry with .npy file, column_names must be provided "
         "with at least 3 elements for x,y,z.")

@@ -50,9 +50,43 @@ struct CatalogParams {
     double z_min, z_max;
     double omega_m;
     double h;
-    double hubble_distance;  // c / H0 in Mpc, H0 = 100 h
+    double hubble_distance;  // c / H0 in Mpc
+    int planck18;            // E(z) with photons and a massive neutrino (Planck18Radiation)
+    double ogamma0, ode0, nu_prefac, nu_y, nu_massless;
     Gauss16 gl;
 };
+
+// astropy's Planck18 realisation (H0 = 67.66 km/s/Mpc, Om0 = 0.30966,
+// Tcmb0 = 2.7255 K, Neff = 3.046, m_nu = (0, 0, 0.06) eV, flat), restated
+// from astropy's published FLRW formulas with CODATA 2018 constants:
+//   Ogamma0 = (4 sigma_SB / c^3) Tcmb0^4 / rho_crit0, rho_crit0 = 3 H0^2 / (8 pi G);
+//   the neutrino density relative to photons, for neutrinos of y = m c^2 / (k_B T_nu0)
+//   with T_nu0 = (4/11)^(1/3) Tcmb0 (Komatsu et al. 2011, eq. 26 fit),
+//   n(z) = (7/8)(4/11)^(4/3) (Neff / 3) [sum (1 + (0.3173 y / (1+z))^1.83)^(1/1.83) + N_massless];
+//   E(z)^2 = (1+z)^2 ((Or (1+z) + Om0) (1+z)) + Ode0, Or = Ogamma0 (1 + n(z)),
+//   Ode0 = 1 - Om0 - Ogamma0 - Ogamma0 n(0).
+struct Planck18Radiation {
+    double ogamma0, ode0, nu_prefac, nu_y, nu_massless, hubble_distance;
+};
+static Planck18Radiation planck18_radiation() {
+    const double pi = 3.14159265358979323846;
+    const double sigma_sb = 5.670374419e-8, c = 299792458.0, G = 6.67430e-11;
+    const double kB_eV = 1.380649e-23 / 1.602176634e-19;
+    const double mpc = 3.0856775814913673e22;
+    const double H0 = 67.66, Tcmb0 = 2.7255, Neff = 3.046, m_nu = 0.06;
+    const double h0_si = H0 * 1000.0 / mpc;
+    const double rho_crit = 3.0 * h0_si * h0_si / (8.0 * pi * G);
+    Planck18Radiation r;
+    r.ogamma0 = (4.0 * sigma_sb / (c * c * c)) * Tcmb0 * Tcmb0 * Tcmb0 * Tcmb0 / rho_crit;
+    const double tnu0 = 0.7137658555036082 * Tcmb0;
+    r.nu_y = m_nu / (kB_eV * tnu0);
+    r.nu_prefac = 0.22710731766 * (Neff / 3.0);
+    r.nu_massless = 2.0;
+    const double n0 = r.nu_prefac * (std::pow(1.0 + std::pow(0.3173 * r.nu_y, 1.83), 0.54644808743) + r.nu_massless);
+    r.ode0 = 1.0 - 0.30966 - r.ogamma0 - r.ogamma0 * n0;
+    r.hubble_distance = c / 1000.0 / H0;
+    return r;
+}
 
 __device__ inline double read_column(const uint8_t *row, const cnpc_column &c) {
     const uint8_t *p = row + c.offset;
@@ -100,7 +134,16 @@ __device__ inline double los_integral(double z, const CatalogParams &p) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const double a = 1.0 + (mid + hw * p.gl.x[j]);
-            s += p.gl.w[j] / sqrt(p.omega_m * (a * a * a) + ol);
+            double e2;
+            if (p.planck18) {
+                const double nrel = p.nu_prefac * (pow(1.0 + pow(0.3173 * p.nu_y / a, 1.83), 0.54644808743) +
+                                                   p.nu_massless);
+                const double o_r = p.ogamma0 * (1.0 + nrel);
+                e2 = a * a * ((o_r * a + p.omega_m) * a) + p.ode0;
+            } else {
+                e2 = p.omega_m * (a * a * a) + ol;
+            }
+            s += p.gl.w[j] / sqrt(e2);
         }
         sum += s * hw;
     }
@@ -681,7 +724,10 @@ int cnpc_catalog_decode(cnpc_ctx *ctx, const void *d_rows, int64_t nrows, const 
     if (sp.weight_rule == CNPC_W_BOSS || sp.weight_rule == CNPC_W_EBOSS)
         CNPC_REQUIRE(ctx, sp.col[CNPC_COL_SYSTOT].type && sp.col[CNPC_COL_NOZ].type && sp.col[CNPC_COL_CP].type,
                      "completeness columns missing");
-    CNPC_REQUIRE(ctx, sp.h > 0.0 && sp.omega_m > 0.0 && sp.omega_m < 1.0, "cosmology out of range");
+    CNPC_REQUIRE(ctx, sp.cosmology == CNPC_COSMO_FLAT_LCDM || sp.cosmology == CNPC_COSMO_PLANCK18,
+                 "bad cosmology model");
+    CNPC_REQUIRE(ctx, sp.h > 0.0 && (sp.cosmology == CNPC_COSMO_PLANCK18 || (sp.omega_m > 0.0 && sp.omega_m < 1.0)),
+                 "cosmology out of range");
     *h_kept = 0;
     if (nrows == 0) return CNPC_OK;
     for (int c = 0; c < CNPC_NCOLS; ++c) {
@@ -702,6 +748,18 @@ int cnpc_catalog_decode(cnpc_ctx *ctx, const void *d_rows, int64_t nrows, const 
     p.omega_m = sp.omega_m;
     p.h = sp.h;
     p.hubble_distance = 299792.458 / (100.0 * sp.h);
+    p.planck18 = sp.cosmology == CNPC_COSMO_PLANCK18;
+    p.ogamma0 = p.ode0 = p.nu_prefac = p.nu_y = p.nu_massless = 0.0;
+    if (p.planck18) {
+        const Planck18Radiation r = planck18_radiation();
+        p.omega_m = 0.30966;
+        p.ogamma0 = r.ogamma0;
+        p.ode0 = r.ode0;
+        p.nu_prefac = r.nu_prefac;
+        p.nu_y = r.nu_y;
+        p.nu_massless = r.nu_massless;
+        p.hubble_distance = r.hubble_distance;
+    }
     p.gl = gauss_legendre16();
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t nblk64 = (nrows + kRowsPerBlock - 1) / kRowsPerBlock;

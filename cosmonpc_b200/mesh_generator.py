@@ -1,9 +1,10 @@
 """Mesh builders: catalogs -> painted device meshes.
 
 ``get_mesh_box`` mirrors src/cosmonpc/mesh_generator.py:15-169: it reads up to
-three tracers, computes N_gal, sum(w) and NZ = sum(w)/V in FP64 on the host
-(one process holds the whole catalog), copies positions and weights to the GPU
-and paints them (interlaced pair in one pass) into device meshes.
+three tracers (``.npy`` on the host; ``.fits`` decoded, and shifted into
+redshift space when ``apply_rsd``, on the device), computes N_gal, sum(w) and
+NZ = sum(w)/V in FP64, and paints them (interlaced pair in one pass) into
+device meshes.
 """
 from __future__ import annotations
 
@@ -11,7 +12,7 @@ import numpy as np
 import torch
 
 from . import engine
-from .catalog_processor import read_box_npy
+from .catalog_processor import read_box
 
 
 def catalog_to_device(pos, w, pin=True):
@@ -28,10 +29,14 @@ def catalog_to_device(pos, w, pin=True):
 
 
 def paint_catalog(pos, w, nmesh, boxsize, sampler, interlaced, precision="f64"):
-    """Paint a host catalog; returns (PaintedMesh, N_gal, weight_sum)."""
+    """Paint a host or device catalog; returns (PaintedMesh, N_gal, weight_sum)."""
     n_gal = int(pos.shape[0])
-    weight_sum = float(np.sum(w))
-    dp, dw = catalog_to_device(pos, w)
+    if isinstance(pos, torch.Tensor):
+        weight_sum = float(w.sum().item())
+        dp, dw = pos, w
+    else:
+        weight_sum = float(np.sum(w))
+        dp, dw = catalog_to_device(pos, w)
     pm = engine.paint(dp, dw, int(nmesh[0]), float(boxsize[0]), sampler, interlaced, precision,
                       sum_w=weight_sum)
     return pm, n_gal, weight_sum
@@ -51,7 +56,8 @@ def get_mesh_box(catalogs, correlation_mode, nmesh, geometry, boxsize, sampler, 
     meshes = {}
     attrs = {}
     for t in letters:
-        pos, w = read_box_npy(catalogs["data_" + t], column_names)
+        pos, w = read_box(catalogs["data_" + t], column_names, apply_rsd, para_cosmo, redshift_box, los,
+                          boxsize)
         pm, n_gal, wsum = paint_catalog(pos, w, Nmesh, box, sampler, interlaced, precision)
         meshes[t] = pm
         attrs["N_gal_" + t] = n_gal

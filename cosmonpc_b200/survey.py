@@ -153,7 +153,12 @@ def _decode_file(path, column_names, z_range, comp_weight_plan, catalog_type, co
     if z_range is not None:
         spec.z_min, spec.z_max = float(z_range[0]), float(z_range[1])
     spec.h = float(cosmology["h"])
-    spec.omega_m = float(cosmology["Omega0"])
+    if "Omega0" in cosmology:
+        spec.omega_m = float(cosmology["Omega0"])
+        spec.cosmology = _lib.COSMO_FLAT_LCDM
+    else:  # catalog_processor.py:610-625: Planck18, distances still times the config's h
+        spec.omega_m = 0.0
+        spec.cosmology = _lib.COSMO_PLANCK18
     dev = _device()
     nr = t.nrows
     # file rows -> one pinned buffer (a single host copy, split over threads:
@@ -186,13 +191,17 @@ def read_catalog(catalog, column_names, z_range, comp_weight_plan, catalog_type,
         raise NotImplementedError("survey-like catalogs are read from .fits files")
     assert "Z" in column_names, \
         "For survey-like geometry with .fits file, column_names must include 'Z' for redshift slice."
-    if cosmology is None or "h" not in cosmology or "Omega0" not in cosmology:
-        raise NotImplementedError("survey catalogs need cosmology with 'h' and 'Omega0' "
-                                  "(the Planck18 fallback with radiation is not implemented)")
+    # the reference falls back to Planck18 when h or Omega0 is missing
+    # (catalog_processor.py:610-625) and then multiplies by cosmology["h"]:
+    # without a config dict, or without h, it fails there
+    if cosmology is None:
+        raise TypeError("'NoneType' object is not subscriptable")
+    if "h" not in cosmology:
+        raise KeyError("h")
     paths = [catalog] if isinstance(catalog, str) else list(catalog)
     key = (tuple(paths), tuple(column_names), None if z_range is None else tuple(z_range),
            comp_weight_plan["scheme"], comp_weight_plan["name_alias"], catalog_type,
-           float(cosmology["h"]), float(cosmology["Omega0"]), normalization_scheme == "particle",
+           float(cosmology["h"]), float(cosmology.get("Omega0", -1.0)), normalization_scheme == "particle",
            torch.cuda.current_device())
     hit = _cache.get(key)
     if hit is not None:

@@ -254,7 +254,43 @@ typedef struct cnpc_catalog_spec {
     int has_zrange;              /* keep rows with z_min < Z < z_max (cp:506-508) */
     double z_min, z_max;
     double h, omega_m;           /* flat LCDM, no radiation (cp:617-632)          */
+    int cosmology;               /* CNPC_COSMO_FLAT_LCDM: (h, omega_m);
+                                    CNPC_COSMO_PLANCK18: the fallback of cp:610-625
+                                    when the config gives h but no Omega0:
+                                    astropy's Planck18 (H0 67.66, Om0 0.30966,
+                                    Tcmb0 2.7255 K, Neff 3.046, one 0.06 eV
+                                    neutrino), distances times the config's h;
+                                    omega_m is ignored */
 } cnpc_catalog_spec;
+enum cnpc_cosmology { CNPC_COSMO_FLAT_LCDM = 0, CNPC_COSMO_PLANCK18 = 1 };
+
+/* ------------------------------------------------------------ box catalogs
+ * Box catalogs in FITS or HDF5 files (catalog_processor.py:388-445).  A
+ * column is a strided run of scalars in device memory: the raw rows of a FITS
+ * binary table (big_endian = 1, stride = the row size, d_base = rows + column
+ * offset) or one contiguous HDF5 dataset (stride = the element size). */
+typedef struct cnpc_colref {
+    const void *d_base; /* value of row 0; unused when type is CNPC_CT_ABSENT */
+    int64_t stride;     /* bytes between consecutive rows                      */
+    int type;           /* cnpc_coltype                                        */
+    int big_endian;
+    double scale;       /* value = zero + scale * raw                          */
+    double zero;
+} cnpc_colref;
+enum cnpc_box_colid {
+    CNPC_BOX_X = 0, CNPC_BOX_Y, CNPC_BOX_Z, CNPC_BOX_VX, CNPC_BOX_VY, CNPC_BOX_VZ, CNPC_BOX_W, CNPC_BOX_NCOLS
+};
+
+/* Decode a box catalog: d_pos (nrows, 3) from the X/Y/Z columns (absent:
+ * 0, as the reference leaves Position zero when no position columns match),
+ * d_weight from the W column (absent: 1).  With apply_rsd, the shift of
+ * add_rsd (catalog_processor.py:648-693, box branch) is applied on the device:
+ * x_d = (x_d + h_shift[d] * v_d) mod box_length with h_shift[d] =
+ * rsd_factor * los_d (the reference multiplies los and the velocity
+ * elementwise) and numpy's float remainder; the velocity columns must exist. */
+int cnpc_box_catalog(cnpc_ctx *ctx, int64_t nrows, const cnpc_colref *h_cols, int apply_rsd,
+                     const double *h_shift, double box_length, double *d_pos, double *d_weight,
+                     cnpc_stream_t stream);
 
 /* Decode, z-cut and convert a survey catalog: catalog_reader's survey branch
  * (catalog_processor.py:493-586) with ra_dec_z_to_xyz (cp:589-645).

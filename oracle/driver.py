@@ -12,8 +12,41 @@ import numpy as np
 from . import box
 
 
-def read_box_catalog(path, column_names):
-    """``catalog_reader`` box ``.npy`` branch (catalog_processor.py:354-386)."""
+def _efunc_flat(om0, z):
+    """E(z) of astropy's FlatLambdaCDM(H0, Om0) (Tcmb0 = 0), its evaluation order."""
+    zp1 = float(z) + 1.0
+    return np.sqrt(zp1 ** 2 * ((0.0 * zp1 + om0) * zp1 + 0.0) + (1.0 - om0))
+
+
+def read_box_catalog(path, column_names, apply_rsd=False, cosmology=None, redshift_box=None, los=None,
+                     boxsize=None):
+    """``catalog_reader`` box branches: ``.npy`` (catalog_processor.py:354-386),
+    and ``.fits`` (:388-445) with ``add_rsd`` (:648-693) when ``apply_rsd``."""
+    if str(path).lower().endswith(".fits"):
+        from cosmonpc_b200.fits import open_table
+
+        t = open_table(path)
+        names = [c for c in column_names if c in t.colnames()]
+        data = t.read_columns(names)
+        pos = np.zeros((t.nrows, 3))
+        for axes in (("X", "Y", "Z"), ("x", "y", "z")):
+            if all(a in names for a in axes):
+                pos = np.column_stack([data[a] for a in axes]).astype(np.float64)
+                break
+        if apply_rsd:
+            vel = None
+            for axes in (("VX", "VY", "VZ"), ("vx", "vy", "vz")):
+                if all(a in names for a in axes):
+                    vel = np.column_stack([data[a] for a in axes]).astype(np.float64)
+                    break
+            factor = (1 + redshift_box) / (_efunc_flat(cosmology["Omega0"], redshift_box) * 100)
+            los_v = np.array(los)
+            if np.linalg.norm(los_v) != 1:
+                raise ValueError("LOS must be a 3d unit vector")
+            pos += factor * los_v * vel
+            pos = pos % np.asarray(boxsize, dtype=np.float64)[0]
+        w = np.asarray(data["w"], dtype=np.float64) if "w" in names else np.ones(t.nrows)
+        return pos, w
     arr = np.load(path, mmap_mode="r")
     idx = [column_names.index(a) for a in ("x", "y", "z")]
     pos = np.column_stack([arr[:, i] for i in idx]).astype(np.float64)
@@ -39,7 +72,9 @@ def run_box(config):
         letters.append("c")
     fields, N_gal, NZ = {}, {}, {}
     for t in letters:
-        pos, w = read_box_catalog(cats["data_" + t], cfg["column_names"])
+        pos, w = read_box_catalog(cats["data_" + t], cfg["column_names"], cfg.get("apply_rsd", False),
+                                  cfg.get("cosmology"), cfg.get("redshift_box"), cfg.get("rsd"),
+                                  cfg["boxsize"])
         N_gal[t] = w.shape[0]
         NZ[t] = np.sum(w) / V
         fields[t] = box.paint_field(pos, w, n, L, cfg["sampler"], cfg["interlaced"])

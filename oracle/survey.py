@@ -84,7 +84,12 @@ def read_catalog(paths, column_names, z_range, comp_weight_plan, catalog_type, c
     # ra_dec_z_to_xyz (cp:589-645)
     ra = np.deg2rad(arr["RA"])
     dec = np.deg2rad(arr["DEC"])
-    d = comoving_distance(arr["Z"], cosmology["h"], cosmology["Omega0"])
+    if "Omega0" in cosmology:
+        d = comoving_distance(arr["Z"], cosmology["h"], cosmology["Omega0"])
+    else:  # cp:610-625: Planck18, then times the config's h
+        from .cosmology import comoving_distance_mpc
+
+        d = comoving_distance_mpc(arr["Z"]) * cosmology["h"]
     pos = np.column_stack([d * np.cos(dec) * np.cos(ra), d * np.cos(dec) * np.sin(ra), d * np.sin(dec)])
     if "WEIGHT_FKP" not in names:
         raise ValueError("WEIGHT_FKP column is missing in the catalog.")

@@ -92,6 +92,24 @@ CASES = [
                                k_min=0.005, k_max=0.045, k_bins=3, angu_config=[2, 0, 2],
                                data_vector_mode="full", shotnoise_mode="ana"),
      {"a": (26, 15000, False), "b": (27, 12000, True), "c": (28, 10000, False)}),
+    # box catalogs in FITS files with velocity columns: the reference applies its
+    # redshift-space shift (catalog_processor.py:410-433, :648-693); "_format"
+    # names the file layout (lower- or upper-case column names, weights)
+    ("bk_fits_rsd_tsc", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                             nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="tsc", interlaced=True,
+                             k_min=0.005, k_max=0.045, k_bins=4, angu_config=[2, 0, 2],
+                             data_vector_mode="diagonal", shotnoise_mode="both", apply_rsd=True,
+                             redshift_box=0.5, rsd=[0, 0, 1], _format="fits_lower"),
+     {"a": (29, 20000, False)}),
+    ("pk_fits_rsd_upper_w", dict(statistic="pk", correlation_mode="auto", nmesh=[32] * 3,
+                                 boxsize=[800.0] * 3, sampler="pcs", interlaced=True, k_min=0.005,
+                                 k_max=0.115, k_bins=8, poles=[0, 2, 4], apply_rsd=True, redshift_box=1.0,
+                                 rsd=[0, 1, 0], cosmology={"h": 0.7, "Omega0": 0.3}, _format="fits_upper"),
+     {"a": (30, 20000, True)}),
+    ("pk_fits_norsd_cross", dict(statistic="pk", correlation_mode="cross", nmesh=[32] * 3,
+                                 boxsize=[1000.0] * 3, sampler="cic", interlaced=False, k_min=0.005,
+                                 k_max=0.095, k_bins=9, poles=[0, 2], apply_rsd=False, _format="fits_lower"),
+     {"a": (31, 15000, True), "b": (32, 12000, False)}),
 ]
 
 
@@ -153,6 +171,11 @@ SURVEY_CASES = [
                                 sampler="cic", interlaced=True, k_min=0.005, k_max=0.045, k_bins=4,
                                 angu_config=[2, 0, 2], data_vector_mode="diagonal", shotnoise_mode="ana",
                                 normalization_scheme="mixed-mesh"), _SAB),
+    # cosmology without Omega0: the reference converts redshifts with Planck18
+    # (catalog_processor.py:610-625) and still multiplies by the config's h
+    ("sv_pk_auto_planck18", dict(statistic="pk", correlation_mode="auto", sampler="cic", interlaced=True,
+                                 k_min=0.005, k_max=0.085, k_bins=8, poles=[0, 2], cosmology={"h": 0.6766},
+                                 normalization_scheme="particle"), _SA),
     ("sv_bk_abc_000_diag", dict(statistic="bk_sugi", correlation_mode="cross", tracer_type="abc",
                                 sampler="tsc", interlaced=False, k_min=0.005, k_max=0.045, k_bins=4,
                                 angu_config=[0, 0, 0], data_vector_mode="diagonal", shotnoise_mode="ana",
@@ -191,6 +214,12 @@ def catalog_positions(seed, n_particles, boxsize):
     return lognormal_box(n_particles, boxsize, seed, grid=32)
 
 
+def catalog_velocities(seed, n):
+    """Peculiar velocities in km/s, N(0, 300) per axis."""
+    rng = np.random.Generator(np.random.PCG64(seed + 2000))
+    return rng.normal(0.0, 300.0, (n, 3))
+
+
 def catalog_weights(seed, n):
     rng = np.random.Generator(np.random.PCG64(seed + 1000))
     return 0.5 + rng.random(n)
@@ -205,9 +234,16 @@ def build_case(name, workdir):
             continue
         cfg = copy.deepcopy(_BASE)
         cfg.update(copy.deepcopy(over))
+        fmt = cfg.pop("_format", "npy")
         L = cfg["boxsize"][0]
         weighted = any(v[2] for v in cats.values())
         cfg["column_names"] = ["x", "y", "z", "w"] if weighted else ["x", "y", "z"]
+        if fmt.startswith("fits"):
+            names = ["x", "y", "z", "vx", "vy", "vz"]
+            if fmt == "fits_upper":
+                names = [c.upper() for c in names]
+            # an extra column the reference must ignore, and the weight column
+            cfg["column_names"] = names + (["w"] if weighted else []) + ["ID"]
         catalogs = {"data_a": None, "randoms_a": None, "data_b": None, "randoms_b": None}
         sums = {}
         os.makedirs(workdir, exist_ok=True)
@@ -217,8 +253,22 @@ def build_case(name, workdir):
             if weighted:
                 w = catalog_weights(seed, len(pos)) if wflag else np.ones(len(pos))
                 arr = np.column_stack([pos, w])
-            path = os.path.join(workdir, "%s_%s.npy" % (name, letter))
-            np.save(path, arr)
+            if fmt.startswith("fits"):
+                from cosmonpc_b200 import fits
+
+                vel = catalog_velocities(seed, len(pos))
+                cols = {nm: v for nm, v in zip(cfg["column_names"][:6], [pos[:, 0], pos[:, 1], pos[:, 2],
+                                                                           vel[:, 0], vel[:, 1], vel[:, 2]])}
+                if weighted:
+                    cols["w"] = arr[:, 3]
+                cols["ID"] = np.arange(len(pos), dtype=np.int64)
+                cols["MASS"] = np.full(len(pos), 1e12, dtype=np.float32)  # not requested
+                path = os.path.join(workdir, "%s_%s.fits" % (name, letter))
+                fits.write_table(path, cols)
+                arr = np.column_stack([arr, vel])
+            else:
+                path = os.path.join(workdir, "%s_%s.npy" % (name, letter))
+                np.save(path, arr)
             catalogs["data_" + letter] = path
             sums[letter] = float(np.sum(arr))
         cfg["catalogs"] = catalogs

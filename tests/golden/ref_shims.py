@@ -10,7 +10,8 @@ and ``h5py``; none is installed here, so this module places stand-ins in
   caller's frame (the form ``sympy.lambdify(..., "numexpr")`` emits).
 * ``pmesh.pm.ParticleMesh``: ``oracle.pmesh_lite`` (restated pmesh behaviour).
 * ``astropy.cosmology.FlatLambdaCDM``: comoving distance by ``scipy.integrate.quad``
-  (a vectorised 64-point Gauss-Legendre rule for large catalogs).
+  (a vectorised 64-point Gauss-Legendre rule for large catalogs); ``Planck18``
+  with its photon and massive-neutrino densities (``oracle/cosmology.py``).
 * ``fitsio.FITS``: this repository's FITS binary-table reader (``cosmonpc_b200.fits``).
 * ``h5py``: a placeholder (no workload here reads HDF5).
 """
@@ -144,8 +145,9 @@ def _install_astropy():
             self.h = self.H0 / 100.0
 
         def efunc(self, z):
-            z = np.asarray(z, dtype=np.float64)
-            return np.sqrt(self.Om0 * (1 + z) ** 3 + (1 - self.Om0))
+            # astropy's evaluation order for a flat cosmology without radiation
+            zp1 = np.asarray(z, dtype=np.float64) + 1.0
+            return np.sqrt(zp1 ** 2 * ((0.0 * zp1 + self.Om0) * zp1 + 0.0) + (1.0 - self.Om0))
 
         def comoving_distance(self, z):
             # (c / H0) int_0^z dt / E(t).  Few redshifts: scipy quad per value;
@@ -174,8 +176,20 @@ def _install_astropy():
         def value(self):
             return np.asarray(self)
 
+    class _Planck18(FlatLambdaCDM):
+        """astropy's Planck18 realisation: photons and one massive neutrino
+        (oracle/cosmology.py restates its background)."""
+
+        def __init__(self):
+            super().__init__(H0=67.66, Om0=0.30966)
+
+        def efunc(self, z):
+            from oracle import cosmology as oc
+
+            return oc.efunc(z)
+
     cosmo.FlatLambdaCDM = FlatLambdaCDM
-    cosmo.Planck18 = FlatLambdaCDM(67.66, 0.30966)
+    cosmo.Planck18 = _Planck18()
     units.Mpc = 1.0
     units.km = 1.0
     units.s = 1.0
