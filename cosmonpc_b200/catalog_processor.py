@@ -6,11 +6,11 @@ the weight (src/cosmonpc/catalog_processor.py:91-125, :354-386).  One process
 reads the whole file (the reference splits rows over MPI ranks and reduces
 the counts; the totals are identical).
 
-Box ``.fits`` catalogs (src/cosmonpc/catalog_processor.py:388-445): the
-requested columns that exist; positions from X, Y, Z or else x, y, z;
-velocities from VX, VY, VZ or else vx, vy, vz when ``apply_rsd``; weight ``w``.
-The raw rows go to the device unchanged and ``cnpc_box_catalog`` decodes them
-and applies the redshift-space shift of add_rsd (catalog_processor.py:648-693).
+Box ``.fits`` and ``.h5``/``.hdf5`` catalogs (src/cosmonpc/catalog_processor.py:
+16-88, :388-445): positions from X, Y, Z or else x, y, z; velocities from VX,
+VY, VZ or else vx, vy, vz when ``apply_rsd``; weight ``w``.  The raw columns go
+to the device as stored and ``cnpc_box_catalog`` decodes them and applies the
+redshift-space shift of add_rsd (catalog_processor.py:648-693).
 """
 from __future__ import annotations
 
@@ -121,9 +121,78 @@ def read_box(path, column_names, apply_rsd=False, cosmology=None, redshift_box=N
         return read_box_npy(path, column_names)
     if ext == "fits":
         return read_box_fits(path, column_names, apply_rsd, cosmology, redshift_box, los, boxsize)
-    from .hdf5 import read_box_hdf5
-
     return read_box_hdf5(path, column_names, apply_rsd, cosmology, redshift_box, los, boxsize)
+
+
+_CT_OF_NUMPY = {"f8": "F64", "f4": "F32", "i8": "I64", "i4": "I32", "i2": "I16", "u1": "U8"}
+
+
+def read_box_hdf5(paths, column_names, apply_rsd=False, cosmology=None, redshift_box=None, los=None,
+                  boxsize=None):
+    """Box HDF5 catalog(s) (h5_reader, catalog_processor.py:16-88, with the box
+    branch :388-445) decoded, and shifted into redshift space, on the device.
+
+    The reference builds its table with a field for every requested name, so
+    the position, velocity and weight columns are chosen from ``column_names``
+    itself; a chosen column that is not a dataset of the file would be left
+    uninitialised there and raises ValueError here.  Contiguous datasets are
+    copied to the device as stored; chunked (filtered) ones are inflated on the
+    host first."""
+    import torch
+
+    from . import _lib
+    from .hdf5 import _materialise, open_datasets
+
+    paths = [paths] if isinstance(paths, str) else list(paths)
+    names = list(column_names)
+    pos_axes = _pick(names, [("X", "Y", "Z"), ("x", "y", "z")])
+    vel_axes = _pick(names, [("VX", "VY", "VZ"), ("vx", "vy", "vz")]) if apply_rsd else None
+    shift = None
+    if apply_rsd:
+        if vel_axes is None:
+            raise UnboundLocalError("cannot access local variable 'velocities' where it is not associated "
+                                    "with a value")
+        shift = rsd_shift(cosmology, redshift_box, los)
+    box_length = float(np.asarray(boxsize, dtype=np.float64).reshape(-1)[0]) if boxsize is not None else 0.0
+    wanted = list(pos_axes or ()) + list(vel_axes or ()) + (["w"] if "w" in names else [])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = _lib.Context.get()
+    outs_p, outs_w = [], []
+    for path in paths:
+        infos, f = open_datasets(path)
+        nrows = next((infos[c].n for c in names if c in infos), 0)
+        keep = []  # device copies, alive until the decode is queued
+
+        def ref(name):
+            if name is None:
+                return _lib.ColRef(None, 0, _lib.CT_ABSENT, 0, 1.0, 0.0)
+            if name not in infos:
+                raise ValueError(f"{path}: column {name} is not a dataset of the file")
+            d = infos[name]
+            if d.n != nrows:
+                raise ValueError(f"{path}: dataset {name} has {d.n} rows, not {nrows}")
+            code = _CT_OF_NUMPY.get(d.dtype.str[1:])
+            if code is None:
+                raise ValueError(f"{path}: dataset {name}: unsupported element type {d.dtype}")
+            host = np.ascontiguousarray(_materialise(d, f))
+            t = torch.from_numpy(host.view(np.uint8).copy()).pin_memory().to(dev, non_blocking=True)
+            keep.append(t)
+            return _lib.ColRef(t.data_ptr(), d.dtype.itemsize, getattr(_lib, "CT_" + code),
+                               1 if d.dtype.byteorder == ">" else 0, 1.0, 0.0)
+
+        cols = [ref(pos_axes[k] if pos_axes else None) for k in range(3)]
+        cols += [ref(vel_axes[k] if vel_axes else None) for k in range(3)]
+        cols.append(ref("w" if "w" in wanted else None))
+        pos = torch.empty((max(nrows, 1), 3), dtype=torch.float64, device=dev)[:nrows]
+        w = torch.empty(max(nrows, 1), dtype=torch.float64, device=dev)[:nrows]
+        ctx.box_catalog(nrows, cols, apply_rsd, shift, box_length, pos, w)
+        for t in keep:
+            t.record_stream(torch.cuda.current_stream(dev))
+        outs_p.append(pos)
+        outs_w.append(w)
+    if len(outs_p) == 1:
+        return outs_p[0], outs_w[0]
+    return torch.cat(outs_p), torch.cat(outs_w)
 
 
 def read_box_npy(path, column_names):

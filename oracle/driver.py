@@ -21,7 +21,8 @@ def _efunc_flat(om0, z):
 def read_box_catalog(path, column_names, apply_rsd=False, cosmology=None, redshift_box=None, los=None,
                      boxsize=None):
     """``catalog_reader`` box branches: ``.npy`` (catalog_processor.py:354-386),
-    and ``.fits`` (:388-445) with ``add_rsd`` (:648-693) when ``apply_rsd``."""
+    ``.fits`` and ``.h5``/``.hdf5`` (:388-445, h5_reader :16-88) with ``add_rsd``
+    (:648-693) when ``apply_rsd``."""
     if str(path).lower().endswith(".fits"):
         from cosmonpc_b200.fits import open_table
 
@@ -46,6 +47,37 @@ def read_box_catalog(path, column_names, apply_rsd=False, cosmology=None, redshi
             pos += factor * los_v * vel
             pos = pos % np.asarray(boxsize, dtype=np.float64)[0]
         w = np.asarray(data["w"], dtype=np.float64) if "w" in names else np.ones(t.nrows)
+        return pos, w
+    if str(path).lower().endswith((".h5", ".hdf5")):
+        # h5_reader (cp:16-88) gives every requested name a field, so the
+        # columns are chosen from column_names itself
+        from cosmonpc_b200.hdf5 import read_dataset
+
+        col = {}
+        for c in column_names:
+            try:
+                col[c] = np.asarray(read_dataset(path, c), dtype=np.float64)
+            except KeyError:
+                pass
+        n = len(next(iter(col.values()))) if col else 0
+        pos = np.zeros((n, 3))
+        for axes in (("X", "Y", "Z"), ("x", "y", "z")):
+            if all(a in column_names for a in axes):
+                pos = np.column_stack([col[a] for a in axes])
+                break
+        if apply_rsd:
+            vel = None
+            for axes in (("VX", "VY", "VZ"), ("vx", "vy", "vz")):
+                if all(a in column_names for a in axes):
+                    vel = np.column_stack([col[a] for a in axes])
+                    break
+            factor = (1 + redshift_box) / (_efunc_flat(cosmology["Omega0"], redshift_box) * 100)
+            los_v = np.array(los)
+            if np.linalg.norm(los_v) != 1:
+                raise ValueError("LOS must be a 3d unit vector")
+            pos += factor * los_v * vel
+            pos = pos % np.asarray(boxsize, dtype=np.float64)[0]
+        w = col["w"] if "w" in column_names else np.ones(n)
         return pos, w
     arr = np.load(path, mmap_mode="r")
     idx = [column_names.index(a) for a in ("x", "y", "z")]

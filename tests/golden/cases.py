@@ -110,6 +110,18 @@ CASES = [
                                  boxsize=[1000.0] * 3, sampler="cic", interlaced=False, k_min=0.005,
                                  k_max=0.095, k_bins=9, poles=[0, 2], apply_rsd=False, _format="fits_lower"),
      {"a": (31, 15000, True), "b": (32, 12000, False)}),
+    # box catalogs in HDF5 files (h5_reader, catalog_processor.py:16-88): float64,
+    # big-endian, float32 and chunked/deflated columns
+    ("bk_h5_rsd_full", dict(statistic="bk_sugi", correlation_mode="auto", tracer_type="aaa",
+                            nmesh=[32] * 3, boxsize=[1000.0] * 3, sampler="cic", interlaced=True,
+                            k_min=0.005, k_max=0.045, k_bins=3, angu_config=[0, 0, 0],
+                            data_vector_mode="full", shotnoise_mode="ana", apply_rsd=True,
+                            redshift_box=0.3, rsd=[1, 0, 0], _format="h5_lower"),
+     {"a": (33, 20000, True)}),
+    ("pk_h5_upper_norsd", dict(statistic="pk", correlation_mode="auto", nmesh=[32] * 3,
+                               boxsize=[1000.0] * 3, sampler="tsc", interlaced=True, k_min=0.005,
+                               k_max=0.095, k_bins=9, poles=[0, 2, 4], apply_rsd=False, _format="h5_upper"),
+     {"a": (34, 20000, False)}),
 ]
 
 
@@ -238,9 +250,9 @@ def build_case(name, workdir):
         L = cfg["boxsize"][0]
         weighted = any(v[2] for v in cats.values())
         cfg["column_names"] = ["x", "y", "z", "w"] if weighted else ["x", "y", "z"]
-        if fmt.startswith("fits"):
+        if fmt.startswith(("fits", "h5")):
             names = ["x", "y", "z", "vx", "vy", "vz"]
-            if fmt == "fits_upper":
+            if fmt.endswith("_upper"):
                 names = [c.upper() for c in names]
             # an extra column the reference must ignore, and the weight column
             cfg["column_names"] = names + (["w"] if weighted else []) + ["ID"]
@@ -266,6 +278,21 @@ def build_case(name, workdir):
                 path = os.path.join(workdir, "%s_%s.fits" % (name, letter))
                 fits.write_table(path, cols)
                 arr = np.column_stack([arr, vel])
+            elif fmt.startswith("h5"):
+                from cosmonpc_b200 import hdf5
+
+                vel = catalog_velocities(seed, len(pos))
+                n6 = cfg["column_names"][:6]
+                cols = {n6[0]: pos[:, 0], n6[1]: pos[:, 1].astype(">f8"), n6[2]: pos[:, 2],
+                        n6[3]: vel[:, 0].astype(np.float32), n6[4]: vel[:, 1], n6[5]: vel[:, 2]}
+                if weighted:
+                    cols["w"] = arr[:, 3]
+                cols["ID"] = np.arange(len(pos), dtype=np.int64)
+                path = os.path.join(workdir, "%s_%s.h5" % (name, letter))
+                hdf5.write_columns(path, cols, chunked={n6[2]: 4096, n6[5]: 3000})
+                v32 = vel.copy()
+                v32[:, 0] = v32[:, 0].astype(np.float32)
+                arr = np.column_stack([arr, v32])
             else:
                 path = os.path.join(workdir, "%s_%s.npy" % (name, letter))
                 np.save(path, arr)

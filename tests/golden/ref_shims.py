@@ -13,7 +13,7 @@ and ``h5py``; none is installed here, so this module places stand-ins in
   (a vectorised 64-point Gauss-Legendre rule for large catalogs); ``Planck18``
   with its photon and massive-neutrino densities (``oracle/cosmology.py``).
 * ``fitsio.FITS``: this repository's FITS binary-table reader (``cosmonpc_b200.fits``).
-* ``h5py``: a placeholder (no workload here reads HDF5).
+* ``h5py.File``: this repository's HDF5 reader (``cosmonpc_b200.hdf5``).
 """
 from __future__ import annotations
 
@@ -243,6 +243,49 @@ def _install_fitsio():
     sys.modules["fitsio"] = fitsio
 
 
+def _install_h5py():
+    """``h5py.File`` over this repository's HDF5 reader (root-group datasets)."""
+    sys.path.insert(0, _REPO)
+    from cosmonpc_b200 import hdf5 as _h5
+
+    h5py = types.ModuleType("h5py")
+
+    class _Dataset:
+        def __init__(self, path, info):
+            self._path, self._info, self._arr = path, info, None
+
+        def __len__(self):
+            return self._info.n
+
+        def __getitem__(self, sl):
+            if self._arr is None:
+                self._arr = _h5.read_dataset(self._path, self._info.name)
+            return self._arr[sl]
+
+    class File:
+        def __init__(self, path, mode="r"):
+            self._path = path
+            self._infos, _ = _h5.open_datasets(path)
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def __contains__(self, key):
+            return key in self._infos
+
+        def __getitem__(self, key):
+            return _Dataset(self._path, self._infos[key])
+
+        def keys(self):
+            return list(self._infos)
+
+    h5py.File = File
+    sys.modules["h5py"] = h5py
+
+
 def _install_placeholders():
     for name in ("fitsio", "h5py"):
         sys.modules.setdefault(name, types.ModuleType(name))
@@ -255,6 +298,7 @@ def import_reference():
     _install_pmesh()
     _install_astropy()
     _install_fitsio()
+    _install_h5py()
     _install_placeholders()
     if REFERENCE_SRC not in sys.path:
         sys.path.insert(0, REFERENCE_SRC)
