@@ -342,6 +342,13 @@ def _mocks_throughput(per_class, seed, barrier, max_over_ranks, world=1):
                         "256^3/L2000"}
 
 
+def _tuned_plans():
+    """Shell-synthesis batch depth per shape class chosen by the autotuner."""
+    from cosmonpc_b200 import autotune
+
+    return {k: {"fft_batch": v["fft_batch"], "ms_per_field": v["ms_per_field"]} for k, v in autotune.plans().items()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -637,6 +644,7 @@ def main():
         "plain_rel_err_by_key": rel_by_key,
         "survey": survey,
         "amortized": amortized,
+        "plans": _tuned_plans(),
         "serial": {"value": t_serial, "unit": UNIT,
                    "note": "one data vector at a time, host algebra not overlapped with the next vector"},
         "cpu_baseline": cpu,

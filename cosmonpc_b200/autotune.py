@@ -1,0 +1,154 @@
+"""Per-shape-class execution plans, measured once per device and cached on disk.
+
+The reference leaves the memory/throughput trade-off of the bispectrum to its
+``block_size`` setting (clustering_estimator.py:867-879, task_executor.py:
+166-169): how many k-bins' shell fields are held at once.  Here that choice
+and the batch depth of the shell-field synthesis are made per shape class:
+
+* block size: the largest bin block whose shell fields fit the device-memory
+  budget (80 % of the free HBM, ``engine.fields_capacity``), because a block
+  of all bins computes every field once and smaller blocks recompute fields
+  (the reference's own block loop); a requested ``block_size`` still caps it;
+* shell items per synthesis call (``ShellFields.fft_batch``): the fused FP32
+  band-limited kernels and the shell-spectra + cuFFT route both take a batch
+  of fields per call; deeper batches fill the GPU better and cost one pass-1
+  work array (fused) or one half spectrum (cuFFT) per field.  The candidates
+  that fit the budget are timed on a synthetic spectrum of the class (CUDA
+  events, best of a few repetitions) and the fastest per field wins.
+
+Plans are keyed by (device name, n, precision, synthesis route) and kept in a
+JSON file (``$CNPC_TUNE_CACHE``, default ``~/.cache/cosmonpc_b200/plans.json``)
+so a later process reuses them; ``AUTOTUNE = False`` falls back to the fixed
+default batch of 8.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import numpy as np
+
+AUTOTUNE = True
+DEFAULT_BATCH = 8
+CANDIDATES = (2, 4, 8, 12, 16, 24)
+_lock = threading.Lock()
+_plans = None
+
+
+def cache_path():
+    return os.environ.get("CNPC_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "cosmonpc_b200",
+                                                         "plans.json"))
+
+
+def _load():
+    global _plans
+    if _plans is None:
+        try:
+            with open(cache_path()) as f:
+                _plans = json.load(f)
+        except Exception:
+            _plans = {}
+    return _plans
+
+
+def _save():
+    path = cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp%d" % os.getpid()
+        with open(tmp, "w") as f:
+            json.dump(_plans, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only home: the plan stays in memory for this process
+
+
+def _key(n, precision, fused):
+    import torch
+
+    return "%s|n%d|%s|%s" % (torch.cuda.get_device_name(), int(n), precision, "fused" if fused else "cufft")
+
+
+def plans():
+    """All cached plans ({key: plan dict})."""
+    with _lock:
+        return dict(_load())
+
+
+def fft_batch(n, boxsize, edges, precision):
+    """Shell items per synthesis call for this shape class (tuned once)."""
+    from . import engine
+
+    if not AUTOTUNE:
+        return DEFAULT_BATCH
+    fused = engine.fused_shells_apply(n, boxsize, edges, range(len(edges) - 1), precision)
+    key = _key(n, precision, fused)
+    with _lock:
+        p = _load().get(key)
+        if p is not None:
+            return int(p["fft_batch"])
+    import torch
+
+    if torch.cuda.is_current_stream_capturing():
+        return DEFAULT_BATCH  # no timing inside a graph capture
+    plan = _measure(n, boxsize, edges, precision, fused)
+    with _lock:
+        _load()[key] = plan
+        _save()
+    return int(plan["fft_batch"])
+
+
+def _measure(n, boxsize, edges, precision, fused):
+    """Time shell synthesis of 2 x max(candidates) fields at each batch depth."""
+    import torch
+
+    from . import _lib, angular, engine
+
+    ctx = _lib.Context.get()
+    code, rdt, cdt = engine.PRECISION[precision]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    esz = 4 if precision == "f32" else 8
+    per_field = n ** 3 * esz
+    per_batch_item = (n * (n // 2) * (n // 4) * 8) if fused else (n * n * (n // 2 + 1) * 2 * esz)
+    free = engine.free_device_bytes()
+    budget = int(free * 0.5)
+    cands = [b for b in CANDIDATES if b * (per_field + per_batch_item) <= budget]
+    if not cands:
+        return {"fft_batch": 1, "ms_per_field": None, "timed": {}}
+    nitems = 2 * max(cands)
+    while nitems > 1 and nitems * per_field + max(cands) * per_batch_item > budget:
+        nitems -= 1
+    g = torch.Generator(device=dev).manual_seed(20261203)
+    real = torch.randn((n, n, n), generator=g, device=dev, dtype=rdt)
+    spec = torch.empty((n, n, n // 2 + 1), dtype=cdt, device=dev)
+    ctx.r2c(code, n, 1, real, spec)
+    del real
+    nb = len(edges) - 1
+    keys = [((0, 0, 0, False), b % nb, 0) if i % 2 == 0 else ((2, 0, 0, False), b % nb, 0)
+            for i, b in enumerate(range(nitems))]
+    timed = {}
+    for b in cands:
+        sf = engine.ShellFields(n, boxsize, edges, precision, spec, None, capacity=nitems, fft_batch=b)
+        best = None
+        for rep in range(3):
+            sf.release_all()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sf.ensure(keys)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if rep > 0:  # the first repetition makes plans and workspaces
+                best = ms if best is None else min(best, ms)
+        timed[str(b)] = best / nitems
+        del sf
+    torch.cuda.empty_cache()
+    win = min(timed, key=timed.get)
+    _ = angular  # harmonics are made by ShellFields itself
+    return {"fft_batch": int(win), "ms_per_field": timed[win], "timed": timed}
+
+
+def block_plan(bins_needed, k_bins, capacity_fields):
+    """The block size _plan_blocks chose and why (for reports)."""
+    return {"block_size": int(bins_needed), "k_bins": int(k_bins), "fields_resident": int(capacity_fields)}

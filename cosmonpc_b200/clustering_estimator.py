@@ -114,7 +114,9 @@ def _plan_blocks(specs, k_bins, n, precision, requested, diagonal, free_bytes=No
     """Bin block size and shell-field capacity for one pair_sums call.
 
     ``requested`` is the reference's block_size (ce:867-879): "full"/None means all
-    bins at once.  The block shrinks further if the fields do not fit in HBM.
+    bins at once.  The block is the largest one whose fields fit the HBM budget
+    (autotune: a block of all bins computes each field once; smaller blocks
+    recompute them), capped by the request.
     """
     if diagonal or requested == "full" or requested is None:
         bs = k_bins

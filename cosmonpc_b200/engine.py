@@ -177,7 +177,7 @@ class ShellFields:
     2 (unit spectrum).  Fields are stored as rows of one [capacity, n^3] tensor.
     """
 
-    def __init__(self, n, boxsize, edges, precision, spec_a, spec_b, capacity, fft_batch=8,
+    def __init__(self, n, boxsize, edges, precision, spec_a, spec_b, capacity, fft_batch=None,
                  racah=True):
         self.n = n
         self.boxsize = float(boxsize)
@@ -192,6 +192,10 @@ class ShellFields:
         # rows padded off the 2^k-byte stride of an n^3 field (see FIELD_PAD)
         self.stride = n * n * n + FIELD_PAD
         self.fields = torch.empty((self.capacity, self.stride), dtype=self.rdt, device=dev)
+        if fft_batch is None:  # the shape class's tuned batch depth
+            from . import autotune
+
+            fft_batch = autotune.fft_batch(n, boxsize, edges, precision)
         self.fft_batch = max(1, min(int(fft_batch), self.capacity))
         self._scratch = None
         self.slot = {}

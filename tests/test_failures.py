@@ -151,3 +151,31 @@ def test_timed_out_wait_surfaces_from_the_estimator():
             pass
     res = api.bk_sugi_box_vector(pos, None, **kw)[0]
     assert np.isfinite(res["B_sugi"]).all()
+
+
+@pytest.mark.gpu
+def test_autotuned_plan_is_cached_and_exact(tmp_path, monkeypatch):
+    """The autotuner times shell-synthesis batch depths for a shape class once,
+    caches the winner on disk, and the tuned plan gives the same data vector as
+    the fixed default batch."""
+    import json
+
+    from cosmonpc_b200 import api, autotune
+    from cosmonpc_b200.mocks import lognormal_box
+
+    monkeypatch.setenv("CNPC_TUNE_CACHE", str(tmp_path / "plans.json"))
+    monkeypatch.setattr(autotune, "_plans", None)
+    pos = lognormal_box(150000, 800.0, 41)
+    kw = dict(nmesh=64, boxsize=800.0, sampler="tsc", interlaced=True, k_min=0.01, k_max=0.11, k_bins=8,
+              angu_configs=[(0, 0, 0), (2, 0, 2)], data_vector_mode="full", shotnoise_mode="both",
+              precision="f32")
+    tuned = api.bk_sugi_box_vector(pos, None, **kw)
+    saved = json.load(open(tmp_path / "plans.json"))
+    assert any("|n64|f32|fused" in k for k in saved)
+    plan = next(v for k, v in saved.items() if "|n64|f32|fused" in k)
+    assert plan["fft_batch"] in autotune.CANDIDATES and plan["timed"]
+    monkeypatch.setattr(autotune, "AUTOTUNE", False)
+    fixed = api.bk_sugi_box_vector(pos, None, **kw)
+    for a, b in zip(tuned, fixed):
+        for key in ("B_sugi", "Bk_raw", "Shot_noise"):
+            np.testing.assert_allclose(a[key], b[key], rtol=1e-12, atol=0)
