@@ -354,6 +354,190 @@ __global__ void tile_paint_kernel(const double4 *__restrict__ sorted, const int 
     }
 }
 
+// ------------------------------------------------- compact-record tiled paint
+// For windows of order 2..4 (continuous weights) the sort writes a 16-byte
+// record per particle instead of its FP64 grid coordinates: the FP32
+// fraction of the window argument per axis (g - floor(g) for even orders,
+// (g + 1/2) - floor(g + 1/2) for odd ones) and the first stencil node of both
+// grids relative to the tile's region, packed in 5 bits per axis.  Node
+// selection stays FP64-exact (made in the sort); the 1-D weights are the
+// window polynomials of the fraction in FP32 (the per-particle kernel rounds
+// its FP64 weights to FP32 for FP32 meshes; both are within a few FP32 ulps).
+// The +1/2-shifted grid's fraction is f + 1/2 - (its first node - the plain
+// grid's first node).  Weights other than 1 travel in a separate FP32 array.
+struct __align__(16) PaintRec {
+    float fx, fy, fz;
+    uint32_t nodes;  // plain grid x, y, z then shifted grid x, y, z: 5 bits each
+};
+
+template <int P> __device__ inline double window_arg(double g) { return (P % 2 == 0) ? g : __dadd_rn(g, 0.5); }
+
+template <int P>
+__global__ void tile_scatter_rec_kernel(const double *__restrict__ pos, const double *__restrict__ weight,
+                                        int64_t np, int n, Frame scale, const int *tile_of, int *cursor,
+                                        PaintRec *sorted, float *sorted_w) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+        double g[3];
+        grid_coords(pos, i, scale, g);
+        const int tid = tile_of[i];
+        const unsigned same = __match_any_sync(__activemask(), tid);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(same) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&cursor[tid], __popc(same));
+        base = __shfl_sync(same, base, leader);
+        const int slot = base + __popc(same & ((1u << lane) - 1));
+        PaintRec r;
+        float f[3];
+        uint32_t nodes = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int org = region_origin(g[d], n);
+            const double a = window_arg<P>(g[d]);
+            const double fl = floor(a);
+            f[d] = (float)__dsub_rn(a, fl);
+            const uint32_t b0 = (uint32_t)(axis_base<P>(g[d]) - org);
+            const uint32_t b1 = (uint32_t)(axis_base<P>(__dadd_rn(g[d], 0.5)) - org);
+            nodes |= b0 << (5 * d);
+            nodes |= b1 << (15 + 5 * d);
+        }
+        r.fx = f[0], r.fy = f[1], r.fz = f[2];
+        r.nodes = nodes;
+        sorted[slot] = r;
+        if (sorted_w) sorted_w[slot] = (float)mass_of(weight, i, scale);
+    }
+}
+
+// 1-D weights of the nodes first .. first + P - 1 from the window fraction f
+template <int P> __device__ __forceinline__ void window_weights_f32(float f, float *w) {
+    if (P == 2) {
+        w[0] = 1.f - f;
+        w[1] = f;
+    } else if (P == 3) {
+        const float h = 0.5f - f, u = 1.f - f;
+        w[0] = 0.5f * u * u;
+        w[1] = 0.75f - h * h;
+        w[2] = 0.5f * f * f;
+    } else {  // P == 4
+        const float u = 1.f - f, f2 = f * f, u2 = u * u;
+        constexpr float s6 = 1.f / 6.f;
+        w[0] = s6 * u2 * u;
+        w[1] = s6 * (4.f - 6.f * f2 + 3.f * f2 * f);
+        w[2] = s6 * (4.f - 6.f * u2 + 3.f * u2 * u);
+        w[3] = s6 * f2 * f;
+    }
+}
+
+template <int P, bool FIXED>
+__device__ __forceinline__ void deposit_rec(int *reg, float scale, uint32_t bx, uint32_t by, uint32_t bz, float fx,
+                                            float fy, float fz, float mass) {
+    float wx[P], wy[P], wz[P];
+    window_weights_f32<P>(fx, wx);
+    window_weights_f32<P>(fy, wy);
+    window_weights_f32<P>(fz, wz);
+    const int base = ((int)bx * kRegion + (int)by) * kRegion + (int)bz;
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+#pragma unroll
+        for (int b = 0; b < P; ++b) {
+            const float wab = mass * wx[a] * wy[b];
+#pragma unroll
+            for (int c = 0; c < P; ++c) region_add<FIXED>(reg, base + (a * kRegion + b) * kRegion + c, wab * wz[c], scale);
+        }
+    }
+}
+
+template <typename T, int P>
+__global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const float *__restrict__ sorted_w,
+                                      float mass_const, const int *__restrict__ offset, int ntiles, int tpa, int n,
+                                      T *mesh, T *mesh_shifted) {
+    extern __shared__ int reg[];  // [2][kRegionCells]
+    __shared__ int colc[kRegion * kRegion];
+    __shared__ int wrap_t[3][kRegion];
+    __shared__ unsigned s_mbits;
+    __shared__ int s_cmax;
+    const int nreg = mesh_shifted ? 2 : 1;
+    const int lane = threadIdx.x & 31;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int p0 = offset[tile], p1 = offset[tile + 1];
+        if (p0 == p1) continue;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0;
+        for (int i = threadIdx.x; i < kRegion * kRegion; i += blockDim.x) colc[i] = 0;
+        if (threadIdx.x == 0) s_mbits = 0u, s_cmax = 0;
+        if (threadIdx.x < 3 * kRegion) {
+            const int ax = threadIdx.x / kRegion, ri = threadIdx.x % kRegion;
+            const int tcoord = ax == 0 ? tile / (tpa * tpa) : (ax == 1 ? (tile / tpa) % tpa : tile % tpa);
+            wrap_t[ax][ri] = wrapi((int64_t)tcoord * kTile - 1 + ri, n);
+        }
+        __syncthreads();
+        // bound of any node's sum: particles per first-node column, max |mass|
+        float mloc = sorted_w ? 0.f : fabsf(mass_const);
+        for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+            const uint32_t nodes = sorted[i].nodes;
+            atomicAdd(&colc[(int)(nodes & 31u) * kRegion + (int)((nodes >> 5) & 31u)], 1);
+            if (sorted_w) mloc = fmaxf(mloc, fabsf(sorted_w[i]));
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) mloc = fmaxf(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
+        if (lane == 0) atomicMax(&s_mbits, __float_as_uint(mloc));
+        __syncthreads();
+        int cm = 0;
+        for (int c = threadIdx.x; c < kRegion * kRegion; c += blockDim.x) {
+            const int x = c / kRegion, y = c % kRegion;
+            int sum = 0;
+            for (int dx = 0; dx <= P && dx <= x; ++dx)
+                for (int dy = 0; dy <= P && dy <= y; ++dy) sum += colc[(x - dx) * kRegion + (y - dy)];
+            cm = max(cm, sum);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) cm = max(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+        if (lane == 0) atomicMax(&s_cmax, cm);
+        __syncthreads();
+        constexpr float wa = window_wmax<P>();
+        // FP32 weights may exceed wmax^3 by a few ulps: slack (1 + 2^-20)
+        const double one = (double)__uint_as_float(s_mbits) * (double)(wa * wa * wa) * (1.0 + 0x1p-20);
+        const double bound = (double)s_cmax * one;
+        const double room = 2147483647.0 - (double)s_cmax;
+        int e = 100;
+        if (bound > 0.0) e = min(100, min(ilogb(room / bound), ilogb(4194304.0 / one)));
+        const float scale = ldexpf(1.f, e);
+        const bool fixed = s_cmax <= 65536;
+        auto deposit_all = [&](auto fixed_tag) {
+            constexpr bool F = decltype(fixed_tag)::value;
+            for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+                const PaintRec r = sorted[i];
+                const float m = sorted_w ? sorted_w[i] : mass_const;
+                deposit_rec<P, F>(reg, scale, r.nodes & 31u, (r.nodes >> 5) & 31u, (r.nodes >> 10) & 31u, r.fx, r.fy,
+                                  r.fz, m);
+                if (mesh_shifted) {
+                    const uint32_t b1x = (r.nodes >> 15) & 31u, b1y = (r.nodes >> 20) & 31u, b1z = (r.nodes >> 25) & 31u;
+                    const float gx = r.fx + 0.5f - (float)((int)b1x - (int)(r.nodes & 31u));
+                    const float gy = r.fy + 0.5f - (float)((int)b1y - (int)((r.nodes >> 5) & 31u));
+                    const float gz = r.fz + 0.5f - (float)((int)b1z - (int)((r.nodes >> 10) & 31u));
+                    deposit_rec<P, F>(reg + kRegionCells, scale, b1x, b1y, b1z, gx, gy, gz, m);
+                }
+            }
+        };
+        if (fixed)
+            deposit_all(std::true_type{});
+        else
+            deposit_all(std::false_type{});
+        __syncthreads();
+        const double unscale = ldexp(1.0, -e);
+        for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
+            const int word = reg[i];
+            if (word == 0) continue;
+            const float v = fixed ? (float)((double)word * unscale) : __int_as_float(word);
+            const int r = i % kRegionCells;
+            const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
+            const size_t cell = ((size_t)wrap_t[0][rx] * n + wrap_t[1][ry]) * n + wrap_t[2][rz];
+            atomicAdd((i < kRegionCells ? mesh : mesh_shifted) + cell, (T)v);
+        }
+    }
+}
+
 template <typename T>
 static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n, const Frame &scale,
                         int window, T *m1, T *m2, cudaStream_t s) {
@@ -378,6 +562,30 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
     const int pblocks = (int)std::min<int64_t>((np + threads - 1) / threads, (int64_t)ctx->num_sms * 16);
     tile_count_kernel<<<pblocks, threads, 0, s>>>(pos, np, n, scale, tpa, count, tile_of);
     tile_scan_kernel<<<1, 1024, 0, s>>>(count, nt, offset, cursor);
+    if (window >= 2 && std::is_same<T, float>::value) {
+        // compact records: 16 bytes per particle (+4 with weights) in the
+        // space of the FP64 records
+        PaintRec *rec = reinterpret_cast<PaintRec *>(sorted);
+        float *rec_w = w ? reinterpret_cast<float *>(rec + np) : nullptr;
+        const size_t smem = sizeof(int) * kRegionCells * (m2 ? 2 : 1);
+        const int tblocks = (int)std::min<int64_t>(nt, (int64_t)ctx->num_sms * 8);
+        switch (window) {
+#define CNPC_TPR(P_)                                                                                          \
+    case P_:                                                                                                  \
+        tile_scatter_rec_kernel<P_><<<pblocks, threads, 0, s>>>(pos, w, np, n, scale, tile_of, cursor, rec, rec_w); \
+        st = check_cuda(ctx, cudaFuncSetAttribute(tile_paint_rec_kernel<T, P_>,                               \
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),    \
+                        "tile paint smem");                                                                   \
+        if (st) return st;                                                                                    \
+        tile_paint_rec_kernel<T, P_><<<tblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale, offset, nt, \
+                                                                tpa, n, m1, m2);                              \
+        break;
+            CNPC_TPR(2) CNPC_TPR(3) CNPC_TPR(4)
+#undef CNPC_TPR
+            default: return fail(ctx, CNPC_EINVAL, "window must be 1..4");
+        }
+        return check_launch(ctx, "tile_paint_rec_kernel");
+    }
     tile_scatter_kernel<<<pblocks, threads, 0, s>>>(pos, w, np, scale, tile_of, cursor, sorted);
     st = check_launch(ctx, "tile sort");
     if (st) return st;
