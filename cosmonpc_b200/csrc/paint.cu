@@ -448,10 +448,16 @@ __device__ __forceinline__ void deposit_rec(int *reg, float scale, uint32_t bx, 
     }
 }
 
+// color >= 0: only the tiles whose coordinates have the parities of `color`
+// (bit 2: x, 1: y, 0: z), whose regions (20 nodes wide, tiles 32 nodes
+// apart with an even tile count per axis) never overlap, so the flush adds
+// each region to the mesh with plain loads and stores, and 8 launches in a
+// fixed order give bitwise reproducible meshes; color < 0: every tile in one
+// launch, flushed with atomics.
 template <typename T, int P>
 __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const float *__restrict__ sorted_w,
                                       float mass_const, const int *__restrict__ offset, int ntiles, int tpa, int n,
-                                      T *mesh, T *mesh_shifted) {
+                                      T *mesh, T *mesh_shifted, int color) {
     extern __shared__ int reg[];  // [2][kRegionCells]
     __shared__ int colc[kRegion * kRegion];
     __shared__ int wrap_t[3][kRegion];
@@ -459,7 +465,14 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
     __shared__ int s_cmax;
     const int nreg = mesh_shifted ? 2 : 1;
     const int lane = threadIdx.x & 31;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int half = tpa / 2;
+    const int nwork = color < 0 ? ntiles : half * half * half;
+    for (int work = blockIdx.x; work < nwork; work += gridDim.x) {
+        int tile = work;
+        if (color >= 0) {
+            const int i = work / (half * half), j = (work / half) % half, k = work % half;
+            tile = ((2 * i + ((color >> 2) & 1)) * tpa + (2 * j + ((color >> 1) & 1))) * tpa + (2 * k + (color & 1));
+        }
         const int p0 = offset[tile], p1 = offset[tile + 1];
         if (p0 == p1) continue;
         __syncthreads();
@@ -533,7 +546,11 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
             const int r = i % kRegionCells;
             const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
             const size_t cell = ((size_t)wrap_t[0][rx] * n + wrap_t[1][ry]) * n + wrap_t[2][rz];
-            atomicAdd((i < kRegionCells ? mesh : mesh_shifted) + cell, (T)v);
+            T *dst = (i < kRegionCells ? mesh : mesh_shifted) + cell;
+            if (color >= 0)
+                *dst += (T)v;
+            else
+                atomicAdd(dst, (T)v);
         }
     }
 }
@@ -569,6 +586,7 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
         float *rec_w = w ? reinterpret_cast<float *>(rec + np) : nullptr;
         const size_t smem = sizeof(int) * kRegionCells * (m2 ? 2 : 1);
         const int tblocks = (int)std::min<int64_t>(nt, (int64_t)ctx->num_sms * 8);
+        const int cblocks = (int)std::max<int64_t>(1, std::min<int64_t>(nt / 8, (int64_t)ctx->num_sms * 8));
         switch (window) {
 #define CNPC_TPR(P_)                                                                                          \
     case P_:                                                                                                  \
@@ -577,8 +595,14 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),    \
                         "tile paint smem");                                                                   \
         if (st) return st;                                                                                    \
-        tile_paint_rec_kernel<T, P_><<<tblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale, offset, nt, \
-                                                                tpa, n, m1, m2);                              \
+        if (tpa % 2 == 0 && n % kTile == 0) {                                                                 \
+            for (int color = 0; color < 8; ++color)                                                           \
+                tile_paint_rec_kernel<T, P_><<<cblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale,  \
+                                                                        offset, nt, tpa, n, m1, m2, color);   \
+        } else {                                                                                              \
+            tile_paint_rec_kernel<T, P_><<<tblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale, offset, \
+                                                                    nt, tpa, n, m1, m2, -1);                  \
+        }                                                                                                     \
         break;
             CNPC_TPR(2) CNPC_TPR(3) CNPC_TPR(4)
 #undef CNPC_TPR

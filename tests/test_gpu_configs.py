@@ -14,7 +14,6 @@ With CNPC_PARITY_REPORT=<path> each case appends its per-key errors to that
 file as one JSON line.
 """
 import copy
-import json
 import os
 
 import numpy as np
@@ -22,7 +21,7 @@ import pytest
 
 from cases import flatten_result
 from configs import CONFIG_CASES, build_config_case
-from conftest import GOLDEN, rel_err
+from conftest import GOLDEN, parity_report, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -58,10 +57,6 @@ def test_config_case_matches_reference(name, precision, workdir, tmp_path):
             np.testing.assert_array_equal(got[k], gold[k])
         else:
             errs[k] = rel_err(got[k], gold[k])
-    report = os.environ.get("CNPC_PARITY_REPORT")
-    if report:
-        with open(report, "a") as f:
-            f.write(json.dumps({"case": name, "precision": precision, "max": max(errs.values()),
-                                "errors": errs}) + "\n")
+    parity_report(name, precision, errs)
     bad = {k: e for k, e in errs.items() if not e < TOL[precision]}
     assert not bad, (bad, errs)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from cases import SURVEY_CASES, build_case, flatten_result
-from conftest import GOLDEN, rel_err, tol
+from conftest import GOLDEN, parity_report, rel_err, tol
 
 pytestmark = pytest.mark.gpu
 
@@ -166,6 +166,7 @@ def test_survey_golden_case(name, precision, tmp_path):
     for k in ("k_num", "nmodes"):
         if k in keys:
             np.testing.assert_array_equal(got[k], gold[k])
+    parity_report(name, precision, errs)
     bad = {k: e for k, e in errs.items() if not e < tol(precision, name, k)}
     assert not bad, (bad, errs)
     assert res["nmesh"] == cfg["nmesh"] and "nyquist_freq" in res
