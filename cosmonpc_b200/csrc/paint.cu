@@ -448,16 +448,14 @@ __device__ __forceinline__ void deposit_rec(int *reg, float scale, uint32_t bx, 
     }
 }
 
-// color >= 0: only the tiles whose coordinates have the parities of `color`
-// (bit 2: x, 1: y, 0: z), whose regions (20 nodes wide, tiles 32 nodes
-// apart with an even tile count per axis) never overlap, so the flush adds
-// each region to the mesh with plain loads and stores, and 8 launches in a
-// fixed order give bitwise reproducible meshes; color < 0: every tile in one
-// launch, flushed with atomics.
+// region_out != nullptr: each tile writes its whole region (both grids, FP32
+// values) to region_out[tile] with plain stores and tile_gather_kernel sums
+// every node's contributions in a fixed order (bitwise reproducible meshes);
+// otherwise the regions are added to the mesh with atomics.
 template <typename T, int P>
 __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const float *__restrict__ sorted_w,
                                       float mass_const, const int *__restrict__ offset, int ntiles, int tpa, int n,
-                                      T *mesh, T *mesh_shifted, int color) {
+                                      T *mesh, T *mesh_shifted, float *__restrict__ region_out) {
     extern __shared__ int reg[];  // [2][kRegionCells]
     __shared__ int colc[kRegion * kRegion];
     __shared__ int wrap_t[3][kRegion];
@@ -465,14 +463,7 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
     __shared__ int s_cmax;
     const int nreg = mesh_shifted ? 2 : 1;
     const int lane = threadIdx.x & 31;
-    const int half = tpa / 2;
-    const int nwork = color < 0 ? ntiles : half * half * half;
-    for (int work = blockIdx.x; work < nwork; work += gridDim.x) {
-        int tile = work;
-        if (color >= 0) {
-            const int i = work / (half * half), j = (work / half) % half, k = work % half;
-            tile = ((2 * i + ((color >> 2) & 1)) * tpa + (2 * j + ((color >> 1) & 1))) * tpa + (2 * k + (color & 1));
-        }
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int p0 = offset[tile], p1 = offset[tile + 1];
         if (p0 == p1) continue;
         __syncthreads();
@@ -539,6 +530,14 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
             deposit_all(std::false_type{});
         __syncthreads();
         const double unscale = ldexp(1.0, -e);
+        if (region_out) {
+            float *dst = region_out + (size_t)tile * nreg * kRegionCells;
+            for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
+                const int word = reg[i];
+                dst[i] = fixed ? (float)((double)word * unscale) : __int_as_float(word);
+            }
+            continue;
+        }
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) {
             const int word = reg[i];
             if (word == 0) continue;
@@ -546,12 +545,48 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
             const int r = i % kRegionCells;
             const int rz = r % kRegion, ry = (r / kRegion) % kRegion, rx = r / (kRegion * kRegion);
             const size_t cell = ((size_t)wrap_t[0][rx] * n + wrap_t[1][ry]) * n + wrap_t[2][rz];
-            T *dst = (i < kRegionCells ? mesh : mesh_shifted) + cell;
-            if (color >= 0)
-                *dst += (T)v;
-            else
-                atomicAdd(dst, (T)v);
+            atomicAdd((i < kRegionCells ? mesh : mesh_shifted) + cell, (T)v);
         }
+    }
+}
+
+// Tiles whose region holds node coordinate x along one axis (n a multiple of
+// 16): the node's own tile at region index x % 16 + 1, the previous tile at
+// x % 16 + 17 when x % 16 <= 2, the next tile at 0 when x % 16 == 15.
+__device__ __forceinline__ int covering_tiles(int x, int tpa, int *t, int *ri) {
+    const int t0 = x / kTile, r0 = x % kTile + 1;
+    int k = 0;
+    if (r0 + kTile < kRegion) t[k] = (t0 + tpa - 1) % tpa, ri[k++] = r0 + kTile;
+    t[k] = t0, ri[k++] = r0;
+    if (r0 == kTile) t[k] = (t0 + 1) % tpa, ri[k++] = 0;
+    return k;
+}
+
+// mesh[node] += the node's contributions from every non-empty tile region
+// covering it, summed in a fixed order
+template <typename T>
+__global__ void tile_gather_kernel(const float *__restrict__ region, const int *__restrict__ offset, int tpa, int n,
+                                   int nreg, T *mesh, T *mesh_shifted) {
+    const int64_t cells = (int64_t)n * n * n;
+    const int64_t total = cells * nreg;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+        const int k = (int)(idx / cells);
+        const int64_t c = idx - k * cells;
+        const int z = (int)(c % n), y = (int)((c / n) % n), x = (int)(c / ((int64_t)n * n));
+        int tx[2], rx[2], ty[2], ry[2], tz[2], rz[2];
+        const int nx = covering_tiles(x, tpa, tx, rx), ny = covering_tiles(y, tpa, ty, ry),
+                  nz = covering_tiles(z, tpa, tz, rz);
+        float sum = 0.f;
+        for (int a = 0; a < nx; ++a)
+            for (int b = 0; b < ny; ++b)
+                for (int d = 0; d < nz; ++d) {
+                    const int tile = (tx[a] * tpa + ty[b]) * tpa + tz[d];
+                    if (offset[tile] == offset[tile + 1]) continue;  // empty tile: region never written
+                    sum += region[((size_t)tile * nreg + k) * kRegionCells + (rx[a] * kRegion + ry[b]) * kRegion + rz[d]];
+                }
+        T *m = k == 0 ? mesh : mesh_shifted;
+        m[c] += (T)sum;
     }
 }
 
@@ -586,7 +621,15 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
         float *rec_w = w ? reinterpret_cast<float *>(rec + np) : nullptr;
         const size_t smem = sizeof(int) * kRegionCells * (m2 ? 2 : 1);
         const int tblocks = (int)std::min<int64_t>(nt, (int64_t)ctx->num_sms * 8);
-        const int cblocks = (int)std::max<int64_t>(1, std::min<int64_t>(nt / 8, (int64_t)ctx->num_sms * 8));
+        // regions through a buffer and a fixed-order gather when the tiles
+        // cover the mesh exactly (n a multiple of 16), atomics otherwise
+        float *region = nullptr;
+        const int nreg = m2 ? 2 : 1;
+        if (n % kTile == 0) {
+            st = ensure_buffer(ctx, &ctx->aux, &ctx->aux_bytes, sizeof(float) * (size_t)nt * nreg * kRegionCells, s);
+            if (st) return st;
+            region = static_cast<float *>(ctx->aux);
+        }
         switch (window) {
 #define CNPC_TPR(P_)                                                                                          \
     case P_:                                                                                                  \
@@ -595,20 +638,19 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),    \
                         "tile paint smem");                                                                   \
         if (st) return st;                                                                                    \
-        if (tpa % 2 == 0 && n % kTile == 0) {                                                                 \
-            for (int color = 0; color < 8; ++color)                                                           \
-                tile_paint_rec_kernel<T, P_><<<cblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale,  \
-                                                                        offset, nt, tpa, n, m1, m2, color);   \
-        } else {                                                                                              \
-            tile_paint_rec_kernel<T, P_><<<tblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale, offset, \
-                                                                    nt, tpa, n, m1, m2, -1);                  \
-        }                                                                                                     \
+        tile_paint_rec_kernel<T, P_><<<tblocks, 256, smem, s>>>(rec, rec_w, (float)scale.mass_scale, offset, nt, \
+                                                                tpa, n, m1, m2, region);                      \
         break;
             CNPC_TPR(2) CNPC_TPR(3) CNPC_TPR(4)
 #undef CNPC_TPR
             default: return fail(ctx, CNPC_EINVAL, "window must be 1..4");
         }
-        return check_launch(ctx, "tile_paint_rec_kernel");
+        st = check_launch(ctx, "tile_paint_rec_kernel");
+        if (st || !region) return st;
+        const int64_t total = (int64_t)n * n * n * nreg;
+        const int gblocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
+        tile_gather_kernel<T><<<gblocks, 256, 0, s>>>(region, offset, tpa, n, nreg, m1, m2);
+        return check_launch(ctx, "tile_gather_kernel");
     }
     tile_scatter_kernel<<<pblocks, threads, 0, s>>>(pos, w, np, scale, tile_of, cursor, sorted);
     st = check_launch(ctx, "tile sort");
