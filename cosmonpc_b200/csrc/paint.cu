@@ -465,7 +465,12 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
     const int lane = threadIdx.x & 31;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int p0 = offset[tile], p1 = offset[tile + 1];
-        if (p0 == p1) continue;
+        if (p0 == p1) {
+            if (region_out)  // the gather reads every tile's region
+                for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x)
+                    region_out[(size_t)tile * nreg * kRegionCells + i] = 0.f;
+            continue;
+        }
         __syncthreads();
         for (int i = threadIdx.x; i < nreg * kRegionCells; i += blockDim.x) reg[i] = 0;
         for (int i = threadIdx.x; i < kRegion * kRegion; i += blockDim.x) colc[i] = 0;
@@ -550,49 +555,66 @@ __global__ void tile_paint_rec_kernel(const PaintRec *__restrict__ sorted, const
     }
 }
 
-// Tiles whose region holds node coordinate x along one axis (n a multiple of
-// 16): the node's own tile at region index x % 16 + 1, the previous tile at
-// x % 16 + 17 when x % 16 <= 2, the next tile at 0 when x % 16 == 15.
-__device__ __forceinline__ int covering_tiles(int x, int tpa, int *t, int *ri) {
-    const int t0 = x / kTile, r0 = x % kTile + 1;
+// The node at local coordinate l (0..15) of a tile along one axis lies in
+// the regions of (at most) the previous tile at region index l + 17 (when
+// l <= 2), the tile itself at l + 1, and the next tile at 0 (when l == 15);
+// dt = -1, 0, +1 in that fixed order.
+__device__ __forceinline__ int covering(int l, int *dt, int *ri) {
     int k = 0;
-    if (r0 + kTile < kRegion) t[k] = (t0 + tpa - 1) % tpa, ri[k++] = r0 + kTile;
-    t[k] = t0, ri[k++] = r0;
-    if (r0 == kTile) t[k] = (t0 + 1) % tpa, ri[k++] = 0;
+    if (l <= 2) dt[k] = -1, ri[k++] = l + kTile + 1;
+    dt[k] = 0, ri[k++] = l + 1;
+    if (l == kTile - 1) dt[k] = 1, ri[k++] = 0;
     return k;
 }
 
-// mesh[node] += the node's contributions from every non-empty tile region
-// covering it, summed in a fixed order
+// mesh[node] (+)= the node's contributions from every tile region covering
+// it (empty tiles have zero regions), summed in a fixed order: the node's own
+// x line of each covering (y, z) tile first, then the previous and the next
+// x tile.  One block per (tile core, grid); thread (ly, lz) holds the 16 nodes
+// of its x line, so the loads of the dominant term are independent.
 template <typename T>
-__global__ void tile_gather_kernel(const float *__restrict__ region, const int *__restrict__ offset, int tpa, int n,
-                                   int nreg, T *mesh, T *mesh_shifted) {
-    const int64_t cells = (int64_t)n * n * n;
-    const int64_t total = cells * nreg;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
-        const int k = (int)(idx / cells);
-        const int64_t c = idx - k * cells;
-        const int z = (int)(c % n), y = (int)((c / n) % n), x = (int)(c / ((int64_t)n * n));
-        int tx[2], rx[2], ty[2], ry[2], tz[2], rz[2];
-        const int nx = covering_tiles(x, tpa, tx, rx), ny = covering_tiles(y, tpa, ty, ry),
-                  nz = covering_tiles(z, tpa, tz, rz);
-        float sum = 0.f;
-        for (int a = 0; a < nx; ++a)
-            for (int b = 0; b < ny; ++b)
-                for (int d = 0; d < nz; ++d) {
-                    const int tile = (tx[a] * tpa + ty[b]) * tpa + tz[d];
-                    if (offset[tile] == offset[tile + 1]) continue;  // empty tile: region never written
-                    sum += region[((size_t)tile * nreg + k) * kRegionCells + (rx[a] * kRegion + ry[b]) * kRegion + rz[d]];
-                }
-        T *m = k == 0 ? mesh : mesh_shifted;
-        m[c] += (T)sum;
+__global__ void __launch_bounds__(256) tile_gather_kernel(const float *__restrict__ region, int tpa, int n, int nreg,
+                                                          int accumulate, T *mesh, T *mesh_shifted) {
+    const int ntiles = tpa * tpa * tpa;
+    const int ly = threadIdx.x >> 4, lz = threadIdx.x & 15;
+    int dy[2], ry[2], dz[2], rz[2];
+    const int ny = covering(ly, dy, ry), nz = covering(lz, dz, rz);
+    for (int w = blockIdx.x; w < ntiles * nreg; w += gridDim.x) {
+        const int k = w / ntiles, tile = w - k * ntiles;
+        const int tx = tile / (tpa * tpa), ty = (tile / tpa) % tpa, tz = tile % tpa;
+        auto base = [&](int cx, int b, int d) {
+            const int t = (cx * tpa + (ty + dy[b] + tpa) % tpa) * tpa + (tz + dz[d] + tpa) % tpa;
+            return region + ((size_t)t * nreg + k) * kRegionCells + ry[b] * kRegion + rz[d];
+        };
+        float acc[kTile];
+#pragma unroll
+        for (int lx = 0; lx < kTile; ++lx) acc[lx] = 0.f;
+        for (int b = 0; b < ny; ++b)
+            for (int d = 0; d < nz; ++d) {
+                const float *r = base(tx, b, d);
+#pragma unroll
+                for (int lx = 0; lx < kTile; ++lx) acc[lx] += __ldg(r + (lx + 1) * kRegion * kRegion);
+            }
+        const int px = tx == 0 ? tpa - 1 : tx - 1, nxt = tx + 1 == tpa ? 0 : tx + 1;
+        for (int b = 0; b < ny; ++b)
+            for (int d = 0; d < nz; ++d) {
+                const float *r = base(px, b, d);
+#pragma unroll
+                for (int lx = 0; lx < 3; ++lx) acc[lx] += __ldg(r + (lx + kTile + 1) * kRegion * kRegion);
+                acc[kTile - 1] += __ldg(base(nxt, b, d));
+            }
+        T *m = (k == 0 ? mesh : mesh_shifted) + ((size_t)(tx * kTile) * n + (ty * kTile + ly)) * n + (tz * kTile + lz);
+#pragma unroll
+        for (int lx = 0; lx < kTile; ++lx) {
+            T *dst = m + (size_t)lx * n * n;
+            *dst = accumulate ? *dst + (T)acc[lx] : (T)acc[lx];
+        }
     }
 }
 
 template <typename T>
 static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64_t np, int n, const Frame &scale,
-                        int window, T *m1, T *m2, cudaStream_t s) {
+                        int window, T *m1, T *m2, int accumulate, cudaStream_t s) {
     const int tpa = (n + kTile - 1) / kTile;
     const int nt = tpa * tpa * tpa;
     const size_t off_counts = 0, off_offset = off_counts + sizeof(int) * nt,
@@ -647,9 +669,8 @@ static int launch_tiled(cnpc_ctx *ctx, const double *pos, const double *w, int64
         }
         st = check_launch(ctx, "tile_paint_rec_kernel");
         if (st || !region) return st;
-        const int64_t total = (int64_t)n * n * n * nreg;
-        const int gblocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16);
-        tile_gather_kernel<T><<<gblocks, 256, 0, s>>>(region, offset, tpa, n, nreg, m1, m2);
+        const int gblocks = (int)std::min<int64_t>((int64_t)nt * nreg, (int64_t)ctx->num_sms * 8);
+        tile_gather_kernel<T><<<gblocks, 256, 0, s>>>(region, tpa, n, nreg, accumulate, m1, m2);
         return check_launch(ctx, "tile_gather_kernel");
     }
     tile_scatter_kernel<<<pblocks, threads, 0, s>>>(pos, w, np, scale, tile_of, cursor, sorted);
@@ -693,7 +714,11 @@ extern "C" int cnpc_paint_ex(cnpc_ctx *ctx, int dtype, const double *d_pos, cons
     const size_t cells = (size_t)n * n * n;
     const size_t esz = dtype == CNPC_F32 ? sizeof(float) : sizeof(double);
     int st;
-    if (!accumulate) {
+    // the tiled FP32 paint of windows 2..4 on a multiple of 16 writes every node
+    // itself (fixed-order gather of the tile regions): no zeroing needed
+    const bool tiled = dtype == CNPC_F32 && n >= 2 * kTile && np >= 8 * (int64_t)n * n * n / 64;
+    const bool gathered = tiled && window >= 2 && n % kTile == 0;
+    if (!accumulate && !gathered) {
         st = check_cuda(ctx, cudaMemsetAsync(d_mesh, 0, cells * esz, s), "memset mesh");
         if (st) return st;
         if (d_mesh_shifted) {
@@ -710,11 +735,10 @@ extern "C" int cnpc_paint_ex(cnpc_ctx *ctx, int dtype, const double *d_pos, cons
     f.mass_scale = mass_scale;
     // the tiled deposit pays off once tiles hold many particles; its FP32
     // shared-memory region would round FP64 meshes, so FP64 stays per particle
-    const bool tiled = dtype == CNPC_F32 && n >= 2 * kTile && np >= 8 * (int64_t)n * n * n / 64;
     if (dtype == CNPC_F32) {
         if (tiled)
             return launch_tiled<float>(ctx, d_pos, d_weight, np, n, f, window, (float *)d_mesh,
-                                       (float *)d_mesh_shifted, s);
+                                       (float *)d_mesh_shifted, accumulate, s);
         return launch_paint<float>(ctx, d_pos, d_weight, np, n, f, window, (float *)d_mesh,
                                    (float *)d_mesh_shifted, s);
     }
