@@ -449,7 +449,167 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     }
 }
 
+// Pipelined y/z passes (n = 128): a persistent block walks the (x, y
+// parity, item) units of the call with two warp groups that run concurrently
+// on two shared buffers.  The y group (YW warps) fills B[j % 2] for unit j
+// while the z group (ZW warps) turns B[(j - 1) % 2] into field rows; named
+// barriers hand each buffer over (y: arrive "full", z: wait "full"; z: arrive
+// "empty", y: wait "empty" before refilling), so the block never waits for all
+// its warps at once and the twiddle tables are built once per block.  The
+// y pass is one team FFT per k_z column, the z pass two per row pair, so the
+// groups are sized to finish a unit together.  The arithmetic and the output
+// order of every value are those of shell_yz_kernel.  Timed with CUDA events
+// (shell_fields calls of 20 fields): 0.121 -> 0.100 ms at n = 128; at n = 256
+// (T = 8, YW = 4 and ZW = 8 or 12, one 133 KB double buffer per SM) it was
+// 0.57 -> 0.61 ms, so n = 256 keeps the one-block-per-unit kernel.
+template <int T> struct YZPipe {
+    static constexpr int YW = T == 8 ? 4 : 2, ZW = T == 8 ? 12 : 4;
+    static constexpr int THREADS = 32 * (YW + ZW);
+    static constexpr int M = 16 * T, N = 2 * M, H = M / 2, LD = H + 1;
+    static constexpr int YT = 32 * YW / T, ZT = 32 * ZW / T;  // teams per group
+    static constexpr int kEx = N;
+    static constexpr int kTwt = kEx + (YT + ZT) * Exch<T>::kStride;
+    static constexpr int kB = ((kTwt + team_twiddles<T>() + 1) / 2) * 2;
+    static constexpr int kTotal = kB + 2 * M * LD;  // float2
+};
+
+__device__ __forceinline__ void named_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+template <int T>
+__global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(const float2 *__restrict__ work,
+                                                                               int nitems, const YZOut O) {
+    using YP = YZPipe<T>;
+    constexpr int M = YP::M, N = YP::N, H = YP::H, LD = YP::LD, NT = YP::THREADS;
+    constexpr int Q = 16 / T;
+    constexpr int KC = (kKC < H) ? kKC : H;
+    extern __shared__ float4 smem4[];
+    float2 *tw = reinterpret_cast<float2 *>(smem4);
+    float2 *twt = tw + YP::kTwt;
+    float2 *Bbuf = tw + YP::kB;  // [2][M][LD]
+    fill_twiddles(tw, N);
+    __syncthreads();
+    fill_team_twiddles<T>(twt, tw);
+    __syncthreads();
+    const int nunits = N * 2 * nitems;
+    const int nj = blockIdx.x < nunits ? (nunits - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int warp = threadIdx.x >> 5;
+    const int team = threadIdx.x / T, t = threadIdx.x % T;
+    const unsigned mask = team_mask(T);
+    float2 *tex = tw + YP::kEx + team * Exch<T>::kStride;
+    if (warp < YP::YW) {
+        // ------------------------------------------------ y pass (producer)
+        for (int j = 0; j < nj; ++j) {
+            const int u = blockIdx.x + j * gridDim.x;
+            const int item = u % nitems, ry = (u / nitems) & 1, x = u / (2 * nitems);
+            const int b = j & 1;
+            if (j >= 2) named_sync(3 + b, NT);  // the z group has drained this buffer
+            float2 *Bh = Bbuf + b * M * LD;
+            const float2 *a = work + ((size_t)item * N + x) * M * H;
+            const int rmax = O.rmax[item], r2max = O.r2max[item];
+            const int K = rmax + 1 < H ? rmax + 1 : H;
+            for (int kz = team; kz < K; kz += YP::YT) {
+                const int kz0 = (kz / KC) * KC;
+                float2 u16[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) {
+                    const int slot = T * jj + t;
+                    float2 v = make_float2(0.f, 0.f);
+                    if (slot > 0 && tile_live(slot - H, kz0, r2max)) v = __ldg(a + (size_t)slot * H + kz);
+                    if (ry) v = cmul(v, tw[slot]);
+                    u16[jj] = v;
+                }
+                team_fft<T>(u16, t, tex, twt, mask);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+#pragma unroll
+                    for (int k2 = 0; k2 < T; ++k2) {
+                        const int m = team_out_index<T>(t, q, k2);
+                        Bh[m * LD + kz] = shift_phase(u16[q * T + k2], m, ry);
+                    }
+            }
+            named_arrive(1 + b, NT);
+        }
+    } else {
+        // ------------------------------------------------ z pass (consumer)
+        const int zteam = team - YP::YT;
+        for (int j = 0; j < nj; ++j) {
+            const int u = blockIdx.x + j * gridDim.x;
+            const int item = u % nitems, ry = (u / nitems) & 1, x = u / (2 * nitems);
+            const int b = j & 1;
+            named_sync(1 + b, NT);  // the y group has filled this buffer
+            const float2 *Bh = Bbuf + b * M * LD;
+            const int rmax = O.rmax[item];
+            const int K = rmax + 1 < H ? rmax + 1 : H;
+            float *fout = O.out[item] + (size_t)x * N * N;
+            for (int p0 = 0; p0 < M / 2; p0 += YP::ZT) {
+                // teams of one warp take pairs 4 apart (rows 8 LD float2 apart)
+                const int p = p0 + ((zteam & 3) * 4 + ((zteam >> 2) & 3) + 16 * (zteam >> 4));
+                if (p >= M / 2) continue;
+                const float2 *b1 = Bh + (2 * p) * LD, *b2 = b1 + LD;
+                float2 v[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) {
+                    const int slot = T * jj + t;
+                    const int kz = slot - H;
+                    const int ak = kz < 0 ? -kz : kz;
+                    float2 w = make_float2(0.f, 0.f);
+                    if (slot > 0 && ak < K) {
+                        const float2 c1 = b1[ak], c2 = b2[ak];
+                        if (kz > 0)
+                            w = make_float2(c1.x - c2.y, c1.y + c2.x);
+                        else if (kz < 0)
+                            w = make_float2(c1.x + c2.y, c2.x - c1.y);
+                        else
+                            w = make_float2(c1.x, c2.x);
+                    }
+                    v[jj] = w;
+                }
+                float2 res[2][16];
+#pragma unroll
+                for (int rz = 0; rz < 2; ++rz) {
+                    float2 u16[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) u16[jj] = rz ? cmul(v[jj], tw[T * jj + t]) : v[jj];
+                    team_fft<T>(u16, t, tex, twt, mask);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) res[rz][i] = u16[i];
+                }
+                float *row1 = fout + (size_t)(2 * (2 * p) + ry) * N;
+                float *row2 = fout + (size_t)(2 * (2 * p + 1) + ry) * N;
+#pragma unroll
+                for (int k2 = 0; k2 < T; ++k2) {
+                    float re[2 * Q], im[2 * Q];
+#pragma unroll
+                    for (int q = 0; q < Q; ++q)
+#pragma unroll
+                        for (int rz = 0; rz < 2; ++rz) {
+                            const int m = team_out_index<T>(t, q, k2);
+                            const float2 g = shift_phase(res[rz][q * T + k2], m, rz);
+                            re[2 * q + rz] = g.x;
+                            im[2 * q + rz] = g.y;
+                        }
+                    const int z0 = 2 * Q * t + 32 * k2;
+#pragma unroll
+                    for (int c = 0; c < 2 * Q; c += 4) {
+                        *reinterpret_cast<float4 *>(row1 + z0 + c) = make_float4(re[c], re[c + 1], re[c + 2], re[c + 3]);
+                        *reinterpret_cast<float4 *>(row2 + z0 + c) = make_float4(im[c], im[c + 1], im[c + 2], im[c + 3]);
+                    }
+                }
+            }
+            if (j + 2 < nj) named_arrive(3 + b, NT);  // the y group refills it for unit j + 2
+        }
+    }
+}
+
 // ------------------------------------------------------------ dispatch
+// the pipelined y/z kernel for n = 128 (false: one block per unit)
+constexpr bool kShellPipeline = true;
+
 template <int T> static size_t column_smem(int nedges) {
     const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
     return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride +
@@ -474,7 +634,22 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     if (st) return st;
     const int ni = items.n;
     shell_column_kernel<T><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, workA);
-    shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, O);
+    if constexpr (T == 4 && kShellPipeline) {
+        using YP = YZPipe<T>;
+        const size_t sp = sizeof(float2) * (size_t)YP::kTotal;
+        st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_pipe_kernel<T>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp),
+                        "shell smem");
+        if (st) return st;
+        int per_sm = 1;
+        st = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shell_yz_pipe_kernel<T>,
+                                                                           YP::THREADS, sp), "shell occupancy");
+        if (st) return st;
+        const int grid = std::min(N * 2 * ni, std::max(1, per_sm) * ctx->num_sms);
+        shell_yz_pipe_kernel<T><<<grid, YP::THREADS, sp, s>>>(workA, ni, O);
+    } else {
+        shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, O);
+    }
     return check_launch(ctx, "shell_fields kernels");
 }
 
