@@ -139,11 +139,10 @@ FUSED_SHELLS = True
 # FP32 Gram blocks on the tensor cores (cnpc_contract_gram_tc[_multi_g], TF32
 # pairs, A operand in tensor memory) instead of the CUDA-core FFMA kernel.
 # Off by default: at 256^3 with 40 x 20 outputs the tensor-core kernel takes
-# 3.26 ms against 0.85 ms for the FFMA kernel.  Its tensor pipe is 5.6 %
-# active; the CUDA-core operand preparation (G F products and hi/lo splits
-# for 128 TMEM lanes plus 48 B rows per cell, ~74 warp instructions per cell
-# at 0.36 IPC per scheduler) costs more issue slots than the FFMA contraction
-# itself (800 FMAs = 400 packed FFMA2 per cell for 40 x 20).
+# 1.15-1.19 ms against 0.84 ms for the FFMA kernel (CUDA events).  Its time does
+# not change with 20 rows instead of 40: the per-chunk hand-offs between its
+# producer, converter and MMA warps (an mbarrier wait costs ~240 cycles even on
+# a completed phase) bound it, not the copies or the MMAs.
 GRAM_TC = False
 
 # FP32 Gram blocks of several weight fields (the FFT S3 sums of several
