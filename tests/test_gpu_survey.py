@@ -1,10 +1,9 @@
 """Survey path on the GPU (through the C ABI) against the oracle and the
 reference's own golden vectors.
 
-Tolerances as for the box: FP64 to 1e-8 of each multipole's max |value|, FP32
-to 1e-5 (or 4x the single-precision FFT conditioning of a case, conftest.tol),
-mode counts bit for bit; stage checks against the oracle at FP64
-rounding level.
+Tolerances as for the box (conftest.tol): FP64 to 1e-8 of each multipole's
+max |value|, FP32 to 1e-5, mode counts bit for bit; stage checks against the
+oracle at FP64 rounding level.
 """
 import copy
 import os
