@@ -13,8 +13,11 @@ and the batch depth of the shell-field synthesis are made per shape class:
   band-limited kernels and the shell-spectra + cuFFT route both take a batch
   of fields per call; deeper batches fill the GPU better and cost one pass-1
   work array (fused) or one half spectrum (cuFFT) per field.  The candidates
-  that fit the budget are timed on a synthetic spectrum of the class (CUDA
-  events, best of a few repetitions) and the fastest per field wins.
+  whose batch (with a cuFFT workspace of about its size) stays within 10 % of
+  the device are timed on a synthetic spectrum of the class (CUDA events, best
+  of a few repetitions, on a context of their own that is destroyed after, so
+  the losing plans' workspaces are freed); a depth whose plan cannot be made is
+  skipped, and the fastest per field wins.
 
 Plans are keyed by (device name, n, precision, synthesis route) and kept in a
 JSON file (``$CNPC_TUNE_CACHE``, default ``~/.cache/cosmonpc_b200/plans.json``)
@@ -103,17 +106,37 @@ def _measure(n, boxsize, edges, precision, fused):
     """Time shell synthesis of 2 x max(candidates) fields at each batch depth."""
     import torch
 
-    from . import _lib, angular, engine
+    from . import _lib, engine
 
-    ctx = _lib.Context.get()
     code, rdt, cdt = engine.PRECISION[precision]
     dev = torch.device("cuda", torch.cuda.current_device())
+    # the candidates run on a context of their own, destroyed afterwards: the
+    # cuFFT plans of deep batches hold workspaces of several GB each (512^3)
+    ctx = _lib.Context(dev.index)
+    try:
+        with _lib.Context.scope(ctx):
+            return _measure_in(ctx, n, boxsize, edges, precision, fused, code, rdt, cdt, dev)
+    finally:
+        torch.cuda.synchronize()
+        ctx.close()
+        torch.cuda.empty_cache()
+
+
+def _measure_in(ctx, n, boxsize, edges, precision, fused, code, rdt, cdt, dev):
+    import torch
+
+    from . import _lib, engine
+
     esz = 4 if precision == "f32" else 8
     per_field = n ** 3 * esz
     per_batch_item = (n * (n // 2) * (n // 4) * 8) if fused else (n * n * (n // 2 + 1) * 2 * esz)
     free = engine.free_device_bytes()
     budget = int(free * 0.5)
-    cands = [b for b in CANDIDATES if b * (per_field + per_batch_item) <= budget]
+    # a call's batch (its spectra or work arrays, and a cuFFT workspace of about
+    # the same size) must fit beside the shell fields, which a data vector plans
+    # at 80 % of the free memory: at most 10 % of the device per batch
+    cap = 0.10 * torch.cuda.get_device_properties(dev).total_memory
+    cands = [b for b in CANDIDATES if b * (per_field + per_batch_item) <= budget and 2 * b * per_batch_item <= cap]
     if not cands:
         return {"fft_batch": 1, "ms_per_field": None, "timed": {}}
     nitems = 2 * max(cands)
@@ -129,23 +152,29 @@ def _measure(n, boxsize, edges, precision, fused):
             for i, b in enumerate(range(nitems))]
     timed = {}
     for b in cands:
-        sf = engine.ShellFields(n, boxsize, edges, precision, spec, None, capacity=nitems, fft_batch=b)
-        best = None
-        for rep in range(3):
-            sf.release_all()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            sf.ensure(keys)
-            e1.record()
+        sf = None
+        try:
+            sf = engine.ShellFields(n, boxsize, edges, precision, spec, None, capacity=nitems, fft_batch=b)
+            best = None
+            for rep in range(3):
+                sf.release_all()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                sf.ensure(keys)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                if rep > 0:  # the first repetition makes plans and workspaces
+                    best = ms if best is None else min(best, ms)
+            timed[str(b)] = best / nitems
+        except (_lib.CnpcError, MemoryError, torch.cuda.OutOfMemoryError):
+            # a depth whose cuFFT plan or workspace cannot be made is not a candidate
             torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            if rep > 0:  # the first repetition makes plans and workspaces
-                best = ms if best is None else min(best, ms)
-        timed[str(b)] = best / nitems
         del sf
     torch.cuda.empty_cache()
+    if not timed:
+        return {"fft_batch": 1, "ms_per_field": None, "timed": {}}
     win = min(timed, key=timed.get)
-    _ = angular  # harmonics are made by ShellFields itself
     return {"fft_batch": int(win), "ms_per_field": timed[win], "timed": timed}
 
 

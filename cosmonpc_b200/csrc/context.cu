@@ -66,21 +66,26 @@ static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long r
         *out = it->second;
         return CNPC_OK;
     }
+    // 64-bit plan sizes: a batch of 16 fields of 512^3 holds 2^31 elements,
+    // which the 32-bit cufftPlanMany rejects (CUFFT_INTERNAL_ERROR)
     cufftHandle h;
-    int dims[3] = {n, n, n};
-    int real_embed[3] = {n, n, n};
-    int spec_embed[3] = {n, n, n / 2 + 1};
+    cufftResult r = cufftCreate(&h);
+    if (r != CUFFT_SUCCESS) return fail(ctx, CNPC_ECUFFT, "cufftCreate failed with code " + std::to_string((int)r));
+    long long dims[3] = {n, n, n};
+    long long real_embed[3] = {n, n, n};
+    long long spec_embed[3] = {n, n, n / 2 + 1};
     const long long spec_dist = (long long)n * n * (n / 2 + 1);
     const bool forward = type == CUFFT_R2C || type == CUFFT_D2Z;
-    cufftResult r;
+    size_t work = 0;
     if (forward)
-        r = cufftPlanMany(&h, 3, dims, real_embed, 1, (int)real_dist, spec_embed, 1, (int)spec_dist, type, batch);
+        r = cufftMakePlanMany64(h, 3, dims, real_embed, 1, real_dist, spec_embed, 1, spec_dist, type, batch, &work);
     else
-        r = cufftPlanMany(&h, 3, dims, spec_embed, 1, (int)spec_dist, real_embed, 1, (int)real_dist, type, batch);
+        r = cufftMakePlanMany64(h, 3, dims, spec_embed, 1, spec_dist, real_embed, 1, real_dist, type, batch, &work);
     if (r != CUFFT_SUCCESS) {
+        cufftDestroy(h);
         if (r == CUFFT_ALLOC_FAILED)
-            return fail(ctx, CNPC_ENOMEM, "cufftPlanMany: allocation failed");
-        return fail(ctx, CNPC_ECUFFT, "cufftPlanMany failed with code " + std::to_string((int)r));
+            return fail(ctx, CNPC_ENOMEM, "cufftMakePlanMany64: allocation failed");
+        return fail(ctx, CNPC_ECUFFT, "cufftMakePlanMany64 failed with code " + std::to_string((int)r));
     }
     ctx->plans[key] = h;
     *out = h;
