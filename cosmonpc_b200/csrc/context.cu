@@ -59,36 +59,48 @@ int ensure_status(cnpc_ctx *ctx) {
     return CNPC_OK;
 }
 
-static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long real_dist, cufftHandle *out) {
+// The plan of (type, n, batch, real_dist), made on first use, with the shared
+// work area of the context grown to its needs and attached, and the stream set.
+static int get_plan(cnpc_ctx *ctx, cufftType type, int n, int batch, long long real_dist, cudaStream_t stream,
+                    cufftHandle *out) {
     auto key = std::make_tuple((int)type, n, batch, real_dist);
     auto it = ctx->plans.find(key);
-    if (it != ctx->plans.end()) {
-        *out = it->second;
-        return CNPC_OK;
+    if (it == ctx->plans.end()) {
+        // 64-bit plan sizes: a batch of 16 fields of 512^3 holds 2^31 elements,
+        // which the 32-bit cufftPlanMany rejects (CUFFT_INTERNAL_ERROR)
+        cufftHandle h;
+        cufftResult r = cufftCreate(&h);
+        if (r != CUFFT_SUCCESS)
+            return fail(ctx, CNPC_ECUFFT, "cufftCreate failed with code " + std::to_string((int)r));
+        r = cufftSetAutoAllocation(h, 0);
+        long long dims[3] = {n, n, n};
+        long long real_embed[3] = {n, n, n};
+        long long spec_embed[3] = {n, n, n / 2 + 1};
+        const long long spec_dist = (long long)n * n * (n / 2 + 1);
+        const bool forward = type == CUFFT_R2C || type == CUFFT_D2Z;
+        size_t work = 0;
+        if (r == CUFFT_SUCCESS) {
+            if (forward)
+                r = cufftMakePlanMany64(h, 3, dims, real_embed, 1, real_dist, spec_embed, 1, spec_dist, type, batch,
+                                        &work);
+            else
+                r = cufftMakePlanMany64(h, 3, dims, spec_embed, 1, spec_dist, real_embed, 1, real_dist, type, batch,
+                                        &work);
+        }
+        if (r != CUFFT_SUCCESS) {
+            cufftDestroy(h);
+            if (r == CUFFT_ALLOC_FAILED) return fail(ctx, CNPC_ENOMEM, "cufftMakePlanMany64: allocation failed");
+            return fail(ctx, CNPC_ECUFFT, "cufftMakePlanMany64 failed with code " + std::to_string((int)r));
+        }
+        it = ctx->plans.emplace(key, cnpc_ctx::FftPlan{h, work}).first;
     }
-    // 64-bit plan sizes: a batch of 16 fields of 512^3 holds 2^31 elements,
-    // which the 32-bit cufftPlanMany rejects (CUFFT_INTERNAL_ERROR)
-    cufftHandle h;
-    cufftResult r = cufftCreate(&h);
-    if (r != CUFFT_SUCCESS) return fail(ctx, CNPC_ECUFFT, "cufftCreate failed with code " + std::to_string((int)r));
-    long long dims[3] = {n, n, n};
-    long long real_embed[3] = {n, n, n};
-    long long spec_embed[3] = {n, n, n / 2 + 1};
-    const long long spec_dist = (long long)n * n * (n / 2 + 1);
-    const bool forward = type == CUFFT_R2C || type == CUFFT_D2Z;
-    size_t work = 0;
-    if (forward)
-        r = cufftMakePlanMany64(h, 3, dims, real_embed, 1, real_dist, spec_embed, 1, spec_dist, type, batch, &work);
-    else
-        r = cufftMakePlanMany64(h, 3, dims, spec_embed, 1, spec_dist, real_embed, 1, real_dist, type, batch, &work);
-    if (r != CUFFT_SUCCESS) {
-        cufftDestroy(h);
-        if (r == CUFFT_ALLOC_FAILED)
-            return fail(ctx, CNPC_ENOMEM, "cufftMakePlanMany64: allocation failed");
-        return fail(ctx, CNPC_ECUFFT, "cufftMakePlanMany64 failed with code " + std::to_string((int)r));
-    }
-    ctx->plans[key] = h;
-    *out = h;
+    const cnpc_ctx::FftPlan &p = it->second;
+    int st = ensure_buffer(ctx, &ctx->fft_ws, &ctx->fft_ws_bytes, p.work, stream);
+    if (st) return st;
+    cufftResult r = cufftSetWorkArea(p.h, ctx->fft_ws);
+    if (r == CUFFT_SUCCESS) r = cufftSetStream(p.h, stream);
+    if (r != CUFFT_SUCCESS) return fail(ctx, CNPC_ECUFFT, "cufft work area / stream: code " + std::to_string((int)r));
+    *out = p.h;
     return CNPC_OK;
 }
 
@@ -139,7 +151,8 @@ int cnpc_ctx_create(cnpc_ctx **ctx, int device) {
 
 int cnpc_ctx_destroy(cnpc_ctx *ctx) {
     if (!ctx) return CNPC_OK;
-    for (auto &kv : ctx->plans) cufftDestroy(kv.second);
+    for (auto &kv : ctx->plans) cufftDestroy(kv.second.h);
+    if (ctx->fft_ws) cudaFree(ctx->fft_ws);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->paint_ws) cudaFree(ctx->paint_ws);
     if (ctx->aux) cudaFree(ctx->aux);
@@ -186,9 +199,9 @@ int cnpc_fft_r2c(cnpc_ctx *ctx, int dtype, int n, int batch, const void *d_real,
     const long long cells = (long long)n * n * n;
     CNPC_REQUIRE(ctx, real_dist == 0 || real_dist >= cells, "real_dist must be 0 or >= n^3");
     CNPC_REQUIRE(ctx, real_dist < (1ll << 31), "real_dist too large");
-    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_R2C : CUFFT_D2Z, n, batch, real_dist ? real_dist : cells, &h);
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_R2C : CUFFT_D2Z, n, batch, real_dist ? real_dist : cells,
+                      (cudaStream_t)stream, &h);
     if (st) return st;
-    cufftSetStream(h, (cudaStream_t)stream);
     cufftResult r = dtype == CNPC_F32
                         ? cufftExecR2C(h, (cufftReal *)d_real, (cufftComplex *)d_spec)
                         : cufftExecD2Z(h, (cufftDoubleReal *)d_real, (cufftDoubleComplex *)d_spec);
@@ -206,9 +219,9 @@ int cnpc_fft_c2r(cnpc_ctx *ctx, int dtype, int n, int batch, void *d_spec, void 
     const long long cells = (long long)n * n * n;
     CNPC_REQUIRE(ctx, real_dist == 0 || real_dist >= cells, "real_dist must be 0 or >= n^3");
     CNPC_REQUIRE(ctx, real_dist < (1ll << 31), "real_dist too large");
-    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_C2R : CUFFT_Z2D, n, batch, real_dist ? real_dist : cells, &h);
+    int st = get_plan(ctx, dtype == CNPC_F32 ? CUFFT_C2R : CUFFT_Z2D, n, batch, real_dist ? real_dist : cells,
+                      (cudaStream_t)stream, &h);
     if (st) return st;
-    cufftSetStream(h, (cudaStream_t)stream);
     cufftResult r = dtype == CNPC_F32
                         ? cufftExecC2R(h, (cufftComplex *)d_spec, (cufftReal *)d_real)
                         : cufftExecZ2D(h, (cufftDoubleComplex *)d_spec, (cufftDoubleReal *)d_real);

@@ -285,11 +285,14 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 // shared-memory load of one row is either a broadcast or hits 8 distinct
 // banks.  Two adjacent cells are read per 8-byte load and accumulated with
 // packed FP32x2 FMAs (even and odd cell partial sums); the FP32 partials are
-// folded into FP64 registers after every chunk (32 cells per lane).
+// folded into this warp's FP64 partials (in L2) every kFfFold chunks.
 constexpr int kFfWarps = 8;
 constexpr int kFfChunk = 256;  // cells per block chunk (32 per warp)
 constexpr int kFfRow = 36;     // padded slab row (32 cells + 4)
-constexpr int kFfFold = 4;     // chunks per FP32 partial (128 cells per lane)
+// chunks per FP32 partial: 16 (512 cells per lane); each fold is a dependent
+// read-modify-write of the L2-resident FP64 partials, and folding every 4 / 8 /
+// 16 chunks took the 40 x 20 launch at 256^3 to 0.848 / 0.813 / 0.797 ms
+constexpr int kFfFold = 16;
 constexpr int kFfMaxRows = 80;  // staged rows: <= 4 weights + 48 A + 24 B
 constexpr int kFfTable = kFfMaxRows * 8;  // bytes of the row-source table ahead of the slabs
 

@@ -13,8 +13,17 @@
 struct cnpc_ctx {
     int device = 0;
     std::string last_error;
-    // cuFFT plans keyed by (type, n, batch, real-field distance)
-    std::map<std::tuple<int, int, int, long long>, cufftHandle> plans;
+    // cuFFT plans keyed by (type, n, batch, real-field distance), each with the
+    // work-area size it needs; the plans share one work area (fft_ws), set before
+    // every execution, so cached plans of several batch depths and precisions
+    // do not each hold a workspace of their own
+    struct FftPlan {
+        cufftHandle h;
+        size_t work;
+    };
+    std::map<std::tuple<int, int, int, long long>, FftPlan> plans;
+    void *fft_ws = nullptr;
+    size_t fft_ws_bytes = 0;
     // scratch for per-block partial sums of the x-space reductions
     void *scratch = nullptr;
     size_t scratch_bytes = 0;

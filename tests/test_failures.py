@@ -129,6 +129,38 @@ def test_timed_out_device_wait_reports_status_and_context_recovers():
 
 
 @pytest.mark.gpu
+def test_tensor_core_gram_timed_out_wait_reports_status():
+    """The tcgen05 Gram's waits given a limit of zero polls: every role gives
+    up at its first wait (the producer drains the copies it issued, no MMA is
+    issued, TMEM is freed), the outputs are NaN, the status word reports the
+    timeout, and the next call with the normal limit is correct."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    ctx = _lib.Context(torch.cuda.current_device())
+    try:
+        ncell, na, nb = 64 ** 3, 12, 8
+        g = torch.randn(ncell, dtype=torch.float32, device="cuda")
+        f = torch.randn((na, ncell), dtype=torch.float32, device="cuda")
+        a, b = list(range(na)), list(range(nb))
+        out = torch.zeros((na, nb), dtype=torch.float64, device="cuda")
+        ctx.set_wait_limit(0)
+        ctx.gram_tc(ncell, g, f, ncell, a, b, out)
+        with pytest.raises(_lib.DeviceTimeout):
+            ctx.take_status()
+        assert torch.isnan(out).all()
+        ctx.set_wait_limit(1 << 22)
+        ctx.gram_tc(ncell, g, f, ncell, a, b, out)
+        ctx.take_status()
+        fd, gd = f.double(), g.double()
+        ref = (gd * fd[a]) @ fd[b].T
+        scale = (gd.abs() * fd[a].abs()) @ fd[b].abs().T
+        assert ((out - ref).abs() / scale).max().item() < 2e-6
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
 def test_timed_out_wait_surfaces_from_the_estimator():
     """A full FP64 data vector whose contraction waits time out raises
     DeviceTimeout when its results are read, instead of returning NaN."""

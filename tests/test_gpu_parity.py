@@ -222,6 +222,33 @@ def test_pair_contraction_matches_fp64_sums(dtype, n):
     assert err < (1e-14 if dtype == "f64" else 1e-6), err
 
 
+@pytest.mark.parametrize("ncell,na,nb,shared", [(128 ** 3, 40, 20, True), (256 ** 3, 40, 20, True),
+                                                (64 ** 3 + 100, 17, 9, False), (4096 + 36, 3, 2, False)])
+def test_ffma_gram_matches_fp64(ncell, na, nb, shared):
+    """cnpc_contract_gram in FP32 (CUDA-core FFMA kernel: FP32 partials over
+    512 cells per lane, folded into FP64) against FP64 sums of the same FP32
+    inputs, relative to sum |G F_a F_b|; at 256^3 every warp folds many
+    times."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    rng = np.random.default_rng(ncell + 7 * na + nb)
+    nf = na if shared else na + nb
+    stride = (ncell + 3) // 4 * 4
+    f = torch.from_numpy(rng.standard_normal((nf, stride)).astype(np.float32)).cuda()
+    g = torch.from_numpy(rng.standard_normal(ncell).astype(np.float32)).cuda()
+    a = list(range(na))
+    b = list(range(nb)) if shared else list(range(na, na + nb))
+    ctx = _lib.Context.get()
+    out = torch.empty((na, nb), dtype=torch.float64, device="cuda")
+    ctx.gram(_lib.F32, ncell, g, f, stride, a, b, out)
+    fd, gd = f[:, :ncell].double(), g.double()
+    ref = (gd * fd[a]) @ fd[b].T
+    scale = (gd.abs() * fd[a].abs()) @ fd[b].abs().T
+    err = ((out - ref).abs() / scale).max().item()
+    assert err < 1e-6, err
+
+
 @pytest.mark.parametrize("ncell,na,nb,shared", [(4096 + 36, 1, 1, False), (32 ** 3, 8, 8, True),
                                                 (64 ** 3, 40, 20, True), (64 ** 3, 40, 24, False),
                                                 (48 ** 3, 24, 20, False), (64 ** 3 + 100, 17, 9, False),
