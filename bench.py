@@ -60,7 +60,13 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    The sampler is started before the region (``start`` + ``wait_first``,
+    since nvidia-smi takes a while to print its first sample) and every line
+    is time-stamped; ``summary`` keeps the samples between ``mark_start`` and
+    ``mark_stop``, plus the first one after the stop, so that a region of a
+    few tens of ms still has samples taken under load."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -69,9 +75,10 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (monotonic time, line)
+        self.t0 = self.t1 = None
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
@@ -82,11 +89,26 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def wait_first(self, timeout=5.0):
+        t_end = time.monotonic() + timeout
+        while self.proc is not None and not self.lines and time.monotonic() < t_end:
+            time.sleep(0.01)
+
+    def mark_start(self):
+        self.t0 = time.monotonic()
+
+    def mark_stop(self):
+        self.t1 = time.monotonic()
+        # the first sample after the stop belongs to the region's last 50 ms
+        t_end = self.t1 + 0.5
+        while self.proc is not None and time.monotonic() < t_end and not any(t > self.t1 for t, _ in self.lines):
+            time.sleep(0.01)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
-    def __exit__(self, *a):
+    def stop(self):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -94,10 +116,17 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
+    def _window(self):
+        if self.t0 is None or self.t1 is None:
+            return [ln for _, ln in self.lines]
+        inside = [ln for t, ln in self.lines if self.t0 <= t <= self.t1]
+        after = [ln for t, ln in self.lines if t > self.t1][:1]
+        return inside + after
+
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self._window():
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -117,7 +146,7 @@ class ClockSampler:
                 except Exception:
                     pass
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"],
-                    "note": (self.lines[:2], err)}
+                    "note": ([ln for _, ln in self.lines[:2]], err)}
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
@@ -477,18 +506,24 @@ def main():
 
     # warm-up in the timed form (two data vectors in flight), so that no
     # allocation of the pipelined run falls inside the timed region
+    clk = ClockSampler(local).start()
     run_vectors(args.warmup, pos_dev)
+    clk.wait_first()
     barrier()
     # ---- timed region (device resident inputs)
     launches0 = _lib.launch_count
-    with ClockSampler(local) as clk:
+    try:
         barrier()
+        clk.mark_start()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record()
         res_fast = run_vectors(args.steps, pos_dev)
         ev1.record()
         barrier()
+        clk.mark_stop()
+    finally:
+        clk.stop()
     t_fast = ev0.elapsed_time(ev1) / 1000.0
     launches = (_lib.launch_count - launches0) // args.steps
     t_fast = max_over_ranks(t_fast)

@@ -335,12 +335,50 @@ template <int T> struct YZLayout {
 };
 
 // Output fields and band limits of the items, passed by value (no host-to-device
-// table copy, so a call can be captured in a CUDA graph).
+// table copy, so a call can be captured in a CUDA graph).  rmax carries the
+// item's mirror code in its bits 16+ (yz_mirror).
 struct YZOut {
     float *out[CNPC_MAX_ITEMS];
     int rmax[CNPC_MAX_ITEMS];
     int r2max[CNPC_MAX_ITEMS];
 };
+
+// A shell of the unit spectrum (source 2) is conj(Y_lm) times a shell mask:
+// S(-k) = (-1)^l S(k), so its field has the parity F(-x) = (-1)^l F(x) on the
+// grid.  The y/z passes then compute only the planes x <= N/2 and write plane
+// N - x as the reflection of plane x (y -> -y, z -> -z mod N, times the sign).
+// Code 0: no mirror (data spectra), 1: even (sign +1), 2: odd (sign -1).
+__device__ __forceinline__ int yz_rmax(const YZOut &O, int item) { return O.rmax[item] & 0xFFFF; }
+__device__ __forceinline__ int yz_mirror(const YZOut &O, int item) { return O.rmax[item] >> 16; }
+
+// Reflected copy of a row with 16-byte stores.  Thread t of a team holds the
+// run r(z0 .. z0 + Q2 - 1) of a row, z0 = Q2 t + 32 k2 (Q2 T = 32).  Element z
+// goes to (N - z) mod N of the mirror row, so the aligned run at N - z0 - Q2
+// is {r(z0 + Q2), r(z0 + Q2 - 1), ..., r(z0 + 1)}: the first value of the next
+// run (team lane t + 1 at this k2; for the last lane, lane 0 at k2 + 1, which
+// the caller's loop over k2 downwards passes in `carry`) and this run
+// reversed.  The run that would need r(N) = r(0) (last lane, k2 = T - 1)
+// leaves mirror position 0, which is r(0) itself, to lane 0 after the loop.
+template <int T, int Q2>
+__device__ __forceinline__ void store_reflected(float *row, int t, int k2, const float *v, float &carry, float sgn,
+                                                unsigned mask, int N) {
+    float nxt = __shfl_down_sync(mask, v[0], 1, T);
+    if (t == T - 1) nxt = carry;
+    carry = __shfl_sync(mask, v[0], 0, T);
+    const int base = N - (Q2 * t + 32 * k2) - Q2;  // a multiple of 4
+    float m[Q2];
+    m[0] = sgn * nxt;
+#pragma unroll
+    for (int c = 1; c < Q2; ++c) m[c] = sgn * v[Q2 - c];
+    if (t == T - 1 && k2 == T - 1) {
+#pragma unroll
+        for (int c = 1; c < Q2; ++c) row[base + c] = m[c];
+    } else {
+#pragma unroll
+        for (int c = 0; c < Q2; c += 4)
+            *reinterpret_cast<float4 *>(row + base + c) = make_float4(m[c], m[c + 1], m[c + 2], m[c + 3]);
+    }
+}
 
 template <int T>
 __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work, int nitems,
@@ -354,6 +392,10 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     const int item = blockIdx.x % nitems;
     const int ry = (blockIdx.x / nitems) & 1;
     const int x = blockIdx.x / (2 * nitems);
+    const int mcode = yz_mirror(O, item);
+    if (mcode && x > N / 2) return;  // written by the block of plane N - x
+    const bool mirror = mcode && x > 0 && x < N / 2;
+    const float msign = mcode == 2 ? -1.f : 1.f;
     float2 *twt = tw + YL::kTwt;
     fill_twiddles(tw, N);
     __syncthreads();
@@ -363,7 +405,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     const unsigned mask = team_mask(T);
     float2 *tex = tw + YL::kEx + team * Exch<T>::kStride;
     const float2 *a = work + ((size_t)item * N + x) * M * H;  // A[x][slot][kz]
-    const int rmax = O.rmax[item], r2max = O.r2max[item];
+    const int rmax = yz_rmax(O, item), r2max = O.r2max[item];
     const int K = rmax + 1 < H ? rmax + 1 : H;  // columns k_z >= K are zero
     constexpr int KC = (kKC < H) ? kKC : H;
     // y: one team per k_z column
@@ -389,6 +431,7 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     }
     __syncthreads();
     float *fout = O.out[item] + (size_t)x * N * N;
+    float *fmir = O.out[item] + (size_t)(N - x) * N * N;  // used when mirror
     // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity.  Teams of one warp
     // take pairs 4 apart, so their rows sit 8 * LD float2 (16 banks) apart.
     for (int p0 = 0; p0 < M / 2; p0 += TEAMS) {
@@ -425,10 +468,14 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
 #pragma unroll
             for (int i = 0; i < 16; ++i) res[rz][i] = u[i];
         }
-        float *row1 = fout + (size_t)(2 * (2 * p) + ry) * N;      // y = 2 m1 + ry
-        float *row2 = fout + (size_t)(2 * (2 * p + 1) + ry) * N;  // y = 2 m2 + ry
+        const int y1 = 2 * (2 * p) + ry, y2 = 2 * (2 * p + 1) + ry;  // y = 2 m + ry
+        float *row1 = fout + (size_t)y1 * N;
+        float *row2 = fout + (size_t)y2 * N;
+        float *mrow1 = fmir + (size_t)((N - y1) & (N - 1)) * N;
+        float *mrow2 = fmir + (size_t)((N - y2) & (N - 1)) * N;
+        float carry1 = 0.f, carry2 = 0.f;  // the reflection needs the next (higher) k2's first values
 #pragma unroll
-        for (int k2 = 0; k2 < T; ++k2) {
+        for (int k2 = T - 1; k2 >= 0; --k2) {
             float re[2 * Q], im[2 * Q];
 #pragma unroll
             for (int q = 0; q < Q; ++q)
@@ -444,6 +491,14 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             for (int c = 0; c < 2 * Q; c += 4) {
                 *reinterpret_cast<float4 *>(row1 + z0 + c) = make_float4(re[c], re[c + 1], re[c + 2], re[c + 3]);
                 *reinterpret_cast<float4 *>(row2 + z0 + c) = make_float4(im[c], im[c + 1], im[c + 2], im[c + 3]);
+            }
+            if (mirror) {
+                store_reflected<T, 2 * Q>(mrow1, t, k2, re, carry1, msign, mask, N);
+                store_reflected<T, 2 * Q>(mrow2, t, k2, im, carry2, msign, mask, N);
+                if (k2 == 0 && t == 0) {  // mirror position 0 is r(0) itself
+                    mrow1[0] = msign * re[0];
+                    mrow2[0] = msign * im[0];
+                }
             }
         }
     }
@@ -510,8 +565,11 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
             if (j >= 2) named_sync(3 + b, NT);  // the z group has drained this buffer
             float2 *Bh = Bbuf + b * M * LD;
             const float2 *a = work + ((size_t)item * N + x) * M * H;
-            const int rmax = O.rmax[item], r2max = O.r2max[item];
-            const int K = rmax + 1 < H ? rmax + 1 : H;
+            const int rmax = yz_rmax(O, item), r2max = O.r2max[item];
+            // a mirrored item's planes x > N/2 are written by plane N - x: the
+            // unit keeps its barrier steps and does no work
+            const bool skip = yz_mirror(O, item) && x > N / 2;
+            const int K = skip ? 0 : (rmax + 1 < H ? rmax + 1 : H);
             for (int kz = team; kz < K; kz += YP::YT) {
                 const int kz0 = (kz / KC) * KC;
                 float2 u16[16];
@@ -543,10 +601,15 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
             const int b = j & 1;
             named_sync(1 + b, NT);  // the y group has filled this buffer
             const float2 *Bh = Bbuf + b * M * LD;
-            const int rmax = O.rmax[item];
+            const int rmax = yz_rmax(O, item);
             const int K = rmax + 1 < H ? rmax + 1 : H;
+            const int mcode = yz_mirror(O, item);
+            const bool skip = mcode && x > N / 2;  // same test as the y group
+            const bool mirror = mcode && x > 0 && x < N / 2;
+            const float msign = mcode == 2 ? -1.f : 1.f;
             float *fout = O.out[item] + (size_t)x * N * N;
-            for (int p0 = 0; p0 < M / 2; p0 += YP::ZT) {
+            float *fmir = O.out[item] + (size_t)(N - x) * N * N;
+            for (int p0 = 0; p0 < (skip ? 0 : M / 2); p0 += YP::ZT) {
                 // teams of one warp take pairs 4 apart (rows 8 LD float2 apart)
                 const int p = p0 + ((zteam & 3) * 4 + ((zteam >> 2) & 3) + 16 * (zteam >> 4));
                 if (p >= M / 2) continue;
@@ -579,10 +642,14 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
 #pragma unroll
                     for (int i = 0; i < 16; ++i) res[rz][i] = u16[i];
                 }
-                float *row1 = fout + (size_t)(2 * (2 * p) + ry) * N;
-                float *row2 = fout + (size_t)(2 * (2 * p + 1) + ry) * N;
+                const int y1 = 2 * (2 * p) + ry, y2 = 2 * (2 * p + 1) + ry;
+                float *row1 = fout + (size_t)y1 * N;
+                float *row2 = fout + (size_t)y2 * N;
+                float *mrow1 = fmir + (size_t)((N - y1) & (N - 1)) * N;
+                float *mrow2 = fmir + (size_t)((N - y2) & (N - 1)) * N;
+                float carry1 = 0.f, carry2 = 0.f;
 #pragma unroll
-                for (int k2 = 0; k2 < T; ++k2) {
+                for (int k2 = T - 1; k2 >= 0; --k2) {
                     float re[2 * Q], im[2 * Q];
 #pragma unroll
                     for (int q = 0; q < Q; ++q)
@@ -599,6 +666,14 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
                         *reinterpret_cast<float4 *>(row1 + z0 + c) = make_float4(re[c], re[c + 1], re[c + 2], re[c + 3]);
                         *reinterpret_cast<float4 *>(row2 + z0 + c) = make_float4(im[c], im[c + 1], im[c + 2], im[c + 3]);
                     }
+                    if (mirror) {
+                        store_reflected<T, 2 * Q>(mrow1, t, k2, re, carry1, msign, mask, N);
+                        store_reflected<T, 2 * Q>(mrow2, t, k2, im, carry2, msign, mask, N);
+                        if (k2 == 0 && t == 0) {
+                            mrow1[0] = msign * re[0];
+                            mrow2[0] = msign * im[0];
+                        }
+                    }
                 }
             }
             if (j + 2 < nj) named_arrive(3 + b, NT);  // the y group refills it for unit j + 2
@@ -609,6 +684,8 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
 // ------------------------------------------------------------ dispatch
 // the pipelined y/z kernel for n = 128 (false: one block per unit)
 constexpr bool kShellPipeline = true;
+// unit-spectrum shells: planes x > N/2 written as reflections (yz_mirror)
+constexpr bool kMirrorUnitShells = true;
 
 template <int T> static size_t column_smem(int nedges) {
     const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
@@ -708,7 +785,9 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
     std::memset(&O, 0, sizeof(O));
     for (int j = 0; j < nitems; ++j) {
         O.out[j] = static_cast<float *>(h_out_fields[j]);
-        O.rmax[j] = items.rmax[j];
+        // unit-spectrum shells have the parity (-1)^l: mirror code in bits 16+
+        const int mcode = kMirrorUnitShells && items.it[j].source == 2 ? ((ht.h[items.it[j].harmonic].l & 1) ? 2 : 1) : 0;
+        O.rmax[j] = items.rmax[j] | (mcode << 16);
         O.r2max[j] = items.r2max[j];
     }
     const float2 *A = static_cast<const float2 *>(d_spec_a);

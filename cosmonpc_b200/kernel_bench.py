@@ -32,9 +32,10 @@ def _time(fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def shells(n, items, reps, boxsize=None):
+def shells(n, items, reps, boxsize=None, source=0):
     """cnpc_shell_fields: `items` FP32 shell fields (l = 0 and l = 2, 20 bins
-    up to k_Nyquist / 2) of one source spectrum."""
+    up to k_Nyquist / 2) of one source spectrum (source 0) or of the unit
+    spectrum (source 2, the FFT S3 shells)."""
     ctx = _lib.Context.get()
     L = boxsize or 2000.0 * n / 256
     kf = 2 * np.pi / L
@@ -45,7 +46,7 @@ def shells(n, items, reps, boxsize=None):
     ctx.r2c(_lib.F32, n, 1, real, spec)
     del real
     harms = [angular.harmonic(0, 0), angular.harmonic(2, 0)]
-    its = [_lib.ShellItem(j % 20, (j // 20) % 2, 0, 0, 0) for j in range(items)]
+    its = [_lib.ShellItem(j % 20, (j // 20) % 2, 0, source, 1 if source == 2 else 0) for j in range(items)]
     out = torch.empty((items, n, n, n), dtype=torch.float32, device="cuda")
     ms = _time(lambda: ctx.shell_fields(n, L, spec, None, edges, harms, its, [out[j] for j in range(items)]), reps)
     band = n * (n // 2) * (n // 4) * 8
@@ -94,10 +95,11 @@ def main(argv=None):
     ap.add_argument("--window", type=int, default=4)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--tc", action="store_true", help="gram: the tensor-core kernel")
+    ap.add_argument("--source", type=int, default=0, choices=[0, 2], help="shells: 0 data spectrum, 2 unit spectrum")
     args = ap.parse_args(argv)
     build.build()
     if args.what == "shells":
-        r = shells(args.n, args.items, args.reps)
+        r = shells(args.n, args.items, args.reps, source=args.source)
     elif args.what == "gram":
         r = gram(args.n, args.rows, args.cols, args.reps, args.tc)
     else:
