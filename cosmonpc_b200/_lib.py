@@ -28,6 +28,7 @@ EXPORTED = (
     "cnpc_contract_gram", "cnpc_contract_gram_noalloc", "cnpc_paint_ex", "cnpc_catalog_decode",
     "cnpc_particle_sums", "cnpc_catalog_weights", "cnpc_interlace_split", "cnpc_xspace_harmonic",
     "cnpc_survey_bins", "cnpc_survey_source", "cnpc_field_product_sum", "cnpc_field_axpby",
+    "cnpc_field_parity_fold",
     "cnpc_survey_hermitian_accumulate", "cnpc_shell_fields", "cnpc_contract_pairs",
     "cnpc_contract_gram_tc", "cnpc_contract_gram_multi_g", "cnpc_sn_bins_multi",
     "cnpc_forward_finish_band", "cnpc_ctx_set_wait_limit", "cnpc_ctx_take_status",
@@ -133,6 +134,7 @@ _SIGS = {
                            _d, _vp, _vp, _vp],
     "cnpc_field_product_sum": [_vp, _i, _i64, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _vp],
     "cnpc_field_axpby": [_vp, _i, _i64, _d, _vp, _d, _vp, _vp, _vp],
+    "cnpc_field_parity_fold": [_vp, _i, _i, _vp, _i, _vp, _vp],
     "cnpc_survey_hermitian_accumulate": [_vp, _i, _i, _d, _i, ctypes.POINTER(Operand),
                                          ctypes.POINTER(Harmonic), _d, _vp, _vp],
     "cnpc_shell_fields": [_vp, _i, _d, _vp, _vp, _dp, _i, ctypes.POINTER(Harmonic), _i,
@@ -190,7 +192,7 @@ KERNELS_PER_CALL = {"paint": 1, "forward_finish": 1, "kbin_counts": 1, "pk_bins"
                     "survey_source": 1, "field_product_sum": 2, "field_axpby": 1,
                     "hermitian_accumulate": 1, "shell_fields": 2, "contract_pairs": 3,
                     "gram_tc": 2, "gram_multi_g": 2, "sn_bins_multi": 1, "forward_finish_band": 1,
-                    "box_catalog": 1}
+                    "box_catalog": 1, "field_parity_fold": 1}
 launch_count = 0
 
 
@@ -622,6 +624,13 @@ class Context:
         st = self.lib.cnpc_field_product_sum(self.h, dtype, ncell, nf, ra, ia, _ptr(out), self.stream())
         self._check(st, "cnpc_field_product_sum")
         _count("field_product_sum")
+
+    def field_parity_fold(self, dtype, n, src, sign, out):
+        """out[(n/2 + 1) n^2] = the parity fold of ``src`` (n^3) with ``sign``
+        (cnpc_field_parity_fold)."""
+        st = self.lib.cnpc_field_parity_fold(self.h, dtype, n, _ptr(src), int(sign), _ptr(out), self.stream())
+        self._check(st, "cnpc_field_parity_fold")
+        _count("field_parity_fold")
 
     def field_axpby(self, dtype, ncell, a, x, b, y, out):
         st = self.lib.cnpc_field_axpby(self.h, dtype, ncell, float(a), _ptr(x), float(b), _ptr(y), _ptr(out),

@@ -18,6 +18,7 @@
 // The n/2-point FFT is done by a team of T = n/32 threads holding 16 values
 // each: a 16-point DFT in registers, twiddles, one shared-memory exchange and
 // T-point DFTs.  Twiddles come from an FP64-computed table rounded to FP32.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -198,6 +199,9 @@ __device__ __forceinline__ bool tile_live(int ny, int kz0, int r2max) { return n
 // Work layout per item: A[x][s][n_z] (pass 1 output, s = n_y + n/4) and
 // B[x][y][n_z] (pass 2 output); n_z < n/4 throughout.
 constexpr int kColThreads = 128;   // 16 teams of 8 (n = 256)
+// unit-spectrum shells: planes x > N/2 written as reflections by the y/z
+// passes (yz_mirror), so pass 1 does not store them
+constexpr bool kMirrorUnitShells = true;
 constexpr int kKC = 16;            // n_z columns per block in passes 1 and 2
 
 __device__ __forceinline__ void fill_twiddles(float2 *tw, int N) {
@@ -307,10 +311,11 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
             }
     }
     __syncthreads();
-    // A[x][s][kz]
+    // A[x][s][kz]; a unit-spectrum item's planes x > N/2 are never read
     float2 *d = dst + (size_t)item * N * M * H + (size_t)(row + 1) * H + kz0;
     const size_t stride = (size_t)M * H;
-    for (int e = threadIdx.x; e < N * KC; e += blockDim.x) {
+    const int np = (kMirrorUnitShells && items.it[item].source == 2) ? N / 2 + 1 : N;
+    for (int e = threadIdx.x; e < np * KC; e += blockDim.x) {
         const int p = e / KC, c = e % KC;
         d[p * stride + c] = out[p * LDC + c];
     }
@@ -684,8 +689,6 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
 // ------------------------------------------------------------ dispatch
 // the pipelined y/z kernel for n = 128 (false: one block per unit)
 constexpr bool kShellPipeline = true;
-// unit-spectrum shells: planes x > N/2 written as reflections (yz_mirror)
-constexpr bool kMirrorUnitShells = true;
 
 template <int T> static size_t column_smem(int nedges) {
     const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
@@ -730,9 +733,44 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
     return check_launch(ctx, "shell_fields kernels");
 }
 
+// out[x][y][z] for the planes x = 0 .. n/2: in[x][y][z] on the planes 0 and
+// n/2, in[x][y][z] + sign in[n - x][-y][-z] (indices mod n) on the others.
+template <typename T>
+__global__ void parity_fold_kernel(const T *__restrict__ in, T *__restrict__ out, int n, T sign) {
+    const int64_t nn = (int64_t)n * n;
+    const int64_t total = (int64_t)(n / 2 + 1) * nn;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i / nn);
+        const int y = (int)((i / n) % n), z = (int)(i % n);
+        T v = in[i];
+        if (x > 0 && x < n / 2) {
+            const int yr = y == 0 ? 0 : n - y, zr = z == 0 ? 0 : n - z;
+            v += sign * in[((int64_t)(n - x) * n + yr) * n + zr];
+        }
+        out[i] = v;
+    }
+}
+
 }  // namespace cnpc
 
 using namespace cnpc;
+
+extern "C" int cnpc_field_parity_fold(cnpc_ctx *ctx, int dtype, int n, const void *d_in, int sign, void *d_out,
+                                      cnpc_stream_t stream) {
+    CNPC_REQUIRE(ctx, ctx != nullptr, "null context");
+    CNPC_REQUIRE(ctx, dtype == CNPC_F32 || dtype == CNPC_F64, "bad dtype");
+    CNPC_REQUIRE(ctx, n >= 2 && n % 2 == 0 && n <= 2048, "n must be even, 2..2048");
+    CNPC_REQUIRE(ctx, sign == 1 || sign == -1, "sign must be +1 or -1");
+    CNPC_REQUIRE(ctx, d_in && d_out && d_in != d_out, "null or aliased buffer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t total = (int64_t)(n / 2 + 1) * n * n;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
+    if (dtype == CNPC_F32)
+        parity_fold_kernel<float><<<blocks, 256, 0, s>>>((const float *)d_in, (float *)d_out, n, (float)sign);
+    else
+        parity_fold_kernel<double><<<blocks, 256, 0, s>>>((const double *)d_in, (double *)d_out, n, (double)sign);
+    return check_launch(ctx, "parity_fold_kernel");
+}
 
 extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const void *d_spec_a, const void *d_spec_b,
                                  const double *h_edges, int nedges, const cnpc_harmonic *h_harmonics,

@@ -200,6 +200,9 @@ class ShellFields:
         self.slot = {}
         self.free = list(range(self.capacity))[::-1]
         self.persistent = False  # fields survive release calls (unit-shell cache)
+        # cells the contractions run over: n^3, or the planes x <= n/2 while
+        # pair_sums contracts parity-folded weights (fold_weights)
+        self.ncell_contract = n * n * n
         self.ready = None        # event after the last synthesis (persistent fields)
 
     @property
@@ -313,7 +316,7 @@ def contract(G, sf, rows, cols):
     staged rows.  Blocks of rows x columns are split so a launch stages at most
     ~100 rows."""
     ctx = _lib.Context.get()
-    ncell = sf.n ** 3
+    ncell = sf.ncell_contract
     dev = _device()
     T = torch.zeros((len(rows), len(cols)), dtype=torch.float64, device=dev)
     if not rows or not cols:
@@ -428,7 +431,7 @@ def contract_pairs(G, sf, pairs):
     out = torch.empty(len(pairs), dtype=torch.float64, device=_device())
     for p0 in range(0, len(pairs), 256):
         chunk = pairs[p0:p0 + 256]
-        ctx.contract_pairs(sf.code, sf.n ** 3, G, sf.fields, sf.stride, [sf.slot[a] for a, _ in chunk],
+        ctx.contract_pairs(sf.code, sf.ncell_contract, G, sf.fields, sf.stride, [sf.slot[a] for a, _ in chunk],
                            [sf.slot[b] for _, b in chunk], out[p0:p0 + len(chunk)])
     return out
 
@@ -482,6 +485,36 @@ class DeferredPairSums:
         return results
 
 
+# FP32 sums over shells of the unit spectrum run over half the cells: the
+# fields have the parity (-1)^l, so sum_x G F_a F_b is the sum over the planes
+# x <= n/2 of the parity-folded weight (cnpc_field_parity_fold)
+PARITY_FOLD = True
+
+
+def fold_weights(groups, sf):
+    """The groups' weights folded for sums over the planes x <= n/2, or None
+    when the fold does not apply: FP32 shells of the unit spectrum only, and
+    every pair of a group with the same parity (-1)^(l1 + l2)."""
+    if not PARITY_FOLD or sf.precision != "f32" or sf.spec_a is not None or sf.spec_b is not None:
+        return None
+    ctx = _lib.Context.get()
+    n = sf.n
+    folded = []
+    for (G, specs) in groups:
+        signs = set()
+        for ps in specs:
+            leg2 = ps.leg1 if ps.mode != "leg" else ps.leg2
+            if ps.leg1[2] != 2 or leg2[2] != 2:
+                return None  # not unit-spectrum shells
+            signs.add(-1 if (ps.leg1[0] + leg2[0]) % 2 else 1)
+        if len(signs) != 1:
+            return None
+        out = torch.empty((n // 2 + 1) * n * n, dtype=G.dtype, device=G.device)
+        ctx.field_parity_fold(sf.code, n, G, signs.pop(), out)
+        folded.append((out, specs))
+    return folded
+
+
 def pair_sums(groups, sf, k_bins, diagonal, block_size):
     """Enqueue sum_x G F1 F2 for every group (G, [PairSpec, ...]) over all bins,
     with one shared shell-field cache; returns one DeferredPairSums per group
@@ -492,6 +525,17 @@ def pair_sums(groups, sf, k_bins, diagonal, block_size):
     the fields of one row block and one column block are resident
     (clustering_estimator.py:911-981 bounds memory the same way).
     """
+    folded = fold_weights(groups, sf)
+    if folded is not None:
+        sf.ncell_contract = (sf.n // 2 + 1) * sf.n * sf.n
+        try:
+            return _pair_sums(folded, sf, k_bins, diagonal, block_size)
+        finally:
+            sf.ncell_contract = sf.n ** 3
+    return _pair_sums(groups, sf, k_bins, diagonal, block_size)
+
+
+def _pair_sums(groups, sf, k_bins, diagonal, block_size):
     outs = [DeferredPairSums(specs, k_bins, diagonal) for (_, specs) in groups]
     bs = k_bins if block_size is None else int(block_size)
     blocks = [list(range(b0, min(k_bins, b0 + bs))) for b0 in range(0, k_bins, bs)]
@@ -586,9 +630,9 @@ def contract_multi(Gs, sf, rows_list, cols):
     cidx = [sf.slot[k] for k in cols]
     T = torch.empty((len(ridx), len(cidx)), dtype=torch.float64, device=_device())
     if GRAM_TC:
-        ctx.gram_tc_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
+        ctx.gram_tc_multi_g(sf.ncell_contract, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
     else:
-        ctx.gram_multi_g(sf.n ** 3, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
+        ctx.gram_multi_g(sf.ncell_contract, Gs, sf.fields, sf.stride, ridx, ag, cidx, T)
     out, r0 = [], 0
     for rows in rows_list:
         out.append(T[r0:r0 + len(rows)])

@@ -393,6 +393,20 @@ int cnpc_field_product_sum(cnpc_ctx *ctx, int dtype, int64_t ncell, int nf, cons
 int cnpc_field_axpby(cnpc_ctx *ctx, int dtype, int64_t ncell, double a, const void *d_x, double b,
                      const void *d_y, void *d_out, cnpc_stream_t stream);
 
+/* Parity fold of a weight field for sums over fields of definite parity.
+ * When F_a(-x) F_b(-x) = sign F_a(x) F_b(x) on the grid (shell fields of the
+ * unit spectrum, conj(Y_lm) times a shell mask, have the parity (-1)^l, so a
+ * product of two has sign (-1)^(l_a + l_b)),
+ *   sum_x G F_a F_b = sum over the planes x = 0 .. n/2 of G' F_a F_b,
+ * G'[x][y][z] = G[x][y][z] on the planes 0 and n/2 and
+ * G[x][y][z] + sign G[n - x][-y][-z] (indices mod n) on the others.
+ * d_out holds (n/2 + 1) n^2 cells: the contraction then runs over
+ * ncell = (n/2 + 1) n^2 with the fields' first planes (x is the slowest
+ * index).  The FFT S3 sums np.sum(S3_field * F1 * F2)
+ * (clustering_estimator.py:1257, :1341) thus read half of every field. */
+int cnpc_field_parity_fold(cnpc_ctx *ctx, int dtype, int n, const void *d_in, int sign, void *d_out,
+                           cnpc_stream_t stream);
+
 /* Shell fields in one call, FP32: the real fields
  *   h_out_fields[j] = c2r(src * Y * mask_bin * phi)   (item j, as in
  * cnpc_shell_spectra followed by cnpc_fft_c2r) for n = 64, 128 or 256, when

@@ -222,6 +222,50 @@ def test_pair_contraction_matches_fp64_sums(dtype, n):
     assert err < (1e-14 if dtype == "f64" else 1e-6), err
 
 
+@pytest.mark.parametrize("n", [64, 128])
+def test_parity_folded_contraction_matches_full_sum(n):
+    """Shells of the unit spectrum have the parity (-1)^l, so sum_x G F_a F_b
+    over all cells equals the sum over the planes x <= n/2 of the folded weight
+    (cnpc_field_parity_fold, sign (-1)^(l_a + l_b)); checked for even and odd
+    products, with fields from the fused kernel (its reflected planes) and the
+    cuFFT route."""
+    import torch
+    from cosmonpc_b200 import _lib, angular
+
+    L = 1000.0 * n / 64
+    kf = 2 * np.pi / L
+    edges = np.linspace(0.0, (n / 4 - 0.5) * kf, 5)
+    ctx = _lib.Context.get()
+    harms = [angular.harmonic(0, 0), angular.harmonic(1, 0), angular.harmonic(2, 0)]
+    # unit-spectrum items (source 2, conj): l = 0, 1, 2 over 4 bins
+    items = [_lib.ShellItem(b, h, 1 if h == 1 else 0, 2, 1) for h in range(3) for b in range(4)]
+    ls = [angular_l for angular_l in (0, 1, 2) for _ in range(4)]
+    fused = torch.empty((len(items), n ** 3), dtype=torch.float32, device="cuda")
+    ctx.shell_fields(n, L, None, None, edges, harms, items, [fused[j] for j in range(len(items))])
+    half = torch.empty((len(items), n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    ctx.shell_spectra(_lib.F32, n, L, None, None, edges, harms, items, half)
+    direct = torch.empty((len(items), n ** 3), dtype=torch.float32, device="cuda")
+    ctx.c2r(_lib.F32, n, len(items), half, direct)
+    del half
+    rng = np.random.default_rng(n)
+    G = torch.from_numpy(rng.standard_normal(n ** 3).astype(np.float32)).cuda()
+    hcell = (n // 2 + 1) * n * n
+    for fields in (fused, direct):
+        for (la, lb) in ((0, 0), (2, 0), (1, 1), (1, 0), (2, 1)):
+            a = [j for j in range(len(items)) if ls[j] == la]
+            b = [j for j in range(len(items)) if ls[j] == lb]
+            full = torch.empty((len(a), len(b)), dtype=torch.float64, device="cuda")
+            ctx.gram(_lib.F32, n ** 3, G, fields, n ** 3, a, b, full)
+            Gf = torch.empty(hcell, dtype=torch.float32, device="cuda")
+            ctx.field_parity_fold(_lib.F32, n, G, -1 if (la + lb) % 2 else 1, Gf)
+            folded = torch.empty_like(full)
+            ctx.gram(_lib.F32, hcell, Gf, fields, n ** 3, a, b, folded)
+            fd, gd = fields.double(), G.double()
+            scale = (gd.abs() * fd[a].abs()) @ fd[b].abs().T
+            err = ((folded - full).abs() / scale).max().item()
+            assert err < 2e-6, (la, lb, err)
+
+
 @pytest.mark.parametrize("ncell,na,nb,shared", [(128 ** 3, 40, 20, True), (256 ** 3, 40, 20, True),
                                                 (64 ** 3 + 100, 17, 9, False), (4096 + 36, 3, 2, False)])
 def test_ffma_gram_matches_fp64(ncell, na, nb, shared):
