@@ -15,9 +15,11 @@
 // An n-point inverse DFT whose input is confined to |k| < n/4 is computed as
 // two n/2-point FFTs (even and odd outputs; the odd one with input twiddles
 // e^{2 pi i s / n}) and the output phase (-1)^m (-i)^r of the shift by n/4.
-// The n/2-point FFT is done by a team of T = n/32 threads holding 16 values
-// each: a 16-point DFT in registers, twiddles, one shared-memory exchange and
-// T-point DFTs.  Twiddles come from an FP64-computed table rounded to FP32.
+// The n/2-point FFT is done by a team of T threads holding V values each: a
+// V-point DFT in registers, twiddles, one shared-memory exchange and T-point
+// DFTs.  n = 64, 128, 256 use V = 16 and T = n/32; n = 192 (M = 96, which has
+// the factor 3) uses V = 24 (8 x 3 in registers) and T = 4.  Twiddles come
+// from an FP64-computed table rounded to FP32.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -119,37 +121,101 @@ __device__ __forceinline__ void idft16(float2 *v) {
     for (int i = 0; i < 16; ++i) v[i] = o[i];
 }
 
-// Exchange slots of one team: 16 rows of T float2, element (k1, c) at
-// k1 T + (c ^ ((k1 / (16 / T)) % T)), and a team stride of T (mod 16) float2.
-// The row writes (fixed k1, c = t) and the transposed reads (k1 = t 16/T + q,
-// fixed c) of the teams of a warp then hit every bank pair exactly twice: no
-// bank conflicts for T = 2, 4, 8.
-template <int T> struct Exch {
-    static constexpr int kStride = 17 * T;
-};
+// 3-point inverse DFT: with W = e^{2 pi i / 3} = -1/2 + i sqrt(3)/2,
+// X1 = a - (b + c)/2 + i sqrt(3)/2 (b - c) and X2 its partner with -i.
+constexpr float kS3 = 0.86602540378443864676f;  // sin(pi/3)
+__device__ __forceinline__ void idft3(float2 &a, float2 &b, float2 &c) {
+    const float2 s = cadd(b, c), d = csub(b, c);
+    const float2 h = make_float2(a.x - 0.5f * s.x, a.y - 0.5f * s.y);
+    const float2 r = make_float2(-kS3 * d.y, kS3 * d.x);  // i sqrt(3)/2 (b - c)
+    a = cadd(a, s);
+    b = cadd(h, r);
+    c = csub(h, r);
+}
 
-// Per-thread twiddles of team_fft, [k1 - 1][t] = W_M^{t k1} (k1 = 1..15): the
-// T threads of a team read T consecutive slots.
-template <int T> __host__ __device__ constexpr int team_twiddles() { return 15 * T; }
-template <int T> __device__ __forceinline__ void fill_team_twiddles(float2 *twt, const float2 *tw) {
-    for (int e = threadIdx.x; e < 15 * T; e += blockDim.x) {
-        const int k1 = e / T + 1, t = e % T;
-        twt[e] = tw[2 * ((t * k1) % (16 * T))];
+constexpr float kC24 = 0.96592582628906828675f;  // cos(pi/12)
+constexpr float kS24 = 0.25881904510252076235f;  // sin(pi/12)
+
+// W24^m = e^{2 pi i m / 24}, m = 0..14 (the products j2 k1 of idft24)
+__device__ __forceinline__ float2 w24(int m) {
+    switch (m) {
+        case 0: return make_float2(1.f, 0.f);
+        case 1: return make_float2(kC24, kS24);
+        case 2: return make_float2(kS3, 0.5f);
+        case 3: return make_float2(kC8, kC8);
+        case 4: return make_float2(0.5f, kS3);
+        case 5: return make_float2(kS24, kC24);
+        case 6: return make_float2(0.f, 1.f);
+        case 7: return make_float2(-kS24, kC24);
+        case 8: return make_float2(-0.5f, kS3);
+        case 10: return make_float2(-kS3, 0.5f);
+        case 12: return make_float2(-1.f, 0.f);
+        default: return make_float2(-kS3, -0.5f);  // 14
     }
 }
 
-// Team FFT of size M = 16 T (inverse).  On entry thread t of the team holds
-// u[j] = x[T j + t]; on exit it holds X[k1 + 16 k2] for k1 = t (16/T) + q
-// (q < 16/T), k2 < T, stored as u[q * T + k2].  ex: the team's exchange slots
-// (Exch<T>); twt: the per-thread twiddle table (fill_team_twiddles).
-template <int T>
+__device__ __forceinline__ void idft24(float2 *v) {
+    // j = 3 j1 + j2, k = k1 + 8 k2: W24^{jk} = W8^{j1 k1} W24^{j2 k1} W3^{j2 k2}
+    float2 a[3][8];
+#pragma unroll
+    for (int j2 = 0; j2 < 3; ++j2) {
+#pragma unroll
+        for (int j1 = 0; j1 < 8; ++j1) a[j2][j1] = v[3 * j1 + j2];
+        idft8(a[j2]);
+    }
+#pragma unroll
+    for (int j2 = 1; j2 < 3; ++j2)
+#pragma unroll
+        for (int k1 = 1; k1 < 8; ++k1) a[j2][k1] = cmul(a[j2][k1], w24(j2 * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) {
+        idft3(a[0][k1], a[1][k1], a[2][k1]);
+        v[k1] = a[0][k1];
+        v[k1 + 8] = a[1][k1];
+        v[k1 + 16] = a[2][k1];
+    }
+}
+
+// V-point inverse DFT in registers (natural order out)
+template <int V> __device__ __forceinline__ void idft_regs(float2 *v) {
+    if constexpr (V == 16)
+        idft16(v);
+    else
+        idft24(v);
+}
+
+// Exchange slots of one team: V rows of T float2, element (k1, c) at
+// k1 T + (c ^ ((k1 / (V / T)) % T)), and a team stride of T (mod 16) float2.
+// The row writes (fixed k1, c = t) and the transposed reads (k1 = t V/T + q,
+// fixed c) of the teams of a warp then hit every bank pair exactly twice for
+// V = 16: no bank conflicts for T = 2, 4, 8.
+template <int T, int V = 16> struct Exch {
+    static constexpr int kStride = (V + 1) * T;
+};
+
+// Per-thread twiddles of team_fft, [k1 - 1][t] = W_M^{t k1} (k1 = 1..V-1): the
+// T threads of a team read T consecutive slots.
+template <int T, int V = 16> __host__ __device__ constexpr int team_twiddles() { return (V - 1) * T; }
+template <int T, int V = 16> __device__ __forceinline__ void fill_team_twiddles(float2 *twt, const float2 *tw) {
+    for (int e = threadIdx.x; e < (V - 1) * T; e += blockDim.x) {
+        const int k1 = e / T + 1, t = e % T;
+        twt[e] = tw[2 * ((t * k1) % (V * T))];
+    }
+}
+
+// Team FFT of size M = V T (inverse).  On entry thread t of the team holds
+// u[j] = x[T j + t]; on exit it holds X[k1 + V k2] for k1 = t (V/T) + q
+// (q < V/T), k2 < T, stored as u[q * T + k2].  ex: the team's exchange slots
+// (Exch<T, V>); twt: the per-thread twiddle table (fill_team_twiddles).
+template <int T, int V = 16>
 __device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const float2 *twt, unsigned mask) {
-    constexpr int Q = 16 / T;
-    idft16(u);
+    static_assert(V % T == 0, "V must be a multiple of T");
+    constexpr int Q = V / T;
+    idft_regs<V>(u);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) u[k1] = cmul(u[k1], twt[(k1 - 1) * T + t]);
+    for (int k1 = 1; k1 < V; ++k1) u[k1] = cmul(u[k1], twt[(k1 - 1) * T + t]);
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) ex[k1 * T + (t ^ ((k1 / Q) % T))] = u[k1];
+    for (int k1 = 0; k1 < V; ++k1) ex[k1 * T + (t ^ ((k1 / Q) % T))] = u[k1];
     __syncwarp(mask);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -167,9 +233,9 @@ __device__ __forceinline__ void team_fft(float2 *u, int t, float2 *ex, const flo
 }
 
 // output index m (of the M-point transform) held in u[q T + k2]
-template <int T>
+template <int T, int V = 16>
 __device__ __forceinline__ int team_out_index(int t, int q, int k2) {
-    return (t * (16 / T) + q) + 16 * k2;
+    return (t * (V / T) + q) + V * k2;
 }
 
 // (-1)^m (-i)^r phase of the shift by n/4 for output position x = 2 m + r
@@ -219,11 +285,11 @@ __device__ __forceinline__ unsigned team_mask(int T) {
 // Pass 1: block (s, chunk, item) synthesises kKC in-band columns over n_x
 // from the source spectrum, transforms them along x and writes
 // A[x][s][chunk].
-template <int T>
+template <int T, int V>
 __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     const float2 *__restrict__ Aspec, const float2 *__restrict__ Bspec, int n, double L, EdgeSet edges,
     HarmTable harm, ShellItemsDev items, float2 *__restrict__ dst) {
-    constexpr int M = 16 * T, N = 2 * M, H = M / 2;
+    constexpr int M = V * T, N = 2 * M, H = M / 2;
     constexpr int KC = (kKC < H) ? kKC : H;
     constexpr int LDC = KC + 1;
     constexpr int NCH = H / KC;
@@ -231,9 +297,9 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     float2 *in = reinterpret_cast<float2 *>(smem4);  // [M][LDC]
     float2 *out = in + M * LDC;                      // [N][LDC]
     float2 *tw = out + N * LDC;                      // [N]
-    float2 *ex = tw + N;                             // [teams][Exch<T>::kStride]
-    float2 *twt = ex + (kColThreads / T) * Exch<T>::kStride;                  // [15 T]
-    double *kt = reinterpret_cast<double *>(twt + team_twiddles<T>());        // [n + 1]
+    float2 *ex = tw + N;                             // [teams][Exch<T, V>::kStride]
+    float2 *twt = ex + (kColThreads / T) * Exch<T, V>::kStride;               // [(V - 1) T]
+    double *kt = reinterpret_cast<double *>(twt + team_twiddles<T, V>());     // [n + 1]
     double *se = kt + (n + 1);                                                 // [edges.n]
     const int nitems = items.n;
     const int item = blockIdx.x % nitems;
@@ -250,7 +316,7 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
         const cnpc_shell_item it = items.it[item];
         if (threadIdx.x == 0) hm = harm.h[it.harmonic];
         __syncthreads();
-        fill_team_twiddles<T>(twt, tw);  // first read after the barrier below
+        fill_team_twiddles<T, V>(twt, tw);  // first read after the barrier below
         const int s = row + 1;
         const int ny = s - H;
         const int iy = ny < 0 ? ny + n : ny;
@@ -290,23 +356,23 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
     __syncthreads();
     const int team = threadIdx.x / T, t = threadIdx.x % T, nteams = kColThreads / T;
     const unsigned mask = team_mask(T);
-    float2 *tex = ex + team * Exch<T>::kStride;
+    float2 *tex = ex + team * Exch<T, V>::kStride;
     for (int job = team; job < 2 * KC; job += nteams) {
         const int c = job >> 1, r = job & 1;
-        float2 u[16];
+        float2 u[V];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < V; ++j) {
             const int slot = T * j + t;
             float2 v = in[slot * LDC + c];
             if (r) v = cmul(v, tw[slot]);
             u[j] = v;
         }
-        team_fft<T>(u, t, tex, twt, mask);
+        team_fft<T, V>(u, t, tex, twt, mask);
 #pragma unroll
-        for (int q = 0; q < 16 / T; ++q)
+        for (int q = 0; q < V / T; ++q)
 #pragma unroll
             for (int k2 = 0; k2 < T; ++k2) {
-                const int m = team_out_index<T>(t, q, k2);
+                const int m = team_out_index<T, V>(t, q, k2);
                 out[(2 * m + r) * LDC + c] = shift_phase(u[q * T + k2], m, r);
             }
     }
@@ -326,16 +392,20 @@ __global__ void __launch_bounds__(kColThreads) shell_column_kernel(
 // m < n/2, of B[x] into shared memory; the z pass then turns row pairs
 // (m1, m2) into two real rows of the field through one complex transform of
 // v(k_z) = B1~(k_z) + i B2~(k_z), B~(-k_z) = conj B(k_z), B~(0) = Re B(0).
-// Thread t of a team ends the z pass holding z = 2Q t + c + 32 k2 (c < 2Q)
-// of both rows, written as float4 runs without staging.
-constexpr int kYZThreads = 256;
-
-template <int T> struct YZLayout {
-    static constexpr int M = 16 * T, N = 2 * M, H = M / 2, LD = H + 1;
-    static constexpr int TEAMS = kYZThreads / T;
+// Thread t of a team ends the z pass holding z = 2Q t + c + 2V k2 (c < 2Q,
+// Q = V/T) of both rows, written as float4 runs without staging.
+// V = 16: 256 threads, 2 blocks per SM.  V = 24 (n = 192) keeps 24 values
+// per FFT and 48 results of the z pass per thread: 48 teams of 4 (one round
+// for the n/4 = 48 columns of the y pass and the 48 row pairs of the z pass),
+// 2 blocks per SM, so the register limit is 170.
+template <int T, int V = 16> struct YZLayout {
+    static constexpr int THREADS = V == 16 ? 256 : 192;
+    static constexpr int MIN_BLOCKS = 2;
+    static constexpr int M = V * T, N = 2 * M, H = M / 2, LD = H + 1;
+    static constexpr int TEAMS = THREADS / T;
     static constexpr int kEx = N;                                    // after the twiddles
-    static constexpr int kTwt = kEx + TEAMS * Exch<T>::kStride;      // team twiddles
-    static constexpr int kB = ((kTwt + team_twiddles<T>() + 1) / 2) * 2;
+    static constexpr int kTwt = kEx + TEAMS * Exch<T, V>::kStride;   // team twiddles
+    static constexpr int kB = ((kTwt + team_twiddles<T, V>() + 1) / 2) * 2;
     static constexpr int kTotal = kB + M * LD;                       // float2
 };
 
@@ -357,7 +427,7 @@ __device__ __forceinline__ int yz_rmax(const YZOut &O, int item) { return O.rmax
 __device__ __forceinline__ int yz_mirror(const YZOut &O, int item) { return O.rmax[item] >> 16; }
 
 // Reflected copy of a row with 16-byte stores.  Thread t of a team holds the
-// run r(z0 .. z0 + Q2 - 1) of a row, z0 = Q2 t + 32 k2 (Q2 T = 32).  Element z
+// run r(z0 .. z0 + Q2 - 1) of a row, z0 = Q2 t + Q2 T k2 (Q2 T = 2V).  Element z
 // goes to (N - z) mod N of the mirror row, so the aligned run at N - z0 - Q2
 // is {r(z0 + Q2), r(z0 + Q2 - 1), ..., r(z0 + 1)}: the first value of the next
 // run (team lane t + 1 at this k2; for the last lane, lane 0 at k2 + 1, which
@@ -370,7 +440,7 @@ __device__ __forceinline__ void store_reflected(float *row, int t, int k2, const
     float nxt = __shfl_down_sync(mask, v[0], 1, T);
     if (t == T - 1) nxt = carry;
     carry = __shfl_sync(mask, v[0], 0, T);
-    const int base = N - (Q2 * t + 32 * k2) - Q2;  // a multiple of 4
+    const int base = N - (Q2 * t + Q2 * T * k2) - Q2;  // a multiple of 4
     float m[Q2];
     m[0] = sgn * nxt;
 #pragma unroll
@@ -385,12 +455,12 @@ __device__ __forceinline__ void store_reflected(float *row, int t, int k2, const
     }
 }
 
-template <int T>
-__global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *__restrict__ work, int nitems,
-                                                                  const YZOut O) {
-    using YL = YZLayout<T>;
+template <int T, int V>
+__global__ void __launch_bounds__(YZLayout<T, V>::THREADS, YZLayout<T, V>::MIN_BLOCKS)
+    shell_yz_kernel(const float2 *__restrict__ work, int nitems, const YZOut O) {
+    using YL = YZLayout<T, V>;
     constexpr int M = YL::M, N = YL::N, H = YL::H, LD = YL::LD, TEAMS = YL::TEAMS;
-    constexpr int Q = 16 / T;
+    constexpr int Q = V / T;
     extern __shared__ float4 smem4[];
     float2 *tw = reinterpret_cast<float2 *>(smem4);
     float2 *Bh = tw + YL::kB;  // [M][LD]: rows y = 2m + ry
@@ -404,11 +474,11 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     float2 *twt = tw + YL::kTwt;
     fill_twiddles(tw, N);
     __syncthreads();
-    fill_team_twiddles<T>(twt, tw);
+    fill_team_twiddles<T, V>(twt, tw);
     __syncthreads();
     const int team = threadIdx.x / T, t = threadIdx.x % T;
     const unsigned mask = team_mask(T);
-    float2 *tex = tw + YL::kEx + team * Exch<T>::kStride;
+    float2 *tex = tw + YL::kEx + team * Exch<T, V>::kStride;
     const float2 *a = work + ((size_t)item * N + x) * M * H;  // A[x][slot][kz]
     const int rmax = yz_rmax(O, item), r2max = O.r2max[item];
     const int K = rmax + 1 < H ? rmax + 1 : H;  // columns k_z >= K are zero
@@ -416,38 +486,41 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
     // y: one team per k_z column
     for (int kz = team; kz < K; kz += TEAMS) {
         const int kz0 = (kz / KC) * KC;
-        float2 u[16];
+        float2 u[V];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < V; ++j) {
             const int slot = T * j + t;
             float2 v = make_float2(0.f, 0.f);
             if (slot > 0 && tile_live(slot - H, kz0, r2max)) v = __ldg(a + (size_t)slot * H + kz);
             if (ry) v = cmul(v, tw[slot]);
             u[j] = v;
         }
-        team_fft<T>(u, t, tex, twt, mask);
+        team_fft<T, V>(u, t, tex, twt, mask);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int k2 = 0; k2 < T; ++k2) {
-                const int m = team_out_index<T>(t, q, k2);
+                const int m = team_out_index<T, V>(t, q, k2);
                 Bh[m * LD + kz] = shift_phase(u[q * T + k2], m, ry);
             }
     }
     __syncthreads();
     float *fout = O.out[item] + (size_t)x * N * N;
     float *fmir = O.out[item] + (size_t)(N - x) * N * N;  // used when mirror
-    // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity.  Teams of one warp
-    // take pairs 4 apart, so their rows sit 8 * LD float2 (16 banks) apart.
+    // z: row pairs (m1, m2) = (2 p, 2 p + 1) of this parity.  V = 16: teams of
+    // one warp take pairs 4 apart, so their rows sit 8 * LD float2 (16 banks)
+    // apart.  V = 24 (teams of 4, LD = 49): the 4 teams of a half-warp take
+    // pairs 2 apart, rows 4 * LD float2 (8 banks) apart.
     for (int p0 = 0; p0 < M / 2; p0 += TEAMS) {
-        const int p = p0 + ((TEAMS >= 16 && (TEAMS & 15) == 0)
+        const int p = p0 + (V == 24 ? (2 * (team & 3) + ((team >> 2) & 1) + 8 * (team >> 3))
+                            : (TEAMS >= 16 && (TEAMS & 15) == 0)
                                 ? ((team & 3) * 4 + ((team >> 2) & 3) + 16 * (team >> 4))
                                 : team);
         if (p >= M / 2) continue;
         const float2 *b1 = Bh + (2 * p) * LD, *b2 = b1 + LD;
-        float2 v[16];
+        float2 v[V];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < V; ++j) {
             const int slot = T * j + t;
             const int kz = slot - H;
             const int ak = kz < 0 ? -kz : kz;
@@ -463,21 +536,21 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             }
             v[j] = w;
         }
-        float2 res[2][16];
+        float2 res[2][V];
 #pragma unroll
         for (int rz = 0; rz < 2; ++rz) {
-            float2 u[16];
+            float2 u[V];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) u[j] = rz ? cmul(v[j], tw[T * j + t]) : v[j];
-            team_fft<T>(u, t, tex, twt, mask);
+            for (int j = 0; j < V; ++j) u[j] = rz ? cmul(v[j], tw[T * j + t]) : v[j];
+            team_fft<T, V>(u, t, tex, twt, mask);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) res[rz][i] = u[i];
+            for (int i = 0; i < V; ++i) res[rz][i] = u[i];
         }
         const int y1 = 2 * (2 * p) + ry, y2 = 2 * (2 * p + 1) + ry;  // y = 2 m + ry
         float *row1 = fout + (size_t)y1 * N;
         float *row2 = fout + (size_t)y2 * N;
-        float *mrow1 = fmir + (size_t)((N - y1) & (N - 1)) * N;
-        float *mrow2 = fmir + (size_t)((N - y2) & (N - 1)) * N;
+        float *mrow1 = fmir + (size_t)((N - y1) % N) * N;
+        float *mrow2 = fmir + (size_t)((N - y2) % N) * N;
         float carry1 = 0.f, carry2 = 0.f;  // the reflection needs the next (higher) k2's first values
 #pragma unroll
         for (int k2 = T - 1; k2 >= 0; --k2) {
@@ -486,12 +559,12 @@ __global__ void __launch_bounds__(kYZThreads, 2) shell_yz_kernel(const float2 *_
             for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int rz = 0; rz < 2; ++rz) {
-                    const int m = team_out_index<T>(t, q, k2);
+                    const int m = team_out_index<T, V>(t, q, k2);
                     const float2 g = shift_phase(res[rz][q * T + k2], m, rz);
                     re[2 * q + rz] = g.x;
                     im[2 * q + rz] = g.y;
                 }
-            const int z0 = 2 * Q * t + 32 * k2;
+            const int z0 = 2 * Q * t + 2 * V * k2;
 #pragma unroll
             for (int c = 0; c < 2 * Q; c += 4) {
                 *reinterpret_cast<float4 *>(row1 + z0 + c) = make_float4(re[c], re[c + 1], re[c + 2], re[c + 3]);
@@ -690,31 +763,32 @@ __global__ void __launch_bounds__(YZPipe<T>::THREADS, 1) shell_yz_pipe_kernel(co
 // the pipelined y/z kernel for n = 128 (false: one block per unit)
 constexpr bool kShellPipeline = true;
 
-template <int T> static size_t column_smem(int nedges) {
-    const int M = 16 * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
-    return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T>::kStride +
-                             team_twiddles<T>()) +
+template <int T, int V> static size_t column_smem(int nedges) {
+    const int M = V * T, N = 2 * M, H = M / 2, KC = kKC < H ? kKC : H, LDC = KC + 1;
+    return sizeof(float2) * ((size_t)M * LDC + (size_t)N * LDC + N + (kColThreads / T) * Exch<T, V>::kStride +
+                             team_twiddles<T, V>()) +
            sizeof(double) * (N + 1 + nedges);
 }
-template <int T> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLayout<T>::kTotal; }
+template <int T, int V> static size_t yz_smem() { return sizeof(float2) * (size_t)YZLayout<T, V>::kTotal; }
 
-template <int T>
+template <int T, int V>
 static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, const float2 *B, const EdgeSet &es,
                             const HarmTable &ht, const ShellItemsDev &items, float2 *workA,
                             const YZOut &O, cudaStream_t s) {
-    constexpr int M = 16 * T, N = 2 * M, H = M / 2;
+    constexpr int M = V * T, N = 2 * M, H = M / 2;
     constexpr int KC = kKC < H ? kKC : H;
     constexpr int NCH = H / KC;
-    const size_t sc = column_smem<T>(es.n), sr = yz_smem<T>();
-    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T>,
+    static_assert(H % KC == 0, "column chunks must tile n/4");
+    const size_t sc = column_smem<T, V>(es.n), sr = yz_smem<T, V>();
+    int st = check_cuda(ctx, cudaFuncSetAttribute(shell_column_kernel<T, V>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc), "shell smem");
     if (st) return st;
-    st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)sr), "shell smem");
     if (st) return st;
     const int ni = items.n;
-    shell_column_kernel<T><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, workA);
-    if constexpr (T == 4 && kShellPipeline) {
+    shell_column_kernel<T, V><<<(M - 1) * NCH * ni, kColThreads, sc, s>>>(A, B, n, L, es, ht, items, workA);
+    if constexpr (T == 4 && V == 16 && kShellPipeline) {
         using YP = YZPipe<T>;
         const size_t sp = sizeof(float2) * (size_t)YP::kTotal;
         st = check_cuda(ctx, cudaFuncSetAttribute(shell_yz_pipe_kernel<T>,
@@ -728,7 +802,7 @@ static int launch_shell_fft(cnpc_ctx *ctx, int n, double L, const float2 *A, con
         const int grid = std::min(N * 2 * ni, std::max(1, per_sm) * ctx->num_sms);
         shell_yz_pipe_kernel<T><<<grid, YP::THREADS, sp, s>>>(workA, ni, O);
     } else {
-        shell_yz_kernel<T><<<N * 2 * ni, kYZThreads, sr, s>>>(workA, ni, O);
+        shell_yz_kernel<T, V><<<N * 2 * ni, YZLayout<T, V>::THREADS, sr, s>>>(workA, ni, O);
     }
     return check_launch(ctx, "shell_fields kernels");
 }
@@ -751,6 +825,45 @@ __global__ void parity_fold_kernel(const T *__restrict__ in, T *__restrict__ out
     }
 }
 
+// FP32 form of parity_fold_kernel for n % 4 == 0: one warp per row (x, y),
+// 16-byte loads and stores.  Element z of the row needs the mirror row's
+// element (n - z) mod n; for the float4 j (z = 4j .. 4j + 3) those are
+// p.w, p.z, p.y of the mirror row's float4 n/4 - 1 - j and, first, the
+// element n - 4j, which is the x of the float4 the lane before loads (lane 0
+// reads it directly).  Same sums, same rounding as parity_fold_kernel.
+__global__ void parity_fold_rows_kernel(const float *__restrict__ in, float *__restrict__ out, int n, float sign) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const int nrows = (n / 2 + 1) * n, nq = n / 4;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows; r += warps) {
+        const int x = r / n, y = r % n;
+        const float4 *src = reinterpret_cast<const float4 *>(in + (size_t)r * n);
+        float4 *dst = reinterpret_cast<float4 *>(out + (size_t)r * n);
+        if (x == 0 || x == n / 2) {
+            for (int j = lane; j < nq; j += 32) dst[j] = src[j];
+            continue;
+        }
+        const int yr = y == 0 ? 0 : n - y;
+        const float *mrow = in + ((size_t)(n - x) * n + yr) * n;
+        const float4 *m4 = reinterpret_cast<const float4 *>(mrow);
+        for (int j0 = 0; j0 < nq; j0 += 32) {
+            const int j = j0 + lane;
+            const bool ok = j < nq;
+            const float4 p = ok ? m4[nq - 1 - j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            float first = __shfl_up_sync(0xffffffffu, p.x, 1);
+            if (lane == 0) first = mrow[(n - 4 * j) % n];
+            if (ok) {
+                float4 v = src[j];
+                v.x += sign * first;
+                v.y += sign * p.w;
+                v.z += sign * p.z;
+                v.w += sign * p.y;
+                dst[j] = v;
+            }
+        }
+    }
+}
+
 }  // namespace cnpc
 
 using namespace cnpc;
@@ -765,7 +878,14 @@ extern "C" int cnpc_field_parity_fold(cnpc_ctx *ctx, int dtype, int n, const voi
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t total = (int64_t)(n / 2 + 1) * n * n;
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
-    if (dtype == CNPC_F32)
+    const bool rows16 = n % 4 == 0 && reinterpret_cast<uintptr_t>(d_in) % 16 == 0 &&
+                        reinterpret_cast<uintptr_t>(d_out) % 16 == 0;
+    if (dtype == CNPC_F32 && rows16) {
+        // one warp per row, 8 warps per block
+        const int64_t rows = (int64_t)(n / 2 + 1) * n;
+        const int rblocks = (int)std::min<int64_t>((rows + 7) / 8, (int64_t)ctx->num_sms * 8);
+        parity_fold_rows_kernel<<<rblocks, 256, 0, s>>>((const float *)d_in, (float *)d_out, n, (float)sign);
+    } else if (dtype == CNPC_F32)
         parity_fold_kernel<float><<<blocks, 256, 0, s>>>((const float *)d_in, (float *)d_out, n, (float)sign);
     else
         parity_fold_kernel<double><<<blocks, 256, 0, s>>>((const double *)d_in, (double *)d_out, n, (double)sign);
@@ -778,7 +898,7 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
                                  void *const *h_out_fields, cnpc_stream_t stream) {
     int st = check_common(ctx, CNPC_F32, n, boxsize);
     if (st) return st;
-    CNPC_REQUIRE(ctx, n == 64 || n == 128 || n == 256, "fused shell fields support n = 64, 128, 256");
+    CNPC_REQUIRE(ctx, n == 64 || n == 128 || n == 192 || n == 256, "fused shell fields support n = 64, 128, 192, 256");
     CNPC_REQUIRE(ctx, nitems >= 1 && nitems <= CNPC_MAX_ITEMS, "nitems out of range (1..256)");
     CNPC_REQUIRE(ctx, nharmonics >= 1 && nharmonics <= CNPC_MAX_HARMONICS, "nharmonics out of range");
     CNPC_REQUIRE(ctx, h_harmonics && h_items && h_out_fields, "null table");
@@ -812,7 +932,6 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
         items.rmax[j] = (int)std::floor(rt);
         items.r2max[j] = (int)std::floor(rt * rt) + 1;
     }
-    const int T = n / 32;
     const size_t per_item_a = sizeof(float2) * (size_t)n * (n / 2) * (n / 4);  // A[x][s][n_z]
     cudaStream_t s = (cudaStream_t)stream;
     // the pass-1 work array
@@ -830,7 +949,8 @@ extern "C" int cnpc_shell_fields(cnpc_ctx *ctx, int n, double boxsize, const voi
     }
     const float2 *A = static_cast<const float2 *>(d_spec_a);
     const float2 *B = static_cast<const float2 *>(d_spec_b);
-    if (T == 2) return launch_shell_fft<2>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
-    if (T == 4) return launch_shell_fft<4>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
-    return launch_shell_fft<8>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    if (n == 64) return launch_shell_fft<2, 16>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    if (n == 128) return launch_shell_fft<4, 16>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    if (n == 192) return launch_shell_fft<4, 24>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
+    return launch_shell_fft<8, 16>(ctx, n, boxsize, A, B, es, ht, items, workA, O, s);
 }

@@ -130,7 +130,7 @@ def kbin_counts(n, boxsize, edges):
 # Extra elements between consecutive shell fields (0: contiguous batches,
 # which cuFFT writes fastest).
 FIELD_PAD = 0
-# FP32 shell fields of n = 64/128/256 whose bins lie below k_Nyquist / 2 are
+# FP32 shell fields of n = 64/128/192/256 whose bins lie below k_Nyquist / 2 are
 # synthesised and inverse-transformed by the fused band-limited kernels
 # (cnpc_shell_fields) instead of shell spectra + cuFFT C2R.
 FUSED_SHELLS = True
@@ -155,7 +155,7 @@ PAIR_LIST = True
 
 
 def fused_shells_apply(n, boxsize, edges, bins, precision):
-    if not FUSED_SHELLS or precision != "f32" or n not in (64, 128, 256):
+    if not FUSED_SHELLS or precision != "f32" or n not in (64, 128, 192, 256):
         return False
     kf = 2.0 * np.pi / float(boxsize)
     top = max(float(edges[b + 1]) for b in bins)

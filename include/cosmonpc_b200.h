@@ -409,7 +409,7 @@ int cnpc_field_parity_fold(cnpc_ctx *ctx, int dtype, int n, const void *d_in, in
 
 /* Shell fields in one call, FP32: the real fields
  *   h_out_fields[j] = c2r(src * Y * mask_bin * phi)   (item j, as in
- * cnpc_shell_spectra followed by cnpc_fft_c2r) for n = 64, 128 or 256, when
+ * cnpc_shell_spectra followed by cnpc_fft_c2r) for n = 64, 128, 192 or 256, when
  * every item's bin lies below k = (n/4) 2 pi / L -- always the case for the
  * bispectrum shells, whose top edge k_max is below k_Nyquist / 2 by the
  * reference's own check (task_executor.py:192-196).  The inverse FFT runs on

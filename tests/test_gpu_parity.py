@@ -155,7 +155,7 @@ def test_bk_full_64_against_oracle(precision, tmp_path):
             assert rel_err(got[k], ref[k]) < TOL[precision], (k, rel_err(got[k], ref[k]))
 
 
-@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("n", [64, 128, 192, 256])
 def test_fused_shell_fields_match_cufft_route(n):
     """cnpc_shell_fields (band-limited fused transform) against shell spectra
     followed by cuFFT C2R, for every harmonic kind, component, source and conj."""
@@ -220,6 +220,33 @@ def test_pair_contraction_matches_fp64_sums(dtype, n):
     scale = torch.stack([(gl.abs() * fl[i, :ncell].abs() * fl[j, :ncell].abs()).sum() for i, j in zip(a, b)])
     err = ((out - ref).abs() / scale).max().item()
     assert err < (1e-14 if dtype == "f64" else 1e-6), err
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+@pytest.mark.parametrize("n,offset", [(30, 0), (64, 0), (128, 0), (256, 0), (192, 0), (64, 1)])
+def test_parity_fold_matches_torch(dtype, n, offset):
+    """cnpc_field_parity_fold bit for bit against torch: the planes 0 and n/2
+    copied, the others in[x] + sign in[n - x][-y][-z]; the row kernel (FP32,
+    n % 4 == 0, 16-byte aligned) and the element kernel (odd n / 4, an
+    unaligned input, FP64)."""
+    import torch
+    from cosmonpc_b200 import _lib
+
+    code, tdt = (_lib.F32, torch.float32) if dtype == "f32" else (_lib.F64, torch.float64)
+    ctx = _lib.Context.get()
+    g = torch.Generator(device="cuda").manual_seed(n + offset)
+    buf = torch.randn(n ** 3 + offset, dtype=tdt, device="cuda", generator=g)
+    src = buf[offset:]
+    x = src.view(n, n, n)
+    # index (n - i) mod n along y and z, plane n - x along x
+    rev = torch.roll(torch.flip(x, dims=(1, 2)), shifts=(1, 1), dims=(1, 2))
+    for sign in (1, -1):
+        out = torch.full(((n // 2 + 1) * n * n,), float("nan"), dtype=tdt, device="cuda")
+        ctx.field_parity_fold(code, n, src, sign, out)
+        ref = x[: n // 2 + 1].clone()
+        ref[1: n // 2] = x[1: n // 2] + sign * torch.flip(rev[n // 2 + 1:], dims=(0,))
+        torch.cuda.synchronize()
+        assert torch.equal(out.view(n // 2 + 1, n, n), ref), (dtype, n, offset, sign)
 
 
 @pytest.mark.parametrize("n", [64, 128])
