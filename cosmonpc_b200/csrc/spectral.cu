@@ -15,8 +15,17 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
     extern __shared__ double tbl[];
     AxisTable ax;
     fill_axis_table(ax, tbl, n, L, comp, p);
-    __syncthreads();
     const double H = L / n;
+    // the interlacing phase e^{i (kx + ky + kz) H / 2} as the product of one
+    // factor per axis, each from a per-block table of e^{i k H / 2}
+    double2 *ph = reinterpret_cast<double2 *>(tbl + 2 * (n + 1));  // [n + 1]
+    if (spec2)
+        for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+            double sp, cp;
+            sincos(0.5 * (ax.k[i] * H), &sp, &cp);
+            ph[i] = make_double2(cp, sp);
+        }
+    __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
         const Mode m = mode_of(t, n);
@@ -24,9 +33,9 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
         const double kn = knorm_from(kx, ky, kz);
         double re = (double)spec[t].x * inv_n3, im = (double)spec[t].y * inv_n3;
         if (spec2) {
-            const double ph = 0.5 * ((kx * H + ky * H) + kz * H);
-            double sp, cp;
-            sincos(ph, &sp, &cp);
+            const double2 ex = ph[m.nx + n / 2], ey = ph[m.ny + n / 2], ez = ph[m.nz + n / 2];
+            const double cxy = ex.x * ey.x - ex.y * ey.y, sxy = ex.x * ey.y + ex.y * ey.x;
+            const double cp = cxy * ez.x - sxy * ez.y, sp = cxy * ez.y + sxy * ez.x;
             const double r2 = (double)spec2[t].x * inv_n3, i2 = (double)spec2[t].y * inv_n3;
             re = 0.5 * re + 0.5 * (r2 * cp - i2 * sp);
             im = 0.5 * im + 0.5 * (r2 * sp + i2 * cp);
@@ -47,9 +56,30 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
 }
 
 // ------------------------------------------------------------ mode counts
-__global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *counts, double *ksum,
-                                   BandIter bi) {
-    const int64_t nh = bi.count;
+// The counts fold the half spectrum over the signs of n_x and n_y: k = 2 n pi / L
+// is odd in n bit for bit and |k| squares it, so the modes (+-n_x, +-n_y, n_z)
+// share |k| and bin.  The quadrant n_x, n_y in [0, R] (R = n/2 on the whole
+// spectrum, where n_d = n/2 stands for the single mode -n/2) is summed with
+// weight 2 per axis for 0 < n_d < n/2 and 1 otherwise, times the Hermitian
+// multiplicity of n_z: the same counts (exact integers) and |k| sums to
+// rounding, over a quarter of the modes.  Consecutive u are consecutive n_z
+// of one row, as warp_run_add wants.
+struct QuadIter {
+    int n, R, RZ;  // n_x, n_y in [0, R], n_z in [0, RZ]
+    int64_t count;
+};
+
+inline QuadIter quad_iter(int n, double boxsize, double e_last) {
+    const BandIter bi = band_iter(n, boxsize, e_last);
+    QuadIter q;
+    q.n = n;
+    q.R = bi.R < 0 ? n / 2 : bi.R;
+    q.RZ = bi.R < 0 ? n / 2 : bi.R;
+    q.count = (int64_t)(q.R + 1) * (q.R + 1) * (q.RZ + 1);
+    return q;
+}
+
+__global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *counts, double *ksum, QuadIter qi) {
     extern __shared__ double sm[];
     AxisTable ax;
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
@@ -60,17 +90,31 @@ __global__ void kbin_counts_kernel(int n, double L, EdgeSet edges, double *count
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+    const uint32_t w = qi.R + 1, nzc = qi.RZ + 1;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < qi.count;
          base += wstride) {
         const int64_t t = base + lane;
         int bin = -1;
         double kn = 0.0, mult = 0.0;
-        if (t < nh) {
-            int64_t tt;
-            const Mode m = bi.mode(t, &tt);
-            kn = knorm_from(ax.kx(m.nx), ax.kx(m.ny), ax.kx(m.nz));
+        if (t < qi.count) {
+            int iz, jy, jx;
+            if (t < ((int64_t)1 << 31)) {
+                uint32_t rz, ry;
+                const uint32_t r = udiv31((uint32_t)t, nzc, &rz);
+                jx = (int)udiv31(r, w, &ry);
+                iz = (int)rz;
+                jy = (int)ry;
+            } else {
+                iz = (int)(t % nzc);
+                const int64_t r = t / nzc;
+                jy = (int)(r % w);
+                jx = (int)(r / w);
+            }
+            kn = knorm_from(ax.kx(jx), ax.kx(jy), ax.kx(iz));
             bin = find_bin(kn, e, edges.n);
-            mult = m.mult;
+            const int wx = (jx == 0 || 2 * jx == n) ? 1 : 2, wy = (jy == 0 || 2 * jy == n) ? 1 : 2;
+            const int wz = (iz == 0 || 2 * iz == n) ? 1 : 2;
+            mult = (double)(wx * wy * wz);
         }
         double v[2] = {mult, mult * kn};
         warp_run_add<2>(bins, nb, bin, v);
@@ -321,7 +365,7 @@ int cnpc_forward_finish_band(cnpc_ctx *ctx, int dtype, int n, double boxsize, vo
     cudaStream_t s = (cudaStream_t)stream;
     const int threads = 256;
     const int blocks = grid_for(ctx, nh, threads);
-    const size_t tsm = 2 * sizeof(double) * (n + 1);
+    const size_t tsm = 4 * sizeof(double) * (n + 1);  // k, compensation, interlacing phase
     if (dtype == CNPC_F32)
         forward_finish_kernel<float><<<blocks, threads, tsm, s>>>(
             (float2 *)d_spec, (const float2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
@@ -354,11 +398,10 @@ int cnpc_kbin_counts(cnpc_ctx *ctx, int n, double boxsize, const double *h_edges
     if (st) return st;
     st = check_cuda(ctx, cudaMemsetAsync(d_ksum, 0, sizeof(double) * nb, s), "memset");
     if (st) return st;
-    const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
-    const int64_t nh = bi.count;
+    const QuadIter qi = quad_iter(n, boxsize, h_edges[nedges - 1]);
     const int threads = 256;
-    kbin_counts_kernel<<<grid_for(ctx, nh, threads), threads, (n + 1 + 2 * nb + nedges) * sizeof(double), s>>>(
-        n, boxsize, es, d_counts, d_ksum, bi);
+    kbin_counts_kernel<<<grid_for(ctx, qi.count, threads), threads, (n + 1 + 2 * nb + nedges) * sizeof(double), s>>>(
+        n, boxsize, es, d_counts, d_ksum, qi);
     return check_launch(ctx, "kbin_counts_kernel");
 }
 
