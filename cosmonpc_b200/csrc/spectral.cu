@@ -206,7 +206,7 @@ struct SnCfg {
 
 template <typename T, int NC>
 __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, double vsq, int p,
-                               EdgeSet edges, const SnCfg cfg, double band, int64_t nh) {
+                               EdgeSet edges, const SnCfg cfg, double band, int64_t nq) {
     extern __shared__ double sm[];
     bool any_sn0 = false, any_src = false;
 #pragma unroll
@@ -230,46 +230,66 @@ __global__ void sn_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
     for (int c = 0; c < NC; ++c) tot[c] = 0.0;
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+    const int h = n / 2;
+    const uint32_t w1 = h + 1;
+    // item u = (jx, jy, iz), jx, jy, iz in [0, n/2]: the modes (+-jx, +-jy, iz)
+    // (one sign where jx or jy is 0 or n/2, n/2 standing for -n/2) share |k|,
+    // bin and Y_L0 (a function of k_z / |k|); their values are summed in the
+    // item before the warp's run sums
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nq;
          base += wstride) {
-        const int64_t t = base + lane;
+        const int64_t u = base + lane;
         int bin = -1;
         double val[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) val[c] = 0.0;
-        if (t < nh) {
-            const Mode m = mode_of(t, n);
-            const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
+        if (u < nq) {
+            uint32_t rz, ry;
+            const uint32_t r = udiv31((uint32_t)u, w1, &rz);
+            const int jx = (int)udiv31(r, w1, &ry), jy = (int)ry, iz = (int)rz;
+            const double kx = ax.kx(jx), ky = ax.kx(jy), kz = ax.kx(iz);
             const double kn = knorm_from(kx, ky, kz);
             bin = find_bin(kn, e, edges.n);
             const bool keep = !(band > 0.0) || kn < band;
-            if (bin >= 0 || (any_src && keep)) {
-                const cpx_t<T> va = a[t], vb = b[t];
-                const double pr0 = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
-                const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
-                const double w = any_sn0 ? ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz) : 0.0;
+            const double mult = (iz == 0 || 2 * iz == n) ? 1.0 : 2.0;
+            const int nsx = (jx == 0 || jx == h) ? 1 : 2, nsy = (jy == 0 || jy == h) ? 1 : 2;
+            const bool live = bin >= 0 || (any_src && keep);
+            double y[NC];
+            if (live && bin >= 0) {
                 const bool origin = kn == 0.0;
                 const double ik = origin ? 0.0 : 1.0 / kn;
 #pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    double pr = pr0;
-                    if (cfg.sn0[c] != 0.0) pr -= cfg.sn0[c] * w;
-                    if (cfg.source[c]) {
-                        static_cast<cpx_t<T> *>(cfg.source[c])[t] = keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
-                        // the stored source is Hermitian on |k| < band: mult * Re sums the full space
-                        if (keep) tot[c] += m.mult * (double)(T)pr;
-                    }
-                    if (bin >= 0) {
-                        double y = 1.0;
-                        if (cfg.use_y[c]) y = harmonic_eval<double>(s_y[c], kx * ik, ky * ik, kz * ik, origin).x;
-                        val[c] = m.mult * pr * y;
+                for (int c = 0; c < NC; ++c)
+                    y[c] = cfg.use_y[c] ? harmonic_eval<double>(s_y[c], kx * ik, ky * ik, kz * ik, origin).x : 1.0;
+            }
+            for (int sx = 0; sx < nsx; ++sx)
+                for (int sy = 0; sy < nsy; ++sy) {
+                    const int nx = (sx || jx == h) ? -jx : jx, ny = (sy || jy == h) ? -jy : jy;
+                    const int ix = nx < 0 ? nx + n : nx, iy = ny < 0 ? ny + n : ny;
+                    const int64_t t = ((int64_t)ix * n + iy) * w1 + iz;
+                    if (live) {
+                        const cpx_t<T> va = a[t], vb = b[t];
+                        const double pr0 = vsq * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+                        const double pi = vsq * ((double)va.y * (double)vb.x - (double)va.x * (double)vb.y);
+                        const double w = any_sn0 ? ax.f(nx) * ax.f(ny) * ax.f(iz) : 0.0;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            double pr = pr0;
+                            if (cfg.sn0[c] != 0.0) pr -= cfg.sn0[c] * w;
+                            if (cfg.source[c]) {
+                                static_cast<cpx_t<T> *>(cfg.source[c])[t] =
+                                    keep ? mk<T>((T)pr, (T)pi) : mk<T>((T)0, (T)0);
+                                // the stored source is Hermitian on |k| < band: mult * Re sums the full space
+                                if (keep) tot[c] += mult * (double)(T)pr;
+                            }
+                            if (bin >= 0) val[c] += mult * pr * y[c];
+                        }
+                    } else if (any_src) {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c)
+                            if (cfg.source[c]) static_cast<cpx_t<T> *>(cfg.source[c])[t] = mk<T>((T)0, (T)0);
                     }
                 }
-            } else if (any_src) {
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (cfg.source[c]) static_cast<cpx_t<T> *>(cfg.source[c])[t] = mk<T>((T)0, (T)0);
-            }
         }
         warp_run_add<NC>(bins, nbt, bin, val);
     }
@@ -469,14 +489,14 @@ static int run_sn_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const vo
         st = check_cuda(ctx, cudaMemsetAsync(d_sums[c], 0, sizeof(double) * 2 * nbt, s), "memset");
         if (st) return st;
     }
-    const int64_t nh = half_modes(n);
+    const int64_t nq = (int64_t)(n / 2 + 1) * (n / 2 + 1) * (n / 2 + 1);  // sign-folded items
     const int threads = 256;
     const size_t smem = sizeof(double) * (2 * (n + 1) + ncfg * (nb + 1) + nedges);
-    const int grid = grid_for(ctx, nh, threads);
+    const int grid = grid_for(ctx, nq, threads);
 #define CNPC_SN_LAUNCH(T_, NC_)                                                                          \
     sn_bins_kernel<T_, NC_><<<grid, threads, smem, s>>>((const cpx_t<T_> *)d_spec_a,                     \
                                                        (const cpx_t<T_> *)d_spec_b, n, boxsize, volume_sq, \
-                                                       window, es, cfg, band_kmax, nh)
+                                                       window, es, cfg, band_kmax, nq)
     if (dtype == CNPC_F32) {
         if (ncfg == 1) CNPC_SN_LAUNCH(float, 1);
         else CNPC_SN_LAUNCH(float, 2);
