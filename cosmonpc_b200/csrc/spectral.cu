@@ -11,7 +11,7 @@ namespace cnpc {
 template <typename T>
 __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int n, double L,
                                       double inv_n3, double scale, int comp, int p, double k0,
-                                      double band, cpx_t<T> *band_out, double band_out_k, int64_t nh) {
+                                      double band, cpx_t<T> *band_out, double band_out_k, int64_t nq) {
     extern __shared__ double tbl[];
     AxisTable ax;
     fill_axis_table(ax, tbl, n, L, comp, p);
@@ -26,32 +26,61 @@ __global__ void forward_finish_kernel(cpx_t<T> *spec, const cpx_t<T> *spec2, int
             ph[i] = make_double2(cp, sp);
         }
     __syncthreads();
+    // item u = (jx, jy, iz), jx, jy, iz in [0, n/2]: the 1-4 modes
+    // (+-jx, +-jy, iz) (one sign where jx or jy is 0 or n/2, n/2 standing for
+    // -n/2) share |k| and so the band tests; their loads are issued together
+    const int h = n / 2;
+    const uint32_t w1 = h + 1;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nh; t += stride) {
-        const Mode m = mode_of(t, n);
-        const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
-        const double kn = knorm_from(kx, ky, kz);
-        double re = (double)spec[t].x * inv_n3, im = (double)spec[t].y * inv_n3;
-        if (spec2) {
-            const double2 ex = ph[m.nx + n / 2], ey = ph[m.ny + n / 2], ez = ph[m.nz + n / 2];
-            const double cxy = ex.x * ey.x - ex.y * ey.y, sxy = ex.x * ey.y + ex.y * ey.x;
-            const double cp = cxy * ez.x - sxy * ez.y, sp = cxy * ez.y + sxy * ez.x;
-            const double r2 = (double)spec2[t].x * inv_n3, i2 = (double)spec2[t].y * inv_n3;
-            re = 0.5 * re + 0.5 * (r2 * cp - i2 * sp);
-            im = 0.5 * im + 0.5 * (r2 * sp + i2 * cp);
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nq; u += stride) {
+        uint32_t rz, ry;
+        const uint32_t r = udiv31((uint32_t)u, w1, &rz);
+        const int jx = (int)udiv31(r, w1, &ry), jy = (int)ry, iz = (int)rz;
+        const double kn = knorm_from(ax.kx(jx), ax.kx(jy), ax.kx(iz));
+        const bool cut = band > 0.0 && kn >= band;
+        const bool in_out = kn < band_out_k;
+        const int nsx = (jx == 0 || jx == h) ? 1 : 2, nsy = (jy == 0 || jy == h) ? 1 : 2;
+        // mode q = 2 sx + sy of the orbit, present when sx < nsx and sy < nsy
+        auto mode_nx = [&](int q) { return ((q >> 1) || jx == h) ? -jx : jx; };
+        auto mode_ny = [&](int q) { return ((q & 1) || jy == h) ? -jy : jy; };
+        auto mode_t = [&](int q) {
+            const int nx = mode_nx(q), ny = mode_ny(q);
+            return ((int64_t)(nx < 0 ? nx + n : nx) * n + (ny < 0 ? ny + n : ny)) * w1 + iz;
+        };
+        cpx_t<T> va[4], vb[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if ((q >> 1) < nsx && (q & 1) < nsy) {
+                va[q] = spec[mode_t(q)];
+                if (spec2) vb[q] = spec2[mode_t(q)];
+            }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if ((q >> 1) >= nsx || (q & 1) >= nsy) continue;
+            const int64_t t = mode_t(q);
+            const int mxq = mode_nx(q), myq = mode_ny(q);
+            double re = (double)va[q].x * inv_n3, im = (double)va[q].y * inv_n3;
+            if (spec2) {
+                const double2 ex = ph[mxq + h], ey = ph[myq + h], ez = ph[iz + h];
+                const double cxy = ex.x * ey.x - ex.y * ey.y, sxy = ex.x * ey.y + ex.y * ey.x;
+                const double cp = cxy * ez.x - sxy * ez.y, sp = cxy * ez.y + sxy * ez.x;
+                const double r2 = (double)vb[q].x * inv_n3, i2 = (double)vb[q].y * inv_n3;
+                re = 0.5 * re + 0.5 * (r2 * cp - i2 * sp);
+                im = 0.5 * im + 0.5 * (r2 * sp + i2 * cp);
+            }
+            double f = scale;
+            if (ax.cf) f *= ax.f(mxq) * ax.f(myq) * ax.f(iz);
+            re *= f;
+            im *= f;
+            if (t == 0 && !isnan(k0)) {
+                re = k0;
+                im = 0.0;
+            }
+            if (cut) re = im = 0.0;
+            spec[t] = mk<T>((T)re, (T)im);
+            // band_out may be spec2: this thread read its element t above
+            if (band_out) band_out[t] = in_out ? mk<T>((T)re, (T)im) : mk<T>((T)0, (T)0);
         }
-        double f = scale;
-        if (ax.cf) f *= ax.f(m.nx) * ax.f(m.ny) * ax.f(m.nz);
-        re *= f;
-        im *= f;
-        if (t == 0 && !isnan(k0)) {
-            re = k0;
-            im = 0.0;
-        }
-        if (band > 0.0 && kn >= band) re = im = 0.0;
-        spec[t] = mk<T>((T)re, (T)im);
-        // band_out may be spec2: its element t was read above by this thread
-        if (band_out) band_out[t] = kn < band_out_k ? mk<T>((T)re, (T)im) : mk<T>((T)0, (T)0);
     }
 }
 
@@ -380,20 +409,20 @@ int cnpc_forward_finish_band(cnpc_ctx *ctx, int dtype, int n, double boxsize, vo
     CNPC_REQUIRE(ctx, comp >= 0 && comp <= 3, "bad compensation kind");
     CNPC_REQUIRE(ctx, window >= 1 && window <= 4, "window must be 1..4");
     CNPC_REQUIRE(ctx, d_band_out != d_spec, "band output must not be the spectrum");
-    const int64_t nh = half_modes(n);
+    const int64_t nq = (int64_t)(n / 2 + 1) * (n / 2 + 1) * (n / 2 + 1);  // sign orbits of the half spectrum
     const double inv_n3 = 1.0 / ((double)n * n * n);
     cudaStream_t s = (cudaStream_t)stream;
     const int threads = 256;
-    const int blocks = grid_for(ctx, nh, threads);
+    const int blocks = grid_for(ctx, nq, threads);
     const size_t tsm = 4 * sizeof(double) * (n + 1);  // k, compensation, interlacing phase
     if (dtype == CNPC_F32)
         forward_finish_kernel<float><<<blocks, threads, tsm, s>>>(
             (float2 *)d_spec, (const float2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
-            k0_value, band_kmax, (float2 *)d_band_out, band_out_kmax, nh);
+            k0_value, band_kmax, (float2 *)d_band_out, band_out_kmax, nq);
     else
         forward_finish_kernel<double><<<blocks, threads, tsm, s>>>(
             (double2 *)d_spec, (const double2 *)d_spec2, n, boxsize, inv_n3, scale, comp, window,
-            k0_value, band_kmax, (double2 *)d_band_out, band_out_kmax, nh);
+            k0_value, band_kmax, (double2 *)d_band_out, band_out_kmax, nq);
     return check_launch(ctx, "forward_finish_kernel");
 }
 

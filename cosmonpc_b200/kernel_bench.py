@@ -3,6 +3,7 @@
     python -m cosmonpc_b200.kernel_bench shells --n 256 --items 8 [--reps 5]
     python -m cosmonpc_b200.kernel_bench gram --n 256 --rows 40 --cols 20 [--tc]
     python -m cosmonpc_b200.kernel_bench paint --n 256 --particles 4000000 --window 4
+    python -m cosmonpc_b200.kernel_bench spectral --n 256
 
 Each prints one line: the call, its mean device time (CUDA events over
 --reps calls after one warm-up call) and its algorithmic bytes per call.
@@ -84,9 +85,44 @@ def paint(n, particles, window, reps):
             "bytes": particles * 24 + 2 * n ** 3 * 4}
 
 
+def spectral(n, reps):
+    """The per-mode spectral passes of a bk_sugi data vector at the 256^3
+    workload's binning scaled to n (L = 2000 n / 256, 20 bins 0.01-0.2, k3 bins
+    0.02-0.39): cnpc_kbin_counts (k and k3 bins), cnpc_sn_bins_multi (two
+    configurations, one S3 source, band 0.4), cnpc_forward_finish (interlaced,
+    PCS compensation) and cnpc_field_parity_fold (FP32)."""
+    ctx = _lib.Context.get()
+    L = 2000.0 * n / 256
+    k_edge = np.linspace(0.01, 0.2, 21)
+    k3_edge = np.linspace(0.02, 0.4, 41)[:-1]
+    g = torch.Generator(device="cuda").manual_seed(2)
+    real = torch.randn((n, n, n), device="cuda", generator=g)
+    spec = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    spec2 = torch.empty_like(spec)
+    ctx.r2c(_lib.F32, n, 1, real, spec)
+    ctx.r2c(_lib.F32, n, 1, real, spec2)
+    src = torch.empty_like(spec)
+    sums = [torch.empty(2 * 41, dtype=torch.float64, device="cuda") for _ in range(2)]
+    counts = torch.empty(40, dtype=torch.float64, device="cuda")
+    ksum = torch.empty_like(counts)
+    half = torch.empty((n // 2 + 1) * n * n, device="cuda")
+    nh = n * n * (n // 2 + 1)
+    out = {}
+    out["kbin_counts_k"] = _time(lambda: ctx.kbin_counts(n, L, k_edge, counts[:20], ksum[:20]), reps)
+    out["kbin_counts_k3"] = _time(lambda: ctx.kbin_counts(n, L, k3_edge, counts[:39], ksum[:39]), reps)
+    out["sn_bins_multi"] = _time(lambda: ctx.sn_bins_multi(_lib.F32, n, L, spec, spec, 6.4e19, 4, [1e-3, 1e-3],
+                                                           [None, angular.harmonic(2, 0, True)], k3_edge, sums,
+                                                           [src, None], band=0.4), reps)
+    out["forward_finish"] = _time(lambda: ctx.forward_finish(_lib.F32, n, L, spec, spec2, 1.0, _lib.COMP_SINC, 4,
+                                                             0.0, 0.0), reps)
+    out["parity_fold"] = _time(lambda: ctx.field_parity_fold(_lib.F32, n, real.view(-1), -1, half), reps)
+    return {"call": "spectral", "n": n, "ms": out, "bytes": {"sn_bins_multi": 2 * nh * 8, "forward_finish": 3 * nh * 8,
+                                                             "parity_fold": (3 * (n // 2) + 1) * n * n * 4}}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["shells", "gram", "paint"])
+    ap.add_argument("what", choices=["shells", "gram", "paint", "spectral"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--items", type=int, default=8)
     ap.add_argument("--rows", type=int, default=40)
@@ -102,9 +138,14 @@ def main(argv=None):
         r = shells(args.n, args.items, args.reps, source=args.source)
     elif args.what == "gram":
         r = gram(args.n, args.rows, args.cols, args.reps, args.tc)
-    else:
+    elif args.what == "paint":
         r = paint(args.n, args.particles, args.window, args.reps)
-    r["GB_per_s"] = r["bytes"] / (r["ms"] * 1e6)
+    else:
+        r = spectral(args.n, args.reps)
+    if args.what == "spectral":
+        r["GB_per_s"] = {k: b / (r["ms"][k] * 1e6) for k, b in r["bytes"].items()}
+    else:
+        r["GB_per_s"] = r["bytes"] / (r["ms"] * 1e6)
     print(json.dumps(r))
 
 
