@@ -413,19 +413,36 @@ __global__ void __launch_bounds__(kFfWarps * 32, 2)
     fold();  // also defines the partial of a warp that had no chunk
 }
 
-// One warp per output: lane l sums partials l, l+32, ... and a fixed shuffle
-// tree combines the lanes, so the result is bitwise reproducible.
-__global__ void gram_window_reduce_kernel(const double *partial, int nparts, int wr, int wc, int na, int nb,
-                                          double *out) {
-    const int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (o >= na * nb) return;
-    const int i = o / nb, j = o % nb;
+// out[i nb + j] = the sum over the parts p of partial[p][i][j], in a fixed
+// order (bitwise reproducible): block b takes the 32 window entries
+// e = 32 b + lane (e = i wc + j), warp w sums the parts w, w + 32, ... of its
+// lane's entry (each warp load reads 32 consecutive entries of one part), and
+// the 32 warp sums are added in warp order.
+constexpr int kReduceWarps = 32;
+__global__ void __launch_bounds__(32 * kReduceWarps)
+    gram_window_reduce_kernel(const double *partial, int nparts, int wr, int wc, int na, int nb, double *out) {
+    __shared__ double ws[kReduceWarps][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int e = blockIdx.x * 32 + lane;
+    const int64_t W = (int64_t)wr * wc;
     double s = 0.0;
-    for (int p = lane; p < nparts; p += 32) s += partial[(int64_t)p * wr * wc + i * wc + j];
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) out[o] = s;
+    if (e < na * wc) {
+#pragma unroll 4
+        for (int p = warp; p < nparts; p += kReduceWarps) s += partial[p * W + e];
+    }
+    ws[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && e < na * wc) {
+        double t = 0.0;
+        for (int w = 0; w < kReduceWarps; ++w) t += ws[w][lane];
+        const int i = e / wc, j = e - (e / wc) * wc;
+        if (j < nb) out[i * nb + j] = t;
+    }
+}
+
+static inline void launch_window_reduce(const double *partial, int nparts, int wr, int wc, int na, int nb,
+                                        double *out, cudaStream_t s) {
+    gram_window_reduce_kernel<<<(na * wc + 31) / 32, 32 * kReduceWarps, 0, s>>>(partial, nparts, wr, wc, na, nb, out);
 }
 
 // Staged rows and window of an FP32 Gram launch (na <= 48, nb <= 24).
@@ -523,8 +540,7 @@ static int run_gram_ffma(cnpc_ctx *ctx, int64_t ncell, const float *g, const flo
     std::memset(&X, 0, sizeof(X));
     st = check_cuda(ctx, ff_launch<false>(pl, nblocks, g, fields, X, part, s), "gram_ffma_kernel");
     if (st) return st;
-    const int nout = na * nb;
-    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
+    launch_window_reduce(part, nparts, pl.wr, pl.wc, na, nb, out, s);
     return check_launch(ctx, "gram_window_reduce_kernel");
 }
 
@@ -552,8 +568,7 @@ static int run_gram_ffma_mg(cnpc_ctx *ctx, int64_t ncell, const float *const *gs
     double *part = (double *)ctx->scratch;
     st = check_cuda(ctx, ff_launch<true>(pl, nblocks, gs[0], fields, X, part, s), "gram_ffma_kernel");
     if (st) return st;
-    const int nout = na * nb;
-    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(part, nparts, pl.wr, pl.wc, na, nb, out);
+    launch_window_reduce(part, nparts, pl.wr, pl.wc, na, nb, out, s);
     return check_launch(ctx, "gram_window_reduce_kernel");
 }
 
@@ -787,9 +802,7 @@ static int noalloc_gram_f32(int64_t ncell, const float *g, const float *fields, 
     std::memset(&X, 0, sizeof(X));
     st = noalloc_cuda(ff_launch<false>(pl, nblocks, g, fields, X, scratch, s));
     if (st) return st;
-    const int nout = na * nb;
-    gram_window_reduce_kernel<<<(nout + 7) / 8, 256, 0, s>>>(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na, nb,
-                                                             out);
+    launch_window_reduce(scratch, nblocks * kFfWarps, pl.wr, pl.wc, na, nb, out, s);
     return noalloc_cuda(cudaGetLastError());
 }
 
