@@ -502,7 +502,6 @@ template <typename T>
 __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, int p, unsigned kinds,
                                    double sbr, double sbi, int has_z, cnpc_harmonic zh, int conj_z,
                                    double weight, EdgeSet edges, double *sums, BandIter bi) {
-    const int64_t nh = bi.count;
     extern __shared__ double sm[];
     CompTables ct;
     fill_comp_tables(ct, sm, n, L, p, kinds);
@@ -516,45 +515,61 @@ __global__ void survey_bins_kernel(OperandDev u, OperandDev v, int n, double L, 
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const bool sbar = sbr != 0.0 || sbi != 0.0;
+    // item u = (jx, jy, iz) of the band cube folded over the signs of n_x and
+    // n_y: the modes (+-jx, +-jy, iz) (one sign where jx or jy is 0 or n/2,
+    // n/2 standing for -n/2) share |k| and bin; each mode keeps its own
+    // operands, compensation and Z(khat), and the item sums their terms
+    const int h = n / 2, R = bi.R < 0 ? h : bi.R;
+    const uint32_t w1 = R + 1;
+    const int64_t nq = (int64_t)w1 * w1 * w1;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh; base += wstride) {
-        const int64_t t = base + lane;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nq; base += wstride) {
+        const int64_t u_ = base + lane;
         int bin = -1;
         double accr = 0.0, acci = 0.0;
-        if (t < nh) {
-            int64_t tt;
-            const Mode m = bi.mode(t, &tt);
-            const double kx = ct.k[m.nx + ct.half], ky = ct.k[m.ny + ct.half], kz = ct.k[m.nz + ct.half];
-            const double kn = knorm_from(kx, ky, kz);
+        if (u_ < nq) {
+            uint32_t rz, ry;
+            const uint32_t r = udiv31((uint32_t)u_, w1, &rz);
+            const int jx = (int)udiv31(r, w1, &ry), jy = (int)ry, iz = (int)rz;
+            const double kn = knorm_from(ct.k[jx + ct.half], ct.k[jy + ct.half], ct.k[iz + ct.half]);
             bin = find_bin(kn, e, edges.n);
             if (bin >= 0) {
-                double2 uk, um, vk, vm;
-                load_operand<T>(u, tt, ct.factor(u.comp, m.nx, m.ny, m.nz), &uk, &um);
-                load_operand<T>(v, tt, ct.factor(v.comp, m.nx, m.ny, m.nz), &vk, &vm);
-                const double wsn = sbar ? ct.factor(CNPC_COMP_BKNOISE, m.nx, m.ny, m.nz) : 0.0;
-                double zr = 1.0, zi = 0.0;
-                int parity = 1;
-                if (has_z) {
-                    const bool origin = kn == 0.0;
-                    const double2 z = harmonic_eval<double>(s_z, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
-                                                            origin ? 0.0 : kz / kn, origin);
-                    zr = z.x;
-                    zi = conj_z ? -z.y : z.y;
-                    parity = (zh.l & 1) ? -1 : 1;
+                const int nsx = (jx == 0 || jx == h) ? 1 : 2, nsy = (jy == 0 || jy == h) ? 1 : 2;
+                const bool two = !(iz == 0 || 2 * iz == n);  // the mode -k is a distinct mode
+                const double kz = ct.k[iz + ct.half];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if ((q >> 1) >= nsx || (q & 1) >= nsy) continue;
+                    const int nx = ((q >> 1) || jx == h) ? -jx : jx, ny = ((q & 1) || jy == h) ? -jy : jy;
+                    const int64_t tt = ((int64_t)(nx < 0 ? nx + n : nx) * n + (ny < 0 ? ny + n : ny)) * (h + 1) + iz;
+                    const double kx = ct.k[nx + ct.half], ky = ct.k[ny + ct.half];
+                    double2 uk, um, vk, vm;
+                    load_operand<T>(u, tt, ct.factor(u.comp, nx, ny, iz), &uk, &um);
+                    load_operand<T>(v, tt, ct.factor(v.comp, nx, ny, iz), &vk, &vm);
+                    const double wsn = sbar ? ct.factor(CNPC_COMP_BKNOISE, nx, ny, iz) : 0.0;
+                    double zr = 1.0, zi = 0.0;
+                    int parity = 1;
+                    if (has_z) {
+                        const bool origin = kn == 0.0;
+                        const double2 z = harmonic_eval<double>(s_z, origin ? 0.0 : kx / kn, origin ? 0.0 : ky / kn,
+                                                                origin ? 0.0 : kz / kn, origin);
+                        zr = z.x;
+                        zi = conj_z ? -z.y : z.y;
+                        parity = (zh.l & 1) ? -1 : 1;
+                    }
+                    // term(k) = (U conj V - sbar W) Z
+                    double ar = uk.x * vk.x + uk.y * vk.y - sbr * wsn;
+                    double ai = uk.y * vk.x - uk.x * vk.y - sbi * wsn;
+                    double tr = ar * zr - ai * zi, ti = ar * zi + ai * zr;
+                    if (two) {
+                        ar = um.x * vm.x + um.y * vm.y - sbr * wsn;
+                        ai = um.y * vm.x - um.x * vm.y - sbi * wsn;
+                        tr += parity * (ar * zr - ai * zi);
+                        ti += parity * (ar * zi + ai * zr);
+                    }
+                    accr += tr * weight;
+                    acci += ti * weight;
                 }
-                // term(k) = (U conj V - sbar W) Z
-                double ar = uk.x * vk.x + uk.y * vk.y - sbr * wsn;
-                double ai = uk.y * vk.x - uk.x * vk.y - sbi * wsn;
-                accr = ar * zr - ai * zi;
-                acci = ar * zi + ai * zr;
-                if (m.mult == 2) {
-                    ar = um.x * vm.x + um.y * vm.y - sbr * wsn;
-                    ai = um.y * vm.x - um.x * vm.y - sbi * wsn;
-                    accr += parity * (ar * zr - ai * zi);
-                    acci += parity * (ar * zi + ai * zr);
-                }
-                accr *= weight;
-                acci *= weight;
             }
         }
         double v[2] = {accr, acci};
@@ -901,7 +916,8 @@ int cnpc_survey_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, int window
     st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * 2 * nb, s), "memset");
     if (st) return st;
     const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
-    const int64_t nh = bi.count;
+    const int64_t rq = bi.R < 0 ? n / 2 : bi.R;
+    const int64_t nh = (rq + 1) * (rq + 1) * (rq + 1);  // sign-folded items
     const int threads = 256;
     const size_t smem = sizeof(double) * (ntab * (n + 1) + 2 * nb + nedges);
     if (dtype == CNPC_F32)
