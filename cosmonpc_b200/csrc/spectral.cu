@@ -165,7 +165,6 @@ struct PoleSet {
 template <typename T>
 __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, double L, EdgeSet edges,
                                PoleSet poles, double *sums, BandIter bi) {
-    const int64_t nh = bi.count;
     extern __shared__ double sm[];
     AxisTable ax;
     fill_axis_table(ax, sm, n, L, CNPC_COMP_NONE, 1);
@@ -175,44 +174,77 @@ __global__ void pk_bins_kernel(const cpx_t<T> *a, const cpx_t<T> *b, int n, doub
     for (int i = threadIdx.x; i < poles.n * nb; i += blockDim.x) bins[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    // item u = (jx, jy, iz) of the band cube folded over the signs of n_x and
+    // n_y: the modes (+-jx, +-jy, iz) (one sign where jx or jy is 0 or n/2,
+    // n/2 standing for -n/2) share |k| and bin, and with the line of sight
+    // along z also mu and the Legendre values, which then run once per item
+    const bool los_z = poles.los[0] == 0.0 && poles.los[1] == 0.0;
+    const int h = n / 2, R = bi.R < 0 ? h : bi.R;
+    const uint32_t w1 = R + 1;
+    const int64_t nq = (int64_t)w1 * w1 * w1;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nh;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nq;
          base += wstride) {
-        const int64_t t = base + lane;
+        const int64_t u = base + lane;
         int bin = -1;
-        double pv = 0.0, mu = 0.0;
-        if (t < nh) {
-            int64_t tt;
-            const Mode m = bi.mode(t, &tt);
-            const double kx = ax.kx(m.nx), ky = ax.kx(m.ny), kz = ax.kx(m.nz);
-            const double kn = knorm_from(kx, ky, kz);
+        int jx = 0, jy = 0, iz = 0, nsx = 1, nsy = 1;
+        double kn = 0.0, mult = 0.0;
+        if (u < nq) {
+            uint32_t rz, ry;
+            const uint32_t r = udiv31((uint32_t)u, w1, &rz);
+            jx = (int)udiv31(r, w1, &ry);
+            jy = (int)ry;
+            iz = (int)rz;
+            kn = knorm_from(ax.kx(jx), ax.kx(jy), ax.kx(iz));
             bin = find_bin(kn, e, edges.n);
-            if (bin >= 0) {
+            nsx = (jx == 0 || jx == h) ? 1 : 2;
+            nsy = (jy == 0 || jy == h) ? 1 : 2;
+            mult = (iz == 0 || 2 * iz == n) ? 1.0 : 2.0;
+        }
+        // the orbit's members: power |delta|^2 and mu of member q = 2 sx + sy
+        double pvq[4] = {0.0, 0.0, 0.0, 0.0}, muq[4] = {0.0, 0.0, 0.0, 0.0};
+        if (bin >= 0) {
+            const double kz = ax.kx(iz);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if ((q >> 1) >= nsx || (q & 1) >= nsy) continue;
+                const int nx = ((q >> 1) || jx == h) ? -jx : jx, ny = ((q & 1) || jy == h) ? -jy : jy;
+                const int64_t tt = ((int64_t)(nx < 0 ? nx + n : nx) * n + (ny < 0 ? ny + n : ny)) * (h + 1) + iz;
                 const cpx_t<T> va = a[tt], vb = b[tt];
-                pv = m.mult * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
+                pvq[q] = mult * ((double)va.x * (double)vb.x + (double)va.y * (double)vb.y);
                 if (kn > 0.0)
-                    mu = (kx / kn) * poles.los[0] + (ky / kn) * poles.los[1] + (kz / kn) * poles.los[2];
+                    muq[q] = (ax.kx(nx) / kn) * poles.los[0] + (ax.kx(ny) / kn) * poles.los[1] +
+                             (kz / kn) * poles.los[2];
             }
         }
         // poles in groups of four (a warp-uniform loop)
         for (int q0 = 0; q0 < poles.n; q0 += 4) {
-            const int nq = poles.n - q0 < 4 ? poles.n - q0 : 4;
+            const int np_ = poles.n - q0 < 4 ? poles.n - q0 : 4;
             double v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (q >= nq) break;
-                // Legendre P_l(mu) by the three-term recurrence
-                const int l = poles.l[q0 + q];
-                double p0 = 1.0, p1 = mu;
-                double pl = (l == 0) ? 1.0 : mu;
-                for (int j = 1; j < l; ++j) {
-                    pl = ((2 * j + 1) * mu * p1 - j * p0) / (j + 1);
-                    p0 = p1;
-                    p1 = pl;
+            for (int c = 0; c < 4; ++c) {
+                if (c >= np_) break;
+                const int l = poles.l[q0 + c];
+                v[c] = 0.0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (los_z && q > 0) break;  // one mu for the orbit
+                    // Legendre P_l(mu) by the three-term recurrence
+                    const double mu = muq[q];
+                    double p0 = 1.0, p1 = mu;
+                    double pl = (l == 0) ? 1.0 : mu;
+                    for (int j = 1; j < l; ++j) {
+                        pl = ((2 * j + 1) * mu * p1 - j * p0) / (j + 1);
+                        p0 = p1;
+                        p1 = pl;
+                    }
+                    if (los_z)
+                        v[c] += ((pvq[0] + pvq[1]) + (pvq[2] + pvq[3])) * pl;
+                    else
+                        v[c] += pvq[q] * pl;
                 }
-                v[q] = pv * pl;
             }
-            warp_run_add<4>(bins + q0 * nb, nb, bin, v, nq);
+            warp_run_add<4>(bins + q0 * nb, nb, bin, v, np_);
         }
     }
     __syncthreads();
@@ -476,7 +508,8 @@ int cnpc_pk_bins(cnpc_ctx *ctx, int dtype, int n, double boxsize, const void *d_
     st = check_cuda(ctx, cudaMemsetAsync(d_sums, 0, sizeof(double) * nb * npoles, s), "memset");
     if (st) return st;
     const BandIter bi = band_iter(n, boxsize, h_edges[nedges - 1]);
-    const int64_t nh = bi.count;
+    const int64_t rq = bi.R < 0 ? n / 2 : bi.R;
+    const int64_t nh = (rq + 1) * (rq + 1) * (rq + 1);  // sign-folded items
     const int threads = 256;
     const size_t smem = sizeof(double) * (n + 1 + nb * npoles + nedges);
     if (dtype == CNPC_F32)
